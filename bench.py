@@ -1,0 +1,372 @@
+#!/usr/bin/env python
+"""Benchmark of the coarse-grid field step (air + Newtonian gravity) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c1|c2|c4|c5] [--ticks T]
+
+Metric: cell-ticks/s = sum over instances of xcells*ycells * ticks / time;
+one tick is one air step plus one gravity solve of every instance (the
+reference re-solves gravity every tick). One bench "step" is one pass of the
+workload's tick count (1000 ticks for the batched workloads) over all its
+instances. Inputs are seeded synthetic sandboxes with the workloads' shapes
+(the reference publishes no dataset): see workloads.py.
+
+`value` is device-timed (CUDA events on the launching stream, inputs
+resident in HBM; the working set exceeds the 126 MB L2, so no flush is
+needed). `e2e` is the same metric through the public C ABI with host
+buffers: every step uploads the inputs from pinned host memory and reads the
+results back inside the timed region. Multi-GPU runs (torchrun) give every
+rank its own full copy of the workload (weak scaling, no collective in the
+data path); time is the max over ranks.
+
+`--impl reference` times the reference's CPU path -- the oracle's FP32
+restatement of the reference kernels (the reference itself needs Rust and
+wgpu, neither of which exists on these machines) -- on all host cores, on
+bounded samples of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "the-powder-toy-rust-wgpu_b200"))
+
+import numpy as np  # noqa: E402
+
+B_AIR = 52  # algorithmic bytes per cell-tick of the air step (reference layout)
+WORKLOAD_NAMES = {
+    1: "C1 plain FP32 air+gravity, 153x96 cells (612x384 canvas)",
+    2: "C2 plain FP32 air+gravity, 400x225 cells (1600x900 canvas)",
+    4: "C4 batched 256 instances, W,H log-uniform 32..512, FP32 air + FP32 gravity",
+    5: "C5 batched 64x(400x225) + 64 Pareto(1.5) instances, FP32 air + split-BF16 gravity",
+}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), d.get("bf16_tflops_sustained", 1400.0), "measured"
+    return 6650.0, 1590.0, 1400.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(cid: int):
+    import workloads as W
+
+    insts = W.config_instances(cid)
+    if cid == 5:
+        pass
+    return insts
+
+
+def dist_setup(gpus: int):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if gpus > 1 and world != gpus:
+        raise SystemExit(f"--gpus {gpus} needs torchrun with {gpus} ranks (WORLD_SIZE={world})")
+    if torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(v: float, world: int) -> float:
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------- CPU baseline --
+
+def cpu_rate(insts, target_s: float, threads: int | None = None):
+    """Oracle FP32 air + gravity on a bounded sample of `insts` (all host
+    threads); returns (cell-ticks/s, cores, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    if threads:
+        O.set_threads(threads)
+    cores = O.num_threads()
+    sample = insts[: max(1, min(len(insts), 8))]
+
+    def one_tick():
+        t0 = time.perf_counter()
+        for inst in sample:
+            O.air_steps(inst, 1)
+            if inst.config.newton_grav:
+                O.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx)
+        return time.perf_counter() - t0
+
+    t1 = one_tick()
+    ticks = max(1, min(200, int(target_s / max(t1, 1e-6))))
+    cur = [i.copy() for i in sample]
+    t0 = time.perf_counter()
+    for inst in cur:
+        st = O.air_steps(inst, ticks)
+        if inst.config.newton_grav:
+            for _ in range(ticks):
+                O.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx)
+    dt = time.perf_counter() - t0
+    cells = sum(i.cells for i in sample)
+    desc = f"{len(sample)} of {len(insts)} instances ({cells} cells) x {ticks} ticks, air + gravity solve per tick"
+    return cells * ticks / dt, cores, desc
+
+
+# ------------------------------------------------------------------ ours --
+
+def run_ours(args, rank, world, local):
+    import torch
+
+    import tpt_field as tf
+
+    tf.lib()
+    cid = args.workload
+    insts = workload(cid)
+    ticks = args.ticks or (1000 if cid in (4, 5) else (1000 if cid == 1 else 10000))
+    precision = tf.PRECISION_SPLIT_BF16 if cid == 5 else tf.PRECISION_FP32
+    stream = torch.cuda.current_stream()
+    batch = tf.Batch(insts, precision)
+    batch.tune()
+    cells = sum(i.cells for i in insts)
+
+    # device-timed: inputs resident
+    for _ in range(args.warmup):
+        batch.step(ticks)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.step(ticks)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(world)
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    value = cells * ticks * args.steps * world / (ms / 1e3)
+
+    # end to end through the C ABI with pinned host buffers
+    names = [n for n, _ in tf.Batch.GRIDS]
+    host_in = []
+    for inst in insts:
+        d = {}
+        for n, fid in tf.Batch.GRIDS:
+            a = getattr(inst, n)
+            t = torch.empty(a.size, dtype=torch.int32, pin_memory=True)
+            t.numpy().view(a.dtype)[:] = a
+            d[fid] = t.numpy().view(a.dtype)
+        host_in.append(d)
+    out_fields = [(tf.FIELD_PV, np.float32), (tf.FIELD_VX, np.float32), (tf.FIELD_VY, np.float32),
+                  (tf.FIELD_HV, np.float32), (tf.FIELD_GX, np.float32), (tf.FIELD_GY, np.float32)]
+    host_out = [{fid: torch.empty(i.cells, dtype=torch.float32, pin_memory=True).numpy() for fid, _ in out_fields}
+                for i in insts]
+    h2d = sum(a.nbytes for d in host_in for a in d.values())
+    d2h = sum(a.nbytes for d in host_out for a in d.values())
+
+    def e2e_step():
+        for i, d in enumerate(host_in):
+            for fid, a in d.items():
+                tf.check(tf.lib().tpt_batch_write(batch._h, i, fid, tf._ptr(a), a.nbytes, tf._stream(stream)))
+        batch.step(ticks, stream)
+        for i, d in enumerate(host_out):
+            for fid, a in d.items():
+                tf.check(tf.lib().tpt_batch_read(batch._h, i, fid, tf._ptr(a), a.nbytes, tf._stream(stream)))
+
+    e2e_steps = max(1, min(args.steps, 3))
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+    e2e_value = cells * ticks * e2e_steps * world / (e2e_ms / 1e3)
+
+    # per-phase device times for the roofline
+    prof = batch.profile_phases(200)
+    hbm, bf16, bf16s, peak_src = load_peaks()
+    air_gbs = prof.cells * prof.ticks * B_AIR / (prof.air_ms / 1e3) / 1e9
+    air_launch_ms = prof.air_ms / (prof.ticks * prof.air_launches_per_tick)
+    roof_air = {"kernel": "air tick (pressure+velocity, advection+heat+masks)", "bound": "hbm",
+                "achieved": round(air_gbs, 1), "peak": hbm, "unit": "GB/s", "frac": round(air_gbs / hbm, 4),
+                "peak_source": peak_src, "algorithmic_bytes_per_cell_tick": B_AIR,
+                "traffic": None, "ms_per_tick": round(prof.air_ms / prof.ticks, 5),
+                "avg_launch_ms": round(air_launch_ms, 5)}
+    phases = {"air_ms_per_tick": prof.air_ms / prof.ticks, "grav_ms_per_tick": prof.grav_ms / prof.ticks}
+    if precision == tf.PRECISION_SPLIT_BF16 and prof.grav_ms > 0:
+        tfl = prof.grav_flops_per_tick * prof.ticks / (prof.grav_ms / 1e3) / 1e12
+        roof_grav = {"kernel": "split-BF16 DFT-GEMM gravity", "bound": "tensor", "achieved": round(tfl, 2),
+                     "peak": bf16, "unit": "TFLOP/s", "frac": round(tfl / bf16, 4), "peak_source": peak_src,
+                     "traffic": None}
+    else:
+        roof_grav = None
+    dominant = roof_grav if (roof_grav and prof.grav_ms > prof.air_ms) else roof_air
+    launches = (prof.air_launches_per_tick + prof.grav_launches_per_tick) * ticks * args.steps + \
+        (args.steps if ticks % 2 else 0)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, desc = cpu_rate(insts, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "cell-ticks/s", "cores": cores, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": "cell-ticks/s", "value": value, "unit": "cell-ticks/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32" if precision == tf.PRECISION_FP32 else "f32 air + bf16x3 gravity (f32 accumulate)",
+            "data": "synthetic (seeded sandboxes, workloads.py)",
+            "config": {"workload": WORKLOAD_NAMES[cid], "instances": len(insts), "cells": cells,
+                       "ticks_per_step": ticks, "l2": "working set > 126 MB L2, no flush",
+                       "tuning": {"ctas_per_sm": batch.tuning().ctas_per_sm}},
+            "e2e": {"value": e2e_value, "unit": "cell-ticks/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "gpu_launches": launches,
+            "roofline": dominant,
+            "roofline_phases": {"air": roof_air, "gravity": roof_grav, **phases},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cid = args.workload
+    insts = workload(cid)
+    rate_samples = []
+    cores = desc = None
+    for _ in range(args.warmup + args.steps):
+        rate, cores, desc = cpu_rate(insts, args.cpu_seconds / max(args.steps, 1))
+        rate_samples.append(rate)
+    rates = rate_samples[args.warmup:]
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": "cell-ticks/s", "value": value, "unit": "cell-ticks/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sandboxes, workloads.py)",
+        "config": {"workload": WORKLOAD_NAMES[cid], "instances": len(insts)},
+        "cpu_baseline": {"value": value, "unit": "cell-ticks/s", "cores": cores, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": "cell-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", type=int, choices=(1, 2, 4, 5), default=4)
+    ap.add_argument("--ticks", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        run_reference(args, rank, world)
+        return
+    rank, world, local = dist_setup(args.gpus)
+    try:
+        run_ours(args, rank, world, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,304 @@
+/*
+ * tpt_field.h -- C ABI of the B200 coarse-grid field step of tpt-sim.
+ *
+ * The field step is the per-tick work tpt-sim does on the 4x4-pixel cell grid
+ * (`xcells x ycells`, row-major `cy * xcells + cx`):
+ *
+ *   - the Eulerian air solver (pressure `pv`, velocity `vx`/`vy`, ambient heat
+ *     `hv`, wall masks), replacing `step_air_gpu`
+ *     (crates/tpt-sim/src/air_kernel/mod.rs:120);
+ *   - the FFT Newtonian gravity solve (cell mass map -> `gx`/`gy`), replacing
+ *     `GravityFft::solve` (crates/tpt-sim/src/gravity_gpu/mod.rs:114) as called
+ *     by `step_gravity_gpu` (crates/tpt-sim/src/gravity_kernel.rs:920).
+ *
+ * Conventions shared by every entry point:
+ *   - the return value is a status code: TPT_OK (0) or a negative TPT_ERR_*;
+ *     `tpt_last_error_string()` describes the last failure of the calling
+ *     thread. Nothing aborts and no C++ exception crosses the ABI.
+ *   - every buffer argument is a DEVICE pointer unless its name ends in
+ *     `_host`. Grids are `xcells * ycells` elements in the reference layout.
+ *   - work is stream ordered on the `tpt_stream_t` given (a `cudaStream_t`;
+ *     NULL = the legacy default stream). Nothing synchronises the host.
+ *   - the caller owns the field buffers; a plan or a batch owns its scratch.
+ *   - a plan or batch is used from one host thread / one stream at a time.
+ */
+#ifndef TPT_FIELD_H
+#define TPT_FIELD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same object as `cudaStream_t`, declared without the CUDA headers. */
+typedef struct CUstream_st *tpt_stream_t;
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    TPT_OK = 0,
+    TPT_ERR_INVALID_DIMS = -1,   /* zero, too small or too large grid      */
+    TPT_ERR_NULL_POINTER = -2,   /* a required pointer is NULL             */
+    TPT_ERR_CUDA = -3,           /* a CUDA runtime/driver call failed      */
+    TPT_ERR_DEVICE_TIMEOUT = -4, /* a bounded device-side wait gave up     */
+    TPT_ERR_INVALID_ARG = -5,    /* enum value or size out of range        */
+    TPT_ERR_OUT_OF_MEMORY = -6,  /* device allocation failed               */
+    TPT_ERR_UNSUPPORTED = -7     /* no sm_100 device / feature missing     */
+};
+
+/* ---- enums mirroring tpt-core (crates/tpt-core/src/particle.rs:136-165) - */
+enum { /* AirMode */
+    TPT_AIR_ON = 0,
+    TPT_AIR_PRESSURE_OFF = 1,
+    TPT_AIR_VELOCITY_OFF = 2,
+    TPT_AIR_OFF = 3,
+    TPT_AIR_NO_UPDATE = 4
+};
+enum { /* GravityMode (the configured direction, not the Newtonian field) */
+    TPT_GRAVITY_VERTICAL = 0,
+    TPT_GRAVITY_OFF = 1,
+    TPT_GRAVITY_RADIAL = 2,
+    TPT_GRAVITY_CUSTOM = 3
+};
+enum { /* AIRC_* convection modes */
+    TPT_AIRC_NONE = 0,
+    TPT_AIRC_LEGACY = 1,
+    TPT_AIRC_BOUSSINESQ = 2
+};
+enum { /* arithmetic of the gravity solve */
+    TPT_PRECISION_FP32 = 0,      /* FP32 FFT convolution                    */
+    TPT_PRECISION_SPLIT_BF16 = 1 /* DFT-as-GEMM on tcgen05, 3-term bf16 split,
+                                    FP32 accumulate                          */
+};
+
+/* Wall ids the field step reads (crates/tpt-core/src/constants.rs:700-735). */
+enum {
+    TPT_WL_WALLELEC = 1,
+    TPT_WL_EWALL = 2,
+    TPT_WL_FAN = 5,
+    TPT_WL_WALL = 8,
+    TPT_WL_GRAV = 14,
+    TPT_WL_BLOCKAIR = 16
+};
+
+/* Largest grid side the entry points accept (a 8192-px canvas). */
+#define TPT_MAX_CELLS_PER_SIDE 2048u
+
+/* ---- air step ---------------------------------------------------------- */
+
+/*
+ * The `SimulationConfig` fields `step_air_gpu` reads
+ * (crates/tpt-sim/src/air_kernel/mod.rs:121-141), with the reference defaults
+ * listed in `tpt_air_params_default`.
+ */
+typedef struct tpt_air_params {
+    uint32_t xcells, ycells;
+    uint32_t air_mode;        /* TPT_AIR_*                                  */
+    uint32_t aheat_enable;    /* 0/1: run the ambient-heat pass             */
+    uint32_t convection_mode; /* TPT_AIRC_*                                 */
+    uint32_t gravity_mode;    /* TPT_GRAVITY_*                              */
+    float edge_pressure;
+    float edge_vx, edge_vy;
+    float ambient_air_temp; /* Kelvin                                      */
+    float vorticity_coeff;
+    float custom_gx, custom_gy;
+} tpt_air_params;
+
+/*
+ * Device buffers of one air grid, the `SimBuffers` handles of the reference
+ * (crates/tpt-sim/src/buffers/mod.rs:186-230). `opv/ovx/ovy/ohv` are the
+ * reference's scratch grids and are overwritten. `pmap`/`elem_props` feed the
+ * particle HotAir -> pressure pass (crates/tpt-sim/src/air_kernel/settle.rs:
+ * 118-161); pass pmap = NULL to skip it.
+ */
+typedef struct tpt_air_bufs {
+    float *pv, *vx, *vy, *hv;       /* state, read and written            */
+    float *opv, *ovx, *ovy, *ohv;   /* scratch                            */
+    uint32_t *block_air;            /* rebuilt at the end of the step     */
+    uint32_t *block_airh;           /* rebuilt at the end of the step     */
+    const uint32_t *wall_bmap;      /* wall id in the low byte            */
+    uint32_t *wall_emap;            /* decremented once per step if > 0   */
+    const uint32_t *elem_block_air; /* element stamps OR-ed into the masks */
+    const uint32_t *elem_block_airh;
+    const float *fan_vx, *fan_vy;   /* added where wall_bmap == WL_FAN    */
+    /* optional HotAir pass */
+    const uint32_t *pmap;       /* xres*yres packed words, type in bits 0..8 */
+    const uint32_t *elem_props; /* n_elements rows of 32 words; word 11 is
+                                   the f32 bit pattern of `hot_air`          */
+    uint32_t xres, yres, n_elements;
+} tpt_air_bufs;
+
+/* Fills `p` with the reference defaults (crates/tpt-core/src/particle.rs:
+ * 290-345) for an `xcells x ycells` grid. */
+void tpt_air_params_default(tpt_air_params *p, uint32_t xcells, uint32_t ycells);
+
+/*
+ * One air step, replacing `step_air_gpu(&mut SimBuffers)`
+ * (crates/tpt-sim/src/air_kernel/mod.rs:120-299): pressure, velocity,
+ * smoothing/advection/vorticity/fans, then (if aheat_enable) ambient heat and
+ * convection, the wall-mask rebuild and (if pmap) HotAir. xcells or ycells of
+ * 0 returns TPT_OK without work, as the reference does (mod.rs:124-126).
+ */
+int tpt_air_step(const tpt_air_params *params, const tpt_air_bufs *bufs,
+                 tpt_stream_t stream);
+
+/* Host twin of the wall-mask rebuild (crates/tpt-sim/src/buffers/spatial.rs:
+ * 336-352): block masks from wall ids and emap, no element stamps. */
+int tpt_wall_masks_host(const uint32_t *wall_bmap_host,
+                        const uint32_t *wall_emap_host,
+                        uint32_t *block_air_host, uint32_t *block_airh_host,
+                        size_t cells);
+
+/* ---- gravity ----------------------------------------------------------- */
+
+typedef struct tpt_grav_plan tpt_grav_plan;
+
+/*
+ * Plan for one grid size, replacing `FftBuffers::allocate` + `build_kernels`
+ * (crates/tpt-sim/src/gravity_gpu/mod.rs:140-200). The kernel spectra are
+ * built on the device in FP64 once, then rounded to the plan's precision.
+ * The plan owns all of its scratch. Calls cudaMalloc; synchronises the
+ * current device once at the end of creation.
+ */
+int tpt_grav_plan_create(uint32_t xcells, uint32_t ycells, int precision,
+                         tpt_grav_plan **out);
+int tpt_grav_plan_destroy(tpt_grav_plan *plan);
+/* Padded transform size the plan uses (for reporting). */
+int tpt_grav_plan_dims(const tpt_grav_plan *plan, uint32_t *n1, uint32_t *n2);
+
+/*
+ * One gravity solve, replacing `GravityFft::solve(bufs, mass, 1/65536)`
+ * (crates/tpt-sim/src/gravity_gpu/mod.rs:114-135, 204-278):
+ *   gx/gy[p] = mask[p] ? sum_m mask[m] * mass[m] * mass_scale_inv *
+ *                        (-M_GRAV) * (p - m) / |p - m|^3 : 0
+ * `mass_fx` is the fixed-point accumulator (mass * 65536 as i32).
+ */
+int tpt_grav_solve(tpt_grav_plan *plan, const int32_t *mass_fx,
+                   float mass_scale_inv, const uint32_t *mask, float *gx,
+                   float *gy, tpt_stream_t stream);
+/* Same solve with an f32 mass grid (no fixed point). */
+int tpt_grav_solve_f32(tpt_grav_plan *plan, const float *mass,
+                       const uint32_t *mask, float *gx, float *gy,
+                       tpt_stream_t stream);
+
+/*
+ * Host gravity-mask flood fill, replacing `rebuild_gravity_mask`
+ * (crates/tpt-sim/src/gravity_kernel.rs:658-712): cells 4-connected to the
+ * border through non-WL_GRAV cells get 0xFFFFFFFF, the rest 0.
+ */
+int tpt_grav_mask_rebuild(const uint32_t *wall_bmap_host, uint32_t *mask_host,
+                          uint32_t xcells, uint32_t ycells);
+
+/* Fixed-point mass of `m` (crates/tpt-sim/src/gravity_kernel.rs:217-229):
+ * round half away from zero of m * 65536 in f32 arithmetic. */
+int32_t tpt_mass_to_fixed(float m);
+
+/* ---- batched instances ------------------------------------------------- */
+
+typedef struct tpt_batch tpt_batch;
+
+/* One independent sandbox instance of a batch. */
+typedef struct tpt_instance_desc {
+    tpt_air_params air; /* grid size and air config of the instance     */
+    uint32_t newton_grav; /* 0/1: solve gravity every tick (config flag) */
+} tpt_instance_desc;
+
+/* Device pointers of one instance's grids inside a batch's arenas. The
+ * layout of each grid is the reference's (`cy * xcells + cx`), so any
+ * reference-layout kernel can read or edit them between steps. */
+typedef struct tpt_instance_fields {
+    float *pv, *vx, *vy, *hv;
+    uint32_t *block_air, *block_airh, *wall_bmap, *wall_emap;
+    uint32_t *elem_block_air, *elem_block_airh;
+    float *fan_vx, *fan_vy;
+    int32_t *grav_mass;  /* fixed-point mass the solve reads            */
+    uint32_t *grav_mask; /* gravity propagation mask                     */
+    float *gx, *gy;      /* solve output                                 */
+} tpt_instance_fields;
+
+/* Grid ids for tpt_batch_write / tpt_batch_read. */
+enum {
+    TPT_FIELD_PV = 0, TPT_FIELD_VX, TPT_FIELD_VY, TPT_FIELD_HV,
+    TPT_FIELD_BLOCK_AIR, TPT_FIELD_BLOCK_AIRH, TPT_FIELD_WALL_BMAP,
+    TPT_FIELD_WALL_EMAP, TPT_FIELD_ELEM_BLOCK_AIR, TPT_FIELD_ELEM_BLOCK_AIRH,
+    TPT_FIELD_FAN_VX, TPT_FIELD_FAN_VY, TPT_FIELD_GRAV_MASS,
+    TPT_FIELD_GRAV_MASK, TPT_FIELD_GX, TPT_FIELD_GY,
+    TPT_FIELD_COUNT
+};
+
+/*
+ * Host <-> device copy of one grid of one instance (`bytes` must equal
+ * xcells*ycells*4), the batch counterpart of the reference's
+ * `client.write` / `client.read` on a SimBuffers handle
+ * (crates/tpt-sim/src/buffers/gpu_sync.rs:186-197, 375-396). Stream ordered
+ * (cudaMemcpyAsync); synchronise the stream before touching `host` again.
+ */
+int tpt_batch_write(tpt_batch *batch, uint32_t instance, int field,
+                    const void *host, size_t bytes, tpt_stream_t stream);
+int tpt_batch_read(tpt_batch *batch, uint32_t instance, int field,
+                   void *host, size_t bytes, tpt_stream_t stream);
+
+/* Tuning knobs the autotuner picks (and a caller may pin). */
+typedef struct tpt_batch_tuning {
+    uint32_t tile_x, tile_y;  /* air tile shape in cells                  */
+    uint32_t temporal_depth;  /* ticks per air launch (1 = no blocking)   */
+    uint32_t ctas_per_sm;     /* persistent grid size multiplier          */
+} tpt_batch_tuning;
+
+/*
+ * Creates a batch of `n` instances with grids allocated in packed device
+ * arenas (zero-initialised), and gravity plans of `grav_precision`.
+ */
+int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs,
+                     int grav_precision, tpt_batch **out);
+int tpt_batch_destroy(tpt_batch *batch);
+int tpt_batch_fields(tpt_batch *batch, uint32_t instance,
+                     tpt_instance_fields *out);
+/*
+ * Advances every instance by `ticks` field steps (air, then gravity if
+ * newton_grav), the same result as calling tpt_air_step and tpt_grav_solve
+ * once per tick per instance. Uses a CUDA graph per (ticks, stream) that is
+ * captured on first use and replayed after.
+ */
+int tpt_batch_step(tpt_batch *batch, uint32_t ticks, tpt_stream_t stream);
+/* Times candidate tunings on the batch's own data (state is saved and
+ * restored) and keeps the fastest. Synchronous. */
+int tpt_batch_tune(tpt_batch *batch, tpt_stream_t stream);
+int tpt_batch_get_tuning(const tpt_batch *batch, tpt_batch_tuning *out);
+int tpt_batch_set_tuning(tpt_batch *batch, const tpt_batch_tuning *tuning);
+
+/* Device time of the two phases of a batch step, measured separately. */
+typedef struct tpt_batch_profile {
+    float air_ms;              /* `ticks` air ticks alone (all instances)  */
+    float grav_ms;             /* `ticks` gravity solves alone             */
+    uint32_t ticks;
+    uint32_t air_launches_per_tick;
+    uint32_t grav_launches_per_tick;
+    uint64_t cells;            /* sum of xcells*ycells over instances      */
+    uint64_t grav_cells;       /* same, over instances with newton_grav    */
+    double grav_flops_per_tick;/* executed flops of one tick's solves      */
+} tpt_batch_profile;
+
+/*
+ * Times `ticks` air ticks and `ticks` gravity solves of the batch as two
+ * separate chains on `stream` (CUDA events on that stream), restoring the
+ * batch state afterwards. Synchronous. For roofline reporting.
+ */
+int tpt_batch_profile_phases(tpt_batch *batch, uint32_t ticks,
+                             tpt_stream_t stream, tpt_batch_profile *out);
+
+/* ---- diagnostics ------------------------------------------------------- */
+
+/* Message of the last failure on the calling thread ("" if none). */
+const char *tpt_last_error_string(void);
+/* Number of kernel launches this library has issued (all threads). */
+uint64_t tpt_kernel_launch_count(void);
+/* Library version string. */
+const char *tpt_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TPT_FIELD_H */

@@ -1,0 +1,183 @@
+"""ctypes wrapper of the CPU oracle (liboracle.so). TEST INFRASTRUCTURE ONLY:
+used by tests/, the smoke check and bench.py's CPU-baseline leg as the
+checker; the product never imports it.
+
+The oracle restates the reference's field-step kernels (air:
+crates/tpt-sim/src/air_kernel/*.rs, gravity: crates/tpt-sim/src/gravity_gpu/
+*.rs) in an FP32 mirror and an FP64 twin; see tpt_oracle.cpp.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+
+class AirParams(ctypes.Structure):
+    """Same layout as `tpt_air_params` in include/tpt_field.h."""
+
+    _fields_ = [
+        ("xcells", ctypes.c_uint32), ("ycells", ctypes.c_uint32),
+        ("air_mode", ctypes.c_uint32), ("aheat_enable", ctypes.c_uint32),
+        ("convection_mode", ctypes.c_uint32), ("gravity_mode", ctypes.c_uint32),
+        ("edge_pressure", ctypes.c_float), ("edge_vx", ctypes.c_float), ("edge_vy", ctypes.c_float),
+        ("ambient_air_temp", ctypes.c_float), ("vorticity_coeff", ctypes.c_float),
+        ("custom_gx", ctypes.c_float), ("custom_gy", ctypes.c_float),
+    ]
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        u32, f32, i32 = ctypes.c_uint32, ctypes.c_float, ctypes.c_int
+        _lib.ora_air_steps_f32.argtypes = [ctypes.POINTER(AirParams), i32] + [P] * 12 + [P, P, u32, u32, u32]
+        _lib.ora_air_steps_f64.argtypes = _lib.ora_air_steps_f32.argtypes
+        _lib.ora_grav_solve_f32.argtypes = [u32, u32, P, P, f32, P, P, P]
+        _lib.ora_grav_solve_f64.argtypes = [u32, u32, P, P, f32, P, P, P]
+        _lib.ora_grav_direct_f64.argtypes = [u32, u32, P, P, f32, P, P, P]
+        _lib.ora_fft_host_f32.argtypes = [P, u32, u32, u32, u32, u32, f32]
+        _lib.ora_bit_count.argtypes = [u32]
+        _lib.ora_bit_count.restype = u32
+        _lib.ora_twiddle_f32.argtypes = [u32, P, P]
+        _lib.ora_grav_mask.argtypes = [P, P, u32, u32]
+        _lib.ora_mass_to_fixed.argtypes = [f32]
+        _lib.ora_mass_to_fixed.restype = ctypes.c_int32
+        _lib.ora_block_masks.argtypes = [ctypes.c_size_t, P, P, P, P, P, P]
+        _lib.ora_tool_gravity_mass.argtypes = [f32, i32]
+        _lib.ora_tool_gravity_mass.restype = f32
+        _lib.ora_gravity_tool_cell.argtypes = [ctypes.c_int32] * 6
+        _lib.ora_gravity_tool_cell.restype = ctypes.c_int64
+        _lib.ora_align_dim.argtypes = [u32]
+        _lib.ora_align_dim.restype = u32
+        _lib.ora_set_threads.argtypes = [i32]
+        _lib.ora_num_threads.restype = i32
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def params_of(inst) -> AirParams:
+    c = inst.config
+    return AirParams(inst.xcells, inst.ycells, c.air_mode, c.aheat_enable, c.convection_mode, c.gravity_mode,
+                     c.edge_pressure, c.edge_vx, c.edge_vy, c.ambient_air_temp, c.vorticity_coeff,
+                     c.custom_gx, c.custom_gy)
+
+
+def set_threads(n: int) -> None:
+    lib().ora_set_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(lib().ora_num_threads())
+
+
+def air_steps(inst, ticks: int, dtype=np.float32, pmap=None, props=None, xres=0, yres=0):
+    """Runs `ticks` air steps on a copy of `inst`'s state; returns the new
+    state dict (pv, vx, vy, hv in `dtype`; emap, bair, bairh as u32)."""
+    L = lib()
+    f = L.ora_air_steps_f32 if dtype == np.float32 else L.ora_air_steps_f64
+    st = {k: getattr(inst, k).astype(dtype).copy() for k in ("pv", "vx", "vy", "hv", "fan_vx", "fan_vy")}
+    for k in ("wall", "emap", "bair", "bairh", "eair", "eairh"):
+        st[k] = getattr(inst, k).astype(np.uint32).copy()
+    prm = params_of(inst)
+    nprops = 0 if props is None else len(props) // 32
+    rc = f(ctypes.byref(prm), int(ticks), _p(st["pv"]), _p(st["vx"]), _p(st["vy"]), _p(st["hv"]),
+           _p(st["wall"]), _p(st["emap"]), _p(st["bair"]), _p(st["bairh"]), _p(st["eair"]), _p(st["eairh"]),
+           _p(st["fan_vx"]), _p(st["fan_vy"]), _p(pmap), _p(props), nprops, xres, yres)
+    assert rc == 0
+    return st
+
+
+def grav_solve(X, Y, mask, mass_fx=None, mass_f32=None, mass_scale_inv=1.0 / 65536.0, dtype=np.float32,
+               direct=False):
+    """FP32 mirror (dtype f32), FP64 FFT twin (f64) or FP64 direct sum
+    (direct=True) of the gravity solve; returns (gx, gy)."""
+    L = lib()
+    n = X * Y
+    if direct:
+        dtype = np.float64
+    gx = np.zeros(n, dtype)
+    gy = np.zeros(n, dtype)
+    mi = None if mass_fx is None else np.ascontiguousarray(mass_fx, np.int32)
+    mf = None if mass_f32 is None else np.ascontiguousarray(mass_f32, np.float32)
+    mk = np.ascontiguousarray(mask, np.uint32)
+    if direct:
+        fn = L.ora_grav_direct_f64
+    else:
+        fn = L.ora_grav_solve_f32 if dtype == np.float32 else L.ora_grav_solve_f64
+    rc = fn(X, Y, _p(mi), _p(mf), float(mass_scale_inv), _p(mk), _p(gx), _p(gy))
+    assert rc == 0
+    return gx, gy
+
+
+def fft_host(data: np.ndarray, rows, n, inner, stride, tw_bits, sign):
+    """In-place host mirror of the reference's bitrev + stage kernels on an
+    interleaved complex f32 buffer (crates/tpt-sim/src/gravity_gpu/fft.rs:274)."""
+    assert data.dtype == np.float32 and data.flags.c_contiguous
+    lib().ora_fft_host_f32(_p(data), rows, n, inner, stride, tw_bits, float(sign))
+
+
+def bit_count(n: int) -> int:
+    return int(lib().ora_bit_count(n))
+
+
+def twiddle(max_len: int):
+    half = max(max_len // 2, 1)
+    re = np.zeros(half, np.float32)
+    im = np.zeros(half, np.float32)
+    lib().ora_twiddle_f32(max_len, _p(re), _p(im))
+    return re, im
+
+
+def grav_mask(wall: np.ndarray, X: int, Y: int) -> np.ndarray:
+    out = np.zeros(X * Y, np.uint32)
+    w = np.ascontiguousarray(wall, np.uint32)
+    lib().ora_grav_mask(_p(w), _p(out), X, Y)
+    return out
+
+
+def mass_to_fixed(m: float) -> int:
+    return int(lib().ora_mass_to_fixed(float(m)))
+
+
+def block_masks(wall, emap, eair=None, eairh=None):
+    n = len(wall)
+    w = np.ascontiguousarray(wall, np.uint32)
+    e = np.ascontiguousarray(emap, np.uint32).copy()
+    ba = np.zeros(n, np.uint32)
+    bh = np.zeros(n, np.uint32)
+    ea = None if eair is None else np.ascontiguousarray(eair, np.uint32)
+    eh = None if eairh is None else np.ascontiguousarray(eairh, np.uint32)
+    lib().ora_block_masks(n, _p(w), _p(e), _p(ba), _p(bh), _p(ea), _p(eh))
+    return e, ba, bh
+
+
+def tool_gravity_mass(strength: float, attract: bool) -> float:
+    return float(lib().ora_tool_gravity_mass(float(strength), int(attract)))
+
+
+def gravity_tool_cell(x, y, xres, yres, xcells, ycells):
+    r = int(lib().ora_gravity_tool_cell(x, y, xres, yres, xcells, ycells))
+    return None if r < 0 else r
+
+
+def align_dim(v: int) -> int:
+    return int(lib().ora_align_dim(v))

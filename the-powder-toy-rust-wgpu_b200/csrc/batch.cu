@@ -1,0 +1,502 @@
+// batch.cu -- many independent sandbox instances stepped together.
+//
+// Layout: every grid of every instance lives in one of three packed device
+// arenas (f32, u32, i32); each instance's grid is contiguous in the
+// reference layout (`cy * xcells + cx`) and starts on a 256-byte boundary.
+// Ambient heat and the two wall masks have a second copy (ping-pong), so a
+// tick is two air launches over a tile list of all instances (no settle
+// pass); after an odd tick count one copy-back restores the canonical
+// buffers. Gravity (instances with newton_grav) is independent of air in
+// the field step (crates/tpt-sim/src/air_kernel/heat.rs:182-203 uses the
+// configured direction, not the Newtonian field), so it runs on a second
+// stream branch of the captured graph, concurrently with the air chain.
+//
+// N ticks are captured once into a CUDA graph (in chunks of CHUNK ticks so
+// instantiation stays cheap) and replayed on later calls.
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <vector>
+
+#include "air_launch.hpp"
+#include "grav_dft.hpp"
+#include "grav_plan.hpp"
+
+namespace tpt {
+AirInst make_air_inst(const tpt_air_params &p);
+}
+
+using namespace tpt;
+
+namespace {
+constexpr uint32_t CHUNK = 50;  // ticks per captured graph (even)
+constexpr size_t ALIGN = 64;    // elements (256 B)
+
+enum F32 { F_PV, F_VX, F_VY, F_HV, F_HV2, F_OPV, F_OVX, F_OVY, F_FVX, F_FVY, F_GX, F_GY, F_N32 };
+enum U32 { U_BA, U_BH, U_BA2, U_BH2, U_WALL, U_EMAP, U_EA, U_EH, U_GMASK, U_NU32 };
+
+size_t round_up(size_t v) { return (v + ALIGN - 1) / ALIGN * ALIGN; }
+}  // namespace
+
+struct tpt_batch {
+    uint32_t n = 0;
+    int precision = TPT_PRECISION_FP32;
+    std::vector<tpt_instance_desc> descs;
+    std::vector<size_t> off;  // per-instance element offset (same in all arenas)
+    size_t stride = 0;        // elements per grid slot of the arenas
+    float *f32 = nullptr;
+    uint32_t *u32 = nullptr;
+    int32_t *i32 = nullptr;
+    std::vector<AirInst> insts_host;
+    AirInst *insts = nullptr;
+    air::TileRef *tiles = nullptr;
+    uint32_t ntiles = 0;
+    bool any_noupdate_heat = false;
+    bool any_grav = false;
+    tpt_batch_tuning tuning{AIR_TX, AIR_TY, 1, 4};
+    int sms = 148;
+    gfft::FftSet fft;
+    dft::DftSet dft;
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+    std::map<uint32_t, cudaGraphExec_t> graphs;
+
+    float *f(int field, uint32_t i) const { return f32 + (size_t)field * stride + off[i]; }
+    uint32_t *u(int field, uint32_t i) const { return u32 + (size_t)field * stride + off[i]; }
+    uint32_t grid() const { return std::min<uint32_t>(ntiles, (uint32_t)sms * std::max<uint32_t>(tuning.ctas_per_sm, 1)); }
+
+    void drop_graphs() {
+        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+    }
+    ~tpt_batch() {
+        drop_graphs();
+        cudaFree(f32);
+        cudaFree(u32);
+        cudaFree(i32);
+        cudaFree(insts);
+        cudaFree(tiles);
+        if (side) cudaStreamDestroy(side);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+    }
+};
+
+// Records `ticks` field steps on `st` (no graph): air chain on st, gravity
+// chain on the side stream, joined at the end.
+static int record_ticks(tpt_batch *b, uint32_t ticks, cudaStream_t st) {
+    int rc;
+    if (b->any_grav) {
+        TPT_CUDA(cudaEventRecord(b->fork, st));
+        TPT_CUDA(cudaStreamWaitEvent(b->side, b->fork, 0));
+        for (uint32_t t = 0; t < ticks; ++t) {
+            rc = b->precision == TPT_PRECISION_FP32 ? b->fft.launch(b->side) : b->dft.launch(b->side);
+            if (rc) return rc;
+        }
+    }
+    for (uint32_t t = 0; t < ticks; ++t) {
+        rc = air::launch_batch_tick(b->insts, b->tiles, b->ntiles, b->grid(), t & 1u, b->any_noupdate_heat, st);
+        if (rc) return rc;
+    }
+    if (ticks & 1u) {
+        rc = air::launch_copy_back(b->insts, b->tiles, b->ntiles, b->grid(), st);
+        if (rc) return rc;
+    }
+    if (b->any_grav) {
+        TPT_CUDA(cudaEventRecord(b->join, b->side));
+        TPT_CUDA(cudaStreamWaitEvent(st, b->join, 0));
+    }
+    return TPT_OK;
+}
+
+static int graph_for(tpt_batch *b, uint32_t ticks, cudaGraphExec_t *out) {
+    auto it = b->graphs.find(ticks);
+    if (it != b->graphs.end()) {
+        *out = it->second;
+        return TPT_OK;
+    }
+    cudaStream_t cap;
+    TPT_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+    int rc = TPT_OK;
+    if (e == cudaSuccess) {
+        rc = record_ticks(b, ticks, cap);
+        cudaError_t e2 = cudaStreamEndCapture(cap, &g);
+        if (rc == TPT_OK && e2 != cudaSuccess) e = e2;
+    }
+    cudaStreamDestroy(cap);
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        TPT_FAIL(TPT_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    }
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) TPT_FAIL(TPT_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    b->graphs[ticks] = ex;
+    *out = ex;
+    return TPT_OK;
+}
+
+static int field_ptr(tpt_batch *b, uint32_t i, int field, void **p) {
+    switch (field) {
+        case TPT_FIELD_PV: *p = b->f(F_PV, i); break;
+        case TPT_FIELD_VX: *p = b->f(F_VX, i); break;
+        case TPT_FIELD_VY: *p = b->f(F_VY, i); break;
+        case TPT_FIELD_HV: *p = b->f(F_HV, i); break;
+        case TPT_FIELD_BLOCK_AIR: *p = b->u(U_BA, i); break;
+        case TPT_FIELD_BLOCK_AIRH: *p = b->u(U_BH, i); break;
+        case TPT_FIELD_WALL_BMAP: *p = b->u(U_WALL, i); break;
+        case TPT_FIELD_WALL_EMAP: *p = b->u(U_EMAP, i); break;
+        case TPT_FIELD_ELEM_BLOCK_AIR: *p = b->u(U_EA, i); break;
+        case TPT_FIELD_ELEM_BLOCK_AIRH: *p = b->u(U_EH, i); break;
+        case TPT_FIELD_FAN_VX: *p = b->f(F_FVX, i); break;
+        case TPT_FIELD_FAN_VY: *p = b->f(F_FVY, i); break;
+        case TPT_FIELD_GRAV_MASS: *p = b->i32 + b->off[i]; break;
+        case TPT_FIELD_GRAV_MASK: *p = b->u(U_GMASK, i); break;
+        case TPT_FIELD_GX: *p = b->f(F_GX, i); break;
+        case TPT_FIELD_GY: *p = b->f(F_GY, i); break;
+        default: TPT_FAIL(TPT_ERR_INVALID_ARG, "unknown field id %d", field);
+    }
+    return TPT_OK;
+}
+
+extern "C" {
+
+int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, tpt_batch **out) {
+    if (!out) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_create: out is NULL");
+    *out = nullptr;
+    if (n == 0) TPT_FAIL(TPT_ERR_INVALID_DIMS, "tpt_batch_create: no instances");
+    if (!descs) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_create: descs is NULL");
+    if (precision != TPT_PRECISION_FP32 && precision != TPT_PRECISION_SPLIT_BF16)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "unknown precision %d", precision);
+    for (uint32_t i = 0; i < n; ++i) {
+        const tpt_air_params &p = descs[i].air;
+        if (p.xcells < 3 || p.ycells < 3 || p.xcells > TPT_MAX_CELLS_PER_SIDE || p.ycells > TPT_MAX_CELLS_PER_SIDE)
+            TPT_FAIL(TPT_ERR_INVALID_DIMS, "instance %u: grid %ux%u outside 3..%u", i, p.xcells, p.ycells,
+                     TPT_MAX_CELLS_PER_SIDE);
+        if (p.air_mode > 4u || p.convection_mode > 2u || p.gravity_mode > 3u || p.aheat_enable > 1u)
+            TPT_FAIL(TPT_ERR_INVALID_ARG, "instance %u: enum field out of range", i);
+    }
+    int rc = require_sm100();
+    if (rc) return rc;
+    tpt_batch *b = new (std::nothrow) tpt_batch();
+    if (!b) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "host allocation failed");
+    auto bail = [&](int code) {
+        delete b;
+        return code;
+    };
+    b->n = n;
+    b->precision = precision;
+    b->descs.assign(descs, descs + n);
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+    size_t total = 0;
+    b->off.resize(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        b->off[i] = total;
+        total += round_up((size_t)descs[i].air.xcells * descs[i].air.ycells);
+    }
+    b->stride = total;
+    cudaError_t e = cudaMalloc(&b->f32, total * F_N32 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&b->u32, total * U_NU32 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b->i32, total * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(b->f32, 0, total * F_N32 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(b->u32, 0, total * U_NU32 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(b->i32, 0, total * sizeof(int32_t));
+    if (e != cudaSuccess) {
+        set_error("batch arena allocation (%zu cells) failed: %s", total, cudaGetErrorString(e));
+        return bail(e == cudaErrorMemoryAllocation ? TPT_ERR_OUT_OF_MEMORY : TPT_ERR_CUDA);
+    }
+    // two AirInst per instance: parity 0 reads canonical hv/masks and writes
+    // the second copies; parity 1 the reverse.
+    std::vector<air::TileRef> tiles;
+    b->insts_host.resize(2 * (size_t)n);
+    std::vector<JobShape> gshapes;
+    std::vector<uint32_t> gidx;
+    for (uint32_t i = 0; i < n; ++i) {
+        const tpt_air_params &p = descs[i].air;
+        AirInst I = make_air_inst(p);
+        I.pv = b->f(F_PV, i);
+        I.vx = b->f(F_VX, i);
+        I.vy = b->f(F_VY, i);
+        I.opv = b->f(F_OPV, i);
+        I.ovx = b->f(F_OVX, i);
+        I.ovy = b->f(F_OVY, i);
+        I.ohv = nullptr;
+        I.wall = b->u(U_WALL, i);
+        I.emap = b->u(U_EMAP, i);
+        I.eair = b->u(U_EA, i);
+        I.eairh = b->u(U_EH, i);
+        I.fvx = b->f(F_FVX, i);
+        I.fvy = b->f(F_FVY, i);
+        for (int par = 0; par < 2; ++par) {
+            AirInst J = I;
+            if (p.aheat_enable) {
+                J.hv = b->f(par ? F_HV2 : F_HV, i);
+                J.hv_out = b->f(par ? F_HV : F_HV2, i);
+            } else {  // heat never changes: one buffer for both halves
+                J.hv = J.hv_out = b->f(F_HV, i);
+            }
+            J.bair = b->u(par ? U_BA2 : U_BA, i);
+            J.bairh = b->u(par ? U_BH2 : U_BH, i);
+            J.bair_out = b->u(par ? U_BA : U_BA2, i);
+            J.bairh_out = b->u(par ? U_BH : U_BH2, i);
+            b->insts_host[2 * (size_t)i + par] = J;
+        }
+        if (p.air_mode == 4u && p.aheat_enable) b->any_noupdate_heat = true;
+        for (uint32_t ty = 0; ty * AIR_TY < p.ycells; ++ty)
+            for (uint32_t tx = 0; tx * AIR_TX < p.xcells; ++tx) tiles.push_back({i, (uint16_t)tx, (uint16_t)ty});
+        if (descs[i].newton_grav) {
+            gshapes.push_back({p.xcells, p.ycells});
+            gidx.push_back(i);
+        }
+    }
+    b->ntiles = (uint32_t)tiles.size();
+    e = cudaMalloc(&b->insts, b->insts_host.size() * sizeof(AirInst));
+    if (e == cudaSuccess) e = cudaMalloc(&b->tiles, tiles.size() * sizeof(air::TileRef));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->insts, b->insts_host.data(), b->insts_host.size() * sizeof(AirInst), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->tiles, tiles.data(), tiles.size() * sizeof(air::TileRef), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        set_error("batch setup failed: %s", cudaGetErrorString(e));
+        return bail(TPT_ERR_CUDA);
+    }
+    b->any_grav = !gshapes.empty();
+    if (b->any_grav) {
+        if (precision == TPT_PRECISION_FP32) {
+            rc = b->fft.create(gshapes);
+            if (rc) return bail(rc);
+            for (size_t j = 0; j < gidx.size(); ++j) {
+                uint32_t i = gidx[j];
+                b->fft.set_io(j, b->i32 + b->off[i], nullptr, 1.0f / 65536.0f, b->u(U_GMASK, i), b->f(F_GX, i),
+                              b->f(F_GY, i));
+            }
+            rc = b->fft.upload_jobs();
+        } else {
+            rc = b->dft.create(gshapes);
+            for (size_t j = 0; rc == TPT_OK && j < gidx.size(); ++j) {
+                uint32_t i = gidx[j];
+                dft::SolveIO io{b->i32 + b->off[i], nullptr, b->u(U_GMASK, i), b->f(F_GX, i), b->f(F_GY, i),
+                                1.0f / 65536.0f};
+                rc = b->dft.set_io(j, io);
+            }
+        }
+        if (rc) return bail(rc);
+    }
+    *out = b;
+    return TPT_OK;
+}
+
+int tpt_batch_destroy(tpt_batch *b) {
+    delete b;
+    return TPT_OK;
+}
+
+int tpt_batch_fields(tpt_batch *b, uint32_t i, tpt_instance_fields *o) {
+    if (!b || !o) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_fields: NULL pointer");
+    if (i >= b->n) TPT_FAIL(TPT_ERR_INVALID_ARG, "instance %u out of range (batch of %u)", i, b->n);
+    o->pv = b->f(F_PV, i);
+    o->vx = b->f(F_VX, i);
+    o->vy = b->f(F_VY, i);
+    o->hv = b->f(F_HV, i);
+    o->block_air = b->u(U_BA, i);
+    o->block_airh = b->u(U_BH, i);
+    o->wall_bmap = b->u(U_WALL, i);
+    o->wall_emap = b->u(U_EMAP, i);
+    o->elem_block_air = b->u(U_EA, i);
+    o->elem_block_airh = b->u(U_EH, i);
+    o->fan_vx = b->f(F_FVX, i);
+    o->fan_vy = b->f(F_FVY, i);
+    o->grav_mass = b->i32 + b->off[i];
+    o->grav_mask = b->u(U_GMASK, i);
+    o->gx = b->f(F_GX, i);
+    o->gy = b->f(F_GY, i);
+    return TPT_OK;
+}
+
+int tpt_batch_write(tpt_batch *b, uint32_t i, int field, const void *host, size_t bytes, tpt_stream_t stream) {
+    if (!b || !host) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_write: NULL pointer");
+    if (i >= b->n) TPT_FAIL(TPT_ERR_INVALID_ARG, "instance %u out of range", i);
+    size_t cells = (size_t)b->descs[i].air.xcells * b->descs[i].air.ycells;
+    if (bytes != cells * 4) TPT_FAIL(TPT_ERR_INVALID_ARG, "bytes %zu != %zu cells * 4", bytes, cells);
+    void *p;
+    int rc = field_ptr(b, i, field, &p);
+    if (rc) return rc;
+    TPT_CUDA(cudaMemcpyAsync(p, host, bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream));
+    return TPT_OK;
+}
+
+int tpt_batch_read(tpt_batch *b, uint32_t i, int field, void *host, size_t bytes, tpt_stream_t stream) {
+    if (!b || !host) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_read: NULL pointer");
+    if (i >= b->n) TPT_FAIL(TPT_ERR_INVALID_ARG, "instance %u out of range", i);
+    size_t cells = (size_t)b->descs[i].air.xcells * b->descs[i].air.ycells;
+    if (bytes != cells * 4) TPT_FAIL(TPT_ERR_INVALID_ARG, "bytes %zu != %zu cells * 4", bytes, cells);
+    void *p;
+    int rc = field_ptr(b, i, field, &p);
+    if (rc) return rc;
+    TPT_CUDA(cudaMemcpyAsync(host, p, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    return TPT_OK;
+}
+
+int tpt_batch_step(tpt_batch *b, uint32_t ticks, tpt_stream_t stream) {
+    if (!b) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_step: batch is NULL");
+    if (ticks == 0) return TPT_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    uint32_t full = ticks / CHUNK, rest = ticks % CHUNK;
+    cudaGraphExec_t g;
+    int rc;
+    if (full) {
+        rc = graph_for(b, CHUNK, &g);
+        if (rc) return rc;
+        for (uint32_t c = 0; c < full; ++c) {
+            TPT_CUDA(cudaGraphLaunch(g, st));
+        }
+    }
+    if (rest) {
+        rc = graph_for(b, rest, &g);
+        if (rc) return rc;
+        TPT_CUDA(cudaGraphLaunch(g, st));
+    }
+    return TPT_OK;
+}
+
+int tpt_batch_get_tuning(const tpt_batch *b, tpt_batch_tuning *t) {
+    if (!b || !t) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_get_tuning: NULL pointer");
+    *t = b->tuning;
+    return TPT_OK;
+}
+
+int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
+    if (!b || !t) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_set_tuning: NULL pointer");
+    if (t->tile_x != AIR_TX || t->tile_y != AIR_TY)
+        TPT_FAIL(TPT_ERR_UNSUPPORTED, "tile %ux%u not built (only %dx%d)", t->tile_x, t->tile_y, AIR_TX, AIR_TY);
+    if (t->temporal_depth != 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "temporal depth %u not built", t->temporal_depth);
+    if (t->ctas_per_sm < 1 || t->ctas_per_sm > 32) TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm must be 1..32");
+    if (t->ctas_per_sm != b->tuning.ctas_per_sm) b->drop_graphs();
+    b->tuning = *t;
+    return TPT_OK;
+}
+
+// Saved copy of the state arenas, for the calls that run trial ticks.
+struct StateCopy {
+    float *f = nullptr;
+    uint32_t *u = nullptr;
+    size_t fbytes = 0, ubytes = 0;
+    int save(const tpt_batch *b, cudaStream_t st) {
+        fbytes = b->stride * F_N32 * sizeof(float);
+        ubytes = b->stride * U_NU32 * sizeof(uint32_t);
+        TPT_CUDA(cudaMalloc(&f, fbytes));
+        TPT_CUDA(cudaMalloc(&u, ubytes));
+        TPT_CUDA(cudaMemcpyAsync(f, b->f32, fbytes, cudaMemcpyDeviceToDevice, st));
+        TPT_CUDA(cudaMemcpyAsync(u, b->u32, ubytes, cudaMemcpyDeviceToDevice, st));
+        return TPT_OK;
+    }
+    int restore(tpt_batch *b, cudaStream_t st) {
+        TPT_CUDA(cudaMemcpyAsync(b->f32, f, fbytes, cudaMemcpyDeviceToDevice, st));
+        TPT_CUDA(cudaMemcpyAsync(b->u32, u, ubytes, cudaMemcpyDeviceToDevice, st));
+        TPT_CUDA(cudaStreamSynchronize(st));
+        return TPT_OK;
+    }
+    ~StateCopy() {
+        cudaFree(f);
+        cudaFree(u);
+    }
+};
+
+int tpt_batch_profile_phases(tpt_batch *b, uint32_t ticks, tpt_stream_t stream, tpt_batch_profile *out) {
+    if (!b || !out) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_profile_phases: NULL pointer");
+    if (ticks == 0 || (ticks & 1u)) TPT_FAIL(TPT_ERR_INVALID_ARG, "ticks must be even and > 0");
+    cudaStream_t st = (cudaStream_t)stream;
+    StateCopy saved;
+    int rc = saved.save(b, st);
+    if (rc) return rc;
+    memset(out, 0, sizeof(*out));
+    out->ticks = ticks;
+    for (uint32_t i = 0; i < b->n; ++i) {
+        uint64_t c = (uint64_t)b->descs[i].air.xcells * b->descs[i].air.ycells;
+        out->cells += c;
+        if (b->descs[i].newton_grav) out->grav_cells += c;
+    }
+    out->air_launches_per_tick = b->any_noupdate_heat ? 3 : 2;
+    out->grav_launches_per_tick = b->any_grav ? (b->precision == TPT_PRECISION_FP32 ? 3 : b->dft.launches()) : 0;
+    out->grav_flops_per_tick = b->any_grav && b->precision != TPT_PRECISION_FP32 ? b->dft.flops() : 0.0;
+    cudaEvent_t e0, e1, e2;
+    TPT_CUDA(cudaEventCreate(&e0));
+    TPT_CUDA(cudaEventCreate(&e1));
+    TPT_CUDA(cudaEventCreate(&e2));
+    for (uint32_t t = 0; t < 2 && rc == TPT_OK; ++t)  // warm-up
+        rc = air::launch_batch_tick(b->insts, b->tiles, b->ntiles, b->grid(), t, b->any_noupdate_heat, st);
+    cudaEventRecord(e0, st);
+    for (uint32_t t = 0; t < ticks && rc == TPT_OK; ++t)
+        rc = air::launch_batch_tick(b->insts, b->tiles, b->ntiles, b->grid(), t & 1u, b->any_noupdate_heat, st);
+    cudaEventRecord(e1, st);
+    for (uint32_t t = 0; t < ticks && rc == TPT_OK && b->any_grav; ++t)
+        rc = b->precision == TPT_PRECISION_FP32 ? b->fft.launch(st) : b->dft.launch(st);
+    cudaEventRecord(e2, st);
+    if (rc == TPT_OK) {
+        cudaEventSynchronize(e2);
+        cudaEventElapsedTime(&out->air_ms, e0, e1);
+        cudaEventElapsedTime(&out->grav_ms, e1, e2);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    int rc2 = saved.restore(b, st);
+    return rc ? rc : rc2;
+}
+
+int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
+    if (!b) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_tune: batch is NULL");
+    cudaStream_t st = (cudaStream_t)stream;
+    StateCopy saved;
+    int src = saved.save(b, st);
+    if (src) return src;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const uint32_t cands[] = {1, 2, 4, 8};
+    tpt_batch_tuning best = b->tuning;
+    float best_ms = 1e30f;
+    int rc = TPT_OK;
+    for (uint32_t c : cands) {
+        tpt_batch_tuning t = b->tuning;
+        t.ctas_per_sm = c;
+        rc = tpt_batch_set_tuning(b, &t);
+        if (rc) break;
+        const uint32_t trial = 20;
+        for (int rep = 0; rep < 2 && rc == TPT_OK; ++rep) {  // warm-up, then timed
+            cudaEventRecord(e0, st);
+            for (uint32_t k = 0; k < trial && rc == TPT_OK; ++k)
+                rc = air::launch_batch_tick(b->insts, b->tiles, b->ntiles, b->grid(), k & 1u, b->any_noupdate_heat, st);
+            cudaEventRecord(e1, st);
+        }
+        if (rc) break;
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int rrc = saved.restore(b, st);
+    if (rc) return rc;
+    if (rrc) return rrc;
+    return tpt_batch_set_tuning(b, &best);
+}
+
+}  // extern "C"

@@ -1,0 +1,40 @@
+// grav_dft.hpp -- host side of the split-BF16 DFT-as-GEMM gravity solve.
+#pragma once
+
+#include <vector>
+
+#include "common.cuh"
+#include "grav_plan.hpp"
+
+namespace tpt {
+namespace dft {
+
+// Per-call inputs/outputs of a one-job solve.
+struct SolveIO {
+    const int32_t *mass_i;
+    const float *mass_f;
+    const uint32_t *mask;
+    float *gx, *gy;
+    float mass_scale_inv;
+};
+
+struct DftImpl;
+
+// A set of independent split-BF16 gravity solves (one plan = one job; a
+// batch = one job per instance).
+struct DftSet {
+    DftImpl *impl = nullptr;
+    int create(const std::vector<JobShape> &shapes);
+    void dims(size_t j, uint32_t *n1, uint32_t *n2) const;
+    // Binds job j to fixed inputs/outputs (a batch's arenas).
+    int set_io(size_t j, const SolveIO &io);
+    int launch(cudaStream_t st, const SolveIO *io = nullptr) const;
+    // kernel launches and executed tensor flops of one launch() of the set
+    uint32_t launches() const;
+    double flops() const;
+    void destroy();
+    ~DftSet() { destroy(); }
+};
+
+}  // namespace dft
+}  // namespace tpt

@@ -1,0 +1,478 @@
+"""Python host side of the B200 field step: ctypes bindings of
+libtpt_field.so (include/tpt_field.h) and a mirror of the reference's
+interface for this path.
+
+Reference interface mirrored here (paths relative to the reference project):
+
+  SimulationConfig   crates/tpt-core/src/particle.rs:166-345 (hot-path fields)
+  SimBuffers         crates/tpt-sim/src/buffers/mod.rs:186-230 (air, wall and
+                     gravity grids; device tensors in the reference layout)
+  step_air_gpu       crates/tpt-sim/src/air_kernel/mod.rs:120
+  GravityFft.solve   crates/tpt-sim/src/gravity_gpu/mod.rs:114
+  step_gravity       crates/tpt-sim/src/gravity_kernel.rs:826-920 (mask
+                     rebuild on a wall change, then the solve)
+
+Every call goes to the CUDA library; there is no CPU fallback. Importing
+works anywhere, but the first call raises `TptError` if the library is not
+built or no sm_100 GPU is present.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtpt_field.so")
+
+TPT_OK = 0
+ERRORS = {
+    -1: "TPT_ERR_INVALID_DIMS", -2: "TPT_ERR_NULL_POINTER", -3: "TPT_ERR_CUDA",
+    -4: "TPT_ERR_DEVICE_TIMEOUT", -5: "TPT_ERR_INVALID_ARG", -6: "TPT_ERR_OUT_OF_MEMORY",
+    -7: "TPT_ERR_UNSUPPORTED",
+}
+PRECISION_FP32 = 0
+PRECISION_SPLIT_BF16 = 1
+
+(FIELD_PV, FIELD_VX, FIELD_VY, FIELD_HV, FIELD_BLOCK_AIR, FIELD_BLOCK_AIRH, FIELD_WALL_BMAP, FIELD_WALL_EMAP,
+ FIELD_ELEM_BLOCK_AIR, FIELD_ELEM_BLOCK_AIRH, FIELD_FAN_VX, FIELD_FAN_VY, FIELD_GRAV_MASS, FIELD_GRAV_MASK,
+ FIELD_GX, FIELD_GY) = range(16)
+
+# Every symbol include/tpt_field.h declares.
+EXPORTS = [
+    "tpt_air_params_default", "tpt_air_step", "tpt_wall_masks_host", "tpt_grav_plan_create",
+    "tpt_grav_plan_destroy", "tpt_grav_plan_dims", "tpt_grav_solve", "tpt_grav_solve_f32",
+    "tpt_grav_mask_rebuild", "tpt_mass_to_fixed", "tpt_batch_create", "tpt_batch_destroy", "tpt_batch_fields",
+    "tpt_batch_write", "tpt_batch_read", "tpt_batch_step", "tpt_batch_tune", "tpt_batch_get_tuning",
+    "tpt_batch_set_tuning", "tpt_batch_profile_phases", "tpt_last_error_string", "tpt_kernel_launch_count", "tpt_version",
+]
+
+
+class TptError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+class AirParams(ctypes.Structure):
+    _fields_ = [
+        ("xcells", ctypes.c_uint32), ("ycells", ctypes.c_uint32),
+        ("air_mode", ctypes.c_uint32), ("aheat_enable", ctypes.c_uint32),
+        ("convection_mode", ctypes.c_uint32), ("gravity_mode", ctypes.c_uint32),
+        ("edge_pressure", ctypes.c_float), ("edge_vx", ctypes.c_float), ("edge_vy", ctypes.c_float),
+        ("ambient_air_temp", ctypes.c_float), ("vorticity_coeff", ctypes.c_float),
+        ("custom_gx", ctypes.c_float), ("custom_gy", ctypes.c_float),
+    ]
+
+
+class AirBufs(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in (
+        "pv", "vx", "vy", "hv", "opv", "ovx", "ovy", "ohv", "block_air", "block_airh", "wall_bmap", "wall_emap",
+        "elem_block_air", "elem_block_airh", "fan_vx", "fan_vy", "pmap", "elem_props")] + [
+        ("xres", ctypes.c_uint32), ("yres", ctypes.c_uint32), ("n_elements", ctypes.c_uint32)]
+
+
+class InstanceDesc(ctypes.Structure):
+    _fields_ = [("air", AirParams), ("newton_grav", ctypes.c_uint32)]
+
+
+class InstanceFields(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p) for n in (
+        "pv", "vx", "vy", "hv", "block_air", "block_airh", "wall_bmap", "wall_emap", "elem_block_air",
+        "elem_block_airh", "fan_vx", "fan_vy", "grav_mass", "grav_mask", "gx", "gy")]
+
+
+class BatchProfile(ctypes.Structure):
+    _fields_ = [("air_ms", ctypes.c_float), ("grav_ms", ctypes.c_float), ("ticks", ctypes.c_uint32),
+                ("air_launches_per_tick", ctypes.c_uint32), ("grav_launches_per_tick", ctypes.c_uint32),
+                ("cells", ctypes.c_uint64), ("grav_cells", ctypes.c_uint64), ("grav_flops_per_tick", ctypes.c_double)]
+
+
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("tile_x", ctypes.c_uint32), ("tile_y", ctypes.c_uint32), ("temporal_depth", ctypes.c_uint32),
+                ("ctas_per_sm", ctypes.c_uint32)]
+
+
+_lib = None
+
+
+def build() -> None:
+    """Compiles libtpt_field.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    subprocess.run(["make", "-s", "-j8", "-C", HERE], check=True)
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded CUDA library; raises if it is not built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise TptError(-7, f"{LIB_PATH} is not built (run build())")
+        L = ctypes.CDLL(LIB_PATH)
+        P, u32, i32, f32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int, ctypes.c_float
+        L.tpt_air_params_default.argtypes = [ctypes.POINTER(AirParams), u32, u32]
+        L.tpt_air_params_default.restype = None
+        L.tpt_air_step.argtypes = [ctypes.POINTER(AirParams), ctypes.POINTER(AirBufs), P]
+        L.tpt_wall_masks_host.argtypes = [P, P, P, P, ctypes.c_size_t]
+        L.tpt_grav_plan_create.argtypes = [u32, u32, i32, ctypes.POINTER(P)]
+        L.tpt_grav_plan_destroy.argtypes = [P]
+        L.tpt_grav_plan_dims.argtypes = [P, ctypes.POINTER(u32), ctypes.POINTER(u32)]
+        L.tpt_grav_solve.argtypes = [P, P, f32, P, P, P, P]
+        L.tpt_grav_solve_f32.argtypes = [P, P, P, P, P, P]
+        L.tpt_grav_mask_rebuild.argtypes = [P, P, u32, u32]
+        L.tpt_mass_to_fixed.argtypes = [f32]
+        L.tpt_mass_to_fixed.restype = ctypes.c_int32
+        L.tpt_batch_create.argtypes = [u32, ctypes.POINTER(InstanceDesc), i32, ctypes.POINTER(P)]
+        L.tpt_batch_destroy.argtypes = [P]
+        L.tpt_batch_fields.argtypes = [P, u32, ctypes.POINTER(InstanceFields)]
+        L.tpt_batch_write.argtypes = [P, u32, i32, P, ctypes.c_size_t, P]
+        L.tpt_batch_read.argtypes = [P, u32, i32, P, ctypes.c_size_t, P]
+        L.tpt_batch_step.argtypes = [P, u32, P]
+        L.tpt_batch_tune.argtypes = [P, P]
+        L.tpt_batch_get_tuning.argtypes = [P, ctypes.POINTER(BatchTuning)]
+        L.tpt_batch_set_tuning.argtypes = [P, ctypes.POINTER(BatchTuning)]
+        L.tpt_batch_profile_phases.argtypes = [P, u32, P, ctypes.POINTER(BatchProfile)]
+        L.tpt_last_error_string.restype = ctypes.c_char_p
+        L.tpt_kernel_launch_count.restype = ctypes.c_uint64
+        L.tpt_version.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != TPT_OK:
+        raise TptError(rc, lib().tpt_last_error_string().decode())
+
+
+def launch_count() -> int:
+    return int(lib().tpt_kernel_launch_count())
+
+
+def _ptr(t) -> ctypes.c_void_p | None:
+    if t is None:
+        return None
+    if isinstance(t, np.ndarray):
+        return t.ctypes.data_as(ctypes.c_void_p)
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream(stream) -> ctypes.c_void_p | None:
+    if stream is None:
+        import torch
+        return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return ctypes.c_void_p(stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream))
+
+
+# ----------------------------------------------------- reference mirror --
+
+@dataclasses.dataclass
+class SimulationConfig:
+    """Hot-path fields of the reference `SimulationConfig` with its defaults
+    (crates/tpt-core/src/particle.rs:290-345). `xres`/`yres` are pixels; the
+    air grid is (xres/4) x (yres/4) cells."""
+
+    xres: int = 612
+    yres: int = 384
+    air_mode: int = 0
+    aheat_enable: bool = False
+    convection_mode: int = 2
+    gravity_mode: int = 0
+    edge_pressure: float = 0.0
+    edge_velocity_x: float = 0.0
+    edge_velocity_y: float = 0.0
+    ambient_air_temp: float = 295.15
+    vorticity_coeff: float = 0.1
+    custom_gravity_x: float = 0.0
+    custom_gravity_y: float = 1.0
+    newton_grav: bool = False
+
+    @classmethod
+    def new(cls, xres: int, yres: int, **kw) -> "SimulationConfig":
+        """`SimulationConfig::new` (crates/tpt-core/src/particle.rs:290-293,
+        381-383): each side clamped to at least 64 px and rounded up to a
+        multiple of the 4-px cell."""
+        def align(v: int) -> int:
+            v = max(int(v), 64)
+            return (v + 3) // 4 * 4
+        return cls(xres=align(xres), yres=align(yres), **kw)
+
+    def xcells(self) -> int:
+        return self.xres // 4
+
+    def ycells(self) -> int:
+        return self.yres // 4
+
+    def num_cells(self) -> int:
+        return self.xcells() * self.ycells()
+
+    def air_params(self) -> AirParams:
+        return AirParams(self.xcells(), self.ycells(), int(self.air_mode), int(bool(self.aheat_enable)),
+                         int(self.convection_mode), int(self.gravity_mode), self.edge_pressure,
+                         self.edge_velocity_x, self.edge_velocity_y, self.ambient_air_temp, self.vorticity_coeff,
+                         self.custom_gravity_x, self.custom_gravity_y)
+
+
+_F32 = ("air_pv", "air_vx", "air_vy", "air_hv", "air_opv", "air_ovx", "air_ovy", "air_ohv", "fan_vx", "fan_vy",
+        "grav_fx", "grav_fy")
+_U32 = ("block_air", "block_airh", "wall_bmap", "wall_emap", "elem_block_air", "elem_block_airh", "grav_mask")
+
+
+class SimBuffers:
+    """Device grids of one canvas, in the reference layout and names
+    (`gpu_air_pv`, ... of crates/tpt-sim/src/buffers/mod.rs:186-230), held as
+    torch CUDA tensors. `grav_mass_prev` is the fixed-point mass the solve
+    reads; `grav_mask_dirty` triggers the flood fill on the next gravity step
+    (crates/tpt-sim/src/gravity_kernel.rs:868-881)."""
+
+    def __init__(self, config: SimulationConfig, device="cuda"):
+        import torch
+
+        self.config = config
+        n = config.num_cells()
+        for k in _F32:
+            setattr(self, k, torch.zeros(n, dtype=torch.float32, device=device))
+        for k in _U32:
+            setattr(self, k, torch.zeros(n, dtype=torch.int32, device=device))  # u32 bit patterns
+        self.grav_mass_prev = torch.zeros(n, dtype=torch.int32, device=device)
+        self.pmap = None
+        self.elem_props = None
+        self.grav_mask_dirty = True
+
+    @classmethod
+    def from_instance(cls, inst, device="cuda") -> "SimBuffers":
+        """Uploads a `workloads.Instance` (host numpy grids)."""
+        import torch
+
+        c = inst.config
+        cfg = SimulationConfig(xres=inst.xcells * 4, yres=inst.ycells * 4, air_mode=c.air_mode,
+                               aheat_enable=bool(c.aheat_enable), convection_mode=c.convection_mode,
+                               gravity_mode=c.gravity_mode, edge_pressure=c.edge_pressure,
+                               edge_velocity_x=c.edge_vx, edge_velocity_y=c.edge_vy,
+                               ambient_air_temp=c.ambient_air_temp, vorticity_coeff=c.vorticity_coeff,
+                               custom_gravity_x=c.custom_gx, custom_gravity_y=c.custom_gy,
+                               newton_grav=bool(c.newton_grav))
+        b = cls(cfg, device)
+
+        def put(name, arr, dt):
+            getattr(b, name).copy_(torch.from_numpy(np.ascontiguousarray(arr).view(dt)))
+
+        put("air_pv", inst.pv, np.float32)
+        put("air_vx", inst.vx, np.float32)
+        put("air_vy", inst.vy, np.float32)
+        put("air_hv", inst.hv, np.float32)
+        put("fan_vx", inst.fan_vx, np.float32)
+        put("fan_vy", inst.fan_vy, np.float32)
+        for name, arr in (("block_air", inst.bair), ("block_airh", inst.bairh), ("wall_bmap", inst.wall),
+                          ("wall_emap", inst.emap), ("elem_block_air", inst.eair),
+                          ("elem_block_airh", inst.eairh), ("grav_mask", inst.gmask)):
+            put(name, arr.astype(np.uint32), np.int32)
+        b.grav_mass_prev.copy_(torch.from_numpy(inst.mass_fx.astype(np.int32)))
+        b.grav_mask_dirty = False
+        return b
+
+    def air_state(self) -> dict:
+        """Host copies of the state grids (f32 and u32 numpy arrays)."""
+        out = {k: getattr(self, a).cpu().numpy() for k, a in (("pv", "air_pv"), ("vx", "air_vx"), ("vy", "air_vy"),
+                                                                ("hv", "air_hv"))}
+        for k, a in (("emap", "wall_emap"), ("bair", "block_air"), ("bairh", "block_airh")):
+            out[k] = getattr(self, a).cpu().numpy().view(np.uint32)
+        return out
+
+
+def air_bufs(b: SimBuffers) -> AirBufs:
+    x = AirBufs()
+    for name, attr in (("pv", "air_pv"), ("vx", "air_vx"), ("vy", "air_vy"), ("hv", "air_hv"), ("opv", "air_opv"),
+                       ("ovx", "air_ovx"), ("ovy", "air_ovy"), ("ohv", "air_ohv"), ("block_air", "block_air"),
+                       ("block_airh", "block_airh"), ("wall_bmap", "wall_bmap"), ("wall_emap", "wall_emap"),
+                       ("elem_block_air", "elem_block_air"), ("elem_block_airh", "elem_block_airh"),
+                       ("fan_vx", "fan_vx"), ("fan_vy", "fan_vy")):
+        setattr(x, name, _ptr(getattr(b, attr)))
+    if b.pmap is not None:
+        x.pmap = _ptr(b.pmap)
+        x.elem_props = _ptr(b.elem_props)
+        x.xres = b.config.xres
+        x.yres = b.config.yres
+        x.n_elements = b.elem_props.numel() // 32
+    return x
+
+
+def step_air_gpu(bufs: SimBuffers, stream=None) -> None:
+    """One air step on the device (crates/tpt-sim/src/air_kernel/mod.rs:120)."""
+    prm = bufs.config.air_params()
+    check(lib().tpt_air_step(ctypes.byref(prm), ctypes.byref(air_bufs(bufs)), _stream(stream)))
+
+
+class GravityFft:
+    """Gravity solver with a plan cached per canvas size, rebuilt lazily on a
+    size change (crates/tpt-sim/src/gravity_gpu/mod.rs:99-135)."""
+
+    def __init__(self, precision: int = PRECISION_FP32):
+        self.precision = precision
+        self._plan = None
+        self._dims = None
+
+    def _ensure(self, xcells: int, ycells: int):
+        if self._dims != (xcells, ycells):
+            self.close()
+            p = ctypes.c_void_p()
+            check(lib().tpt_grav_plan_create(xcells, ycells, self.precision, ctypes.byref(p)))
+            self._plan, self._dims = p, (xcells, ycells)
+
+    def padded_dims(self):
+        n1, n2 = ctypes.c_uint32(), ctypes.c_uint32()
+        check(lib().tpt_grav_plan_dims(self._plan, ctypes.byref(n1), ctypes.byref(n2)))
+        return n1.value, n2.value
+
+    def solve(self, bufs: SimBuffers, mass, mass_scale_inv: float = 1.0 / 65536.0, stream=None) -> None:
+        """Solves into bufs.grav_fx / grav_fy from a fixed-point i32 `mass`
+        grid, or from an f32 grid (then `mass_scale_inv` is unused)."""
+        import torch
+
+        X, Y = bufs.config.xcells(), bufs.config.ycells()
+        if X == 0 or Y == 0:
+            return
+        self._ensure(X, Y)
+        if mass.dtype == torch.float32:
+            check(lib().tpt_grav_solve_f32(self._plan, _ptr(mass), _ptr(bufs.grav_mask), _ptr(bufs.grav_fx),
+                                           _ptr(bufs.grav_fy), _stream(stream)))
+        else:
+            check(lib().tpt_grav_solve(self._plan, _ptr(mass), float(mass_scale_inv), _ptr(bufs.grav_mask),
+                                       _ptr(bufs.grav_fx), _ptr(bufs.grav_fy), _stream(stream)))
+
+    def close(self):
+        if self._plan is not None:
+            lib().tpt_grav_plan_destroy(self._plan)
+            self._plan, self._dims = None, None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def rebuild_gravity_mask(wall_bmap: np.ndarray, xcells: int, ycells: int) -> np.ndarray:
+    """Host flood fill (crates/tpt-sim/src/gravity_kernel.rs:658-712)."""
+    w = np.ascontiguousarray(wall_bmap, np.uint32)
+    out = np.zeros(xcells * ycells, np.uint32)
+    check(lib().tpt_grav_mask_rebuild(_ptr(w), _ptr(out), xcells, ycells))
+    return out
+
+
+def step_gravity(bufs: SimBuffers, solver: GravityFft, stream=None) -> None:
+    """The field part of `step_gravity_gpu` (crates/tpt-sim/src/gravity_kernel.rs:
+    826-920): skipped unless newton_grav; the mask is rebuilt after a wall
+    change, then the previous tick's mass is solved."""
+    import torch
+
+    if not bufs.config.newton_grav:
+        bufs.grav_fx.zero_()
+        bufs.grav_fy.zero_()
+        return
+    if bufs.grav_mask_dirty:
+        wall = bufs.wall_bmap.cpu().numpy().view(np.uint32)
+        m = rebuild_gravity_mask(wall, bufs.config.xcells(), bufs.config.ycells())
+        bufs.grav_mask.copy_(torch.from_numpy(m.view(np.int32)))
+        bufs.grav_mask_dirty = False
+    solver.solve(bufs, bufs.grav_mass_prev, 1.0 / 65536.0, stream)
+
+
+def mass_to_fixed(m: float) -> int:
+    return int(lib().tpt_mass_to_fixed(float(m)))
+
+
+# ------------------------------------------------------------- batches --
+
+class Batch:
+    """Many independent instances stepped together (tpt_batch_*)."""
+
+    def __init__(self, instances, precision: int = PRECISION_FP32, stream=None):
+        n = len(instances)
+        descs = (InstanceDesc * n)()
+        for i, inst in enumerate(instances):
+            c = inst.config
+            descs[i].air = AirParams(inst.xcells, inst.ycells, c.air_mode, c.aheat_enable, c.convection_mode,
+                                     c.gravity_mode, c.edge_pressure, c.edge_vx, c.edge_vy, c.ambient_air_temp,
+                                     c.vorticity_coeff, c.custom_gx, c.custom_gy)
+            descs[i].newton_grav = int(bool(c.newton_grav))
+        self.n = n
+        self.shapes = [(inst.xcells, inst.ycells) for inst in instances]
+        self.precision = precision
+        self._h = ctypes.c_void_p()
+        check(lib().tpt_batch_create(n, descs, precision, ctypes.byref(self._h)))
+        self.write_all(instances, stream)
+
+    GRIDS = (("pv", FIELD_PV), ("vx", FIELD_VX), ("vy", FIELD_VY), ("hv", FIELD_HV), ("bair", FIELD_BLOCK_AIR),
+             ("bairh", FIELD_BLOCK_AIRH), ("wall", FIELD_WALL_BMAP), ("emap", FIELD_WALL_EMAP),
+             ("eair", FIELD_ELEM_BLOCK_AIR), ("eairh", FIELD_ELEM_BLOCK_AIRH), ("fan_vx", FIELD_FAN_VX),
+             ("fan_vy", FIELD_FAN_VY), ("mass_fx", FIELD_GRAV_MASS), ("gmask", FIELD_GRAV_MASK))
+
+    def write(self, i: int, field: int, arr: np.ndarray, stream=None):
+        a = np.ascontiguousarray(arr)
+        assert a.itemsize == 4
+        check(lib().tpt_batch_write(self._h, i, field, _ptr(a), a.nbytes, _stream(stream)))
+
+    def read(self, i: int, field: int, dtype, out: np.ndarray | None = None, stream=None) -> np.ndarray:
+        X, Y = self.shapes[i]
+        a = np.empty(X * Y, dtype) if out is None else out
+        check(lib().tpt_batch_read(self._h, i, field, _ptr(a), a.nbytes, _stream(stream)))
+        return a
+
+    def write_all(self, instances, stream=None):
+        import torch
+
+        for i, inst in enumerate(instances):
+            for name, fid in self.GRIDS:
+                self.write(i, fid, getattr(inst, name), stream)
+        torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+
+    def step(self, ticks: int, stream=None):
+        check(lib().tpt_batch_step(self._h, int(ticks), _stream(stream)))
+
+    def tune(self, stream=None):
+        check(lib().tpt_batch_tune(self._h, _stream(stream)))
+
+    def profile_phases(self, ticks: int, stream=None) -> BatchProfile:
+        out = BatchProfile()
+        check(lib().tpt_batch_profile_phases(self._h, int(ticks), _stream(stream), ctypes.byref(out)))
+        return out
+
+    def tuning(self) -> BatchTuning:
+        t = BatchTuning()
+        check(lib().tpt_batch_get_tuning(self._h, ctypes.byref(t)))
+        return t
+
+    def set_tuning(self, t: BatchTuning):
+        check(lib().tpt_batch_set_tuning(self._h, ctypes.byref(t)))
+
+    def fields(self, i: int) -> InstanceFields:
+        f = InstanceFields()
+        check(lib().tpt_batch_fields(self._h, i, ctypes.byref(f)))
+        return f
+
+    def state(self, i: int, stream=None) -> dict:
+        import torch
+
+        out = {
+            "pv": self.read(i, FIELD_PV, np.float32, stream=stream), "vx": self.read(i, FIELD_VX, np.float32, stream=stream),
+            "vy": self.read(i, FIELD_VY, np.float32, stream=stream), "hv": self.read(i, FIELD_HV, np.float32, stream=stream),
+            "emap": self.read(i, FIELD_WALL_EMAP, np.uint32, stream=stream),
+            "bair": self.read(i, FIELD_BLOCK_AIR, np.uint32, stream=stream),
+            "bairh": self.read(i, FIELD_BLOCK_AIRH, np.uint32, stream=stream),
+            "gx": self.read(i, FIELD_GX, np.float32, stream=stream), "gy": self.read(i, FIELD_GY, np.float32, stream=stream),
+        }
+        torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+        return out
+
+    def close(self):
+        if self._h:
+            lib().tpt_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
