@@ -255,21 +255,23 @@ def run_ours(args, rank, world, local):
             for fid, a in d.items():
                 tf.check(tf.lib().tpt_batch_read(batch._h, i, fid, tf._ptr(a), a.nbytes, tf._stream(stream)))
 
-    e2e_steps = max(1, min(args.steps, 3))
-    e2e_step()
-    torch.cuda.synchronize()
-    barrier(world)
-    e0.record(stream)
-    for _ in range(e2e_steps):
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
+    e2e_value = None
+    if e2e_steps:
         e2e_step()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier(world)
-    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
-    e2e_value = cells * ticks * e2e_steps * world / (e2e_ms / 1e3)
+        torch.cuda.synchronize()
+        barrier(world)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        e2e_value = cells * ticks * e2e_steps * world / (e2e_ms / 1e3)
 
     # per-phase device times for the roofline
-    prof = batch.profile_phases(200)
+    prof = batch.profile_phases(args.phase_ticks)
     hbm, bf16, bf16s, peak_src = load_peaks()
     air_gbs = prof.cells * prof.ticks * B_AIR / (prof.air_ms / 1e3) / 1e9
     air_launch_ms = prof.air_ms / (prof.ticks * prof.air_launches_per_tick)
@@ -350,6 +352,8 @@ def main():
     ap.add_argument("--ticks", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer run (profiling captures)")
+    ap.add_argument("--phase-ticks", type=int, default=200, help="even tick count of the per-phase timing")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -415,7 +415,7 @@ class Batch:
         check(lib().tpt_batch_write(self._h, i, field, _ptr(a), a.nbytes, _stream(stream)))
 
     def read(self, i: int, field: int, dtype, out: np.ndarray | None = None, stream=None) -> np.ndarray:
-        X, Y = self.shapes[i]
+        X, Y = self.shapes[i] if 0 <= i < self.n else (1, 1)  # the library rejects a bad index
         a = np.empty(X * Y, dtype) if out is None else out
         check(lib().tpt_batch_read(self._h, i, field, _ptr(a), a.nbytes, _stream(stream)))
         return a
