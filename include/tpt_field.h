@@ -143,6 +143,34 @@ void tpt_air_params_default(tpt_air_params *p, uint32_t xcells, uint32_t ycells)
 int tpt_air_step(const tpt_air_params *params, const tpt_air_bufs *bufs,
                  tpt_stream_t stream);
 
+/* Largest grid (cells) tpt_air_step_static_scratch accepts: a 2048x2048-px
+ * canvas, the largest the reference's UI offers. */
+#define TPT_STATIC_SCRATCH_MAX_CELLS (512u * 512u)
+
+/*
+ * The same air step as tpt_air_step, for callers that cannot allocate
+ * device memory -- for example an engine whose device memory all comes from
+ * its own pool or graphics API, or code running where cudaMalloc is not
+ * allowed. No counterpart in the reference (its SimBuffers always owns the
+ * four scratch grids).
+ *
+ * The four scratch grids (`opv`, `ovx`, `ovy`, `ohv` of `bufs`, which are
+ * ignored and may be NULL) come from one 4 MiB array in the library's own
+ * device image instead, so the call allocates nothing, on the device or the
+ * host. Every device that loads the library holds that array until the
+ * process exits. Grids larger than TPT_STATIC_SCRATCH_MAX_CELLS cells are
+ * rejected with TPT_ERR_INVALID_DIMS.
+ *
+ * The first call on a device looks the array up for that device (with the
+ * device current); make that first call outside any stream capture. All
+ * calls share the one array: calls whose work can overlap on the GPU (other
+ * streams, other host threads) race on it and must be serialised by the
+ * caller. Nothing needs clearing between calls -- each step writes every
+ * scratch cell it reads.
+ */
+int tpt_air_step_static_scratch(const tpt_air_params *params,
+                                const tpt_air_bufs *bufs, tpt_stream_t stream);
+
 /* Host twin of the wall-mask rebuild (crates/tpt-sim/src/buffers/spatial.rs:
  * 336-352): block masks from wall ids and emap, no element stamps. */
 int tpt_wall_masks_host(const uint32_t *wall_bmap_host,

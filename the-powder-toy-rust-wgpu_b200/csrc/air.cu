@@ -1,6 +1,7 @@
 // air.cu -- launches of the air step (single grid and batched instances).
 // Compiled with -fmad=false: see air.cuh.
 #include <algorithm>
+#include <mutex>
 
 #include "air.cuh"
 #include "air_launch.hpp"
@@ -187,5 +188,84 @@ int launch_copy_back(const AirInst *insts, const TileRef *tiles, uint32_t ntiles
     return TPT_OK;
 }
 
+// ---- air step with library-owned scratch (no allocation) ------------------
+// The step needs four grids of scratch (new pressure, the two new velocity
+// components and the new heat). tpt_air_step takes them from the caller;
+// this variant takes them from one array that lives in the library's device
+// image, so a call allocates nothing. Every device that loads the library
+// holds the array (4 MiB) until the process exits.
+static __device__ __align__(256) float g_static_scratch[4 * (size_t)TPT_STATIC_SCRATCH_MAX_CELLS];
+
+// Device address of g_static_scratch on the current device. The name is a
+// host-side stand-in in host code, so the address is looked up once per
+// device with that device current, and cached.
+static int static_scratch(float **out) {
+    static std::mutex mu;
+    static float *cache[128] = {};
+    int dev = 0;
+    TPT_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) TPT_FAIL(TPT_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!cache[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess || p == nullptr)
+            TPT_FAIL(TPT_ERR_CUDA, "cudaGetSymbolAddress(static scratch) failed on device %d: %s", dev,
+                     cudaGetErrorString(e));
+        cache[dev] = static_cast<float *>(p);
+    }
+    *out = cache[dev];
+    return TPT_OK;
+}
+
 }  // namespace air
 }  // namespace tpt
+
+extern "C" int tpt_air_step_static_scratch(const tpt_air_params *params, const tpt_air_bufs *b,
+                                           tpt_stream_t stream) {
+    using namespace tpt;
+    if (!params || !b) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_air_step_static_scratch: params or bufs is NULL");
+    const tpt_air_params &p = *params;
+    if (p.air_mode > 4u || p.convection_mode > 2u || p.gravity_mode > 3u || p.aheat_enable > 1u)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "tpt_air_step_static_scratch: enum field out of range");
+    if (p.xcells == 0 || p.ycells == 0) return TPT_OK;
+    const size_t n = (size_t)p.xcells * p.ycells;
+    if (p.xcells > TPT_MAX_CELLS_PER_SIDE || p.ycells > TPT_MAX_CELLS_PER_SIDE || n > TPT_STATIC_SCRATCH_MAX_CELLS)
+        TPT_FAIL(TPT_ERR_INVALID_DIMS,
+                 "tpt_air_step_static_scratch: grid %ux%u = %zu cells exceeds the static scratch of %u cells "
+                 "(use tpt_air_step with caller-owned scratch)",
+                 p.xcells, p.ycells, n, (unsigned)TPT_STATIC_SCRATCH_MAX_CELLS);
+    if (!b->pv || !b->vx || !b->vy || !b->hv || !b->block_air || !b->block_airh || !b->wall_bmap || !b->wall_emap ||
+        !b->fan_vx || !b->fan_vy)
+        TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_air_step_static_scratch: a required grid pointer is NULL");
+    if (b->pmap && (!b->elem_props || b->xres == 0 || b->yres == 0))
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "tpt_air_step_static_scratch: pmap given without elem_props / xres / yres");
+    int rc = require_sm100();
+    if (rc) return rc;
+    float *s = nullptr;
+    rc = air::static_scratch(&s);
+    if (rc) return rc;
+    // Every scratch cell the step reads is written earlier in the same step,
+    // so nothing has to be cleared between calls.
+    AirInst I = make_air_inst(p);
+    I.pv = b->pv;
+    I.vx = b->vx;
+    I.vy = b->vy;
+    I.hv = b->hv;
+    I.opv = s;
+    I.ovx = s + n;
+    I.ovy = s + 2 * n;
+    I.ohv = s + 3 * n;
+    I.bair = b->block_air;
+    I.bairh = b->block_airh;
+    I.wall = b->wall_bmap;
+    I.emap = b->wall_emap;
+    I.eair = b->elem_block_air;
+    I.eairh = b->elem_block_airh;
+    I.fvx = b->fan_vx;
+    I.fvy = b->fan_vy;
+    I.bair_out = b->block_air;
+    I.bairh_out = b->block_airh;
+    I.hv_out = I.ohv;
+    return air::launch_single(I, b->pmap, b->elem_props, b->n_elements, b->xres, b->yres, (cudaStream_t)stream);
+}

@@ -66,6 +66,9 @@ struct AirInst {
     float *hv_out;
 };
 
+// AirInst with the scalar fields of `p` set and every pointer null.
+AirInst make_air_inst(const tpt_air_params &p);
+
 // Air tile shape (cells). One CTA of AIR_TX*AIR_TY threads owns one tile.
 constexpr int AIR_TX = 32;
 constexpr int AIR_TY = 8;

@@ -43,7 +43,7 @@ PRECISION_SPLIT_BF16 = 1
 
 # Every symbol include/tpt_field.h declares.
 EXPORTS = [
-    "tpt_air_params_default", "tpt_air_step", "tpt_wall_masks_host", "tpt_grav_plan_create",
+    "tpt_air_params_default", "tpt_air_step", "tpt_air_step_static_scratch", "tpt_wall_masks_host", "tpt_grav_plan_create",
     "tpt_grav_plan_destroy", "tpt_grav_plan_dims", "tpt_grav_solve", "tpt_grav_solve_f32",
     "tpt_grav_mask_rebuild", "tpt_mass_to_fixed", "tpt_batch_create", "tpt_batch_destroy", "tpt_batch_fields",
     "tpt_batch_write", "tpt_batch_read", "tpt_batch_step", "tpt_batch_tune", "tpt_batch_get_tuning",
@@ -115,6 +115,7 @@ def lib() -> ctypes.CDLL:
         L.tpt_air_params_default.argtypes = [ctypes.POINTER(AirParams), u32, u32]
         L.tpt_air_params_default.restype = None
         L.tpt_air_step.argtypes = [ctypes.POINTER(AirParams), ctypes.POINTER(AirBufs), P]
+        L.tpt_air_step_static_scratch.argtypes = [ctypes.POINTER(AirParams), ctypes.POINTER(AirBufs), P]
         L.tpt_wall_masks_host.argtypes = [P, P, P, P, ctypes.c_size_t]
         L.tpt_grav_plan_create.argtypes = [u32, u32, i32, ctypes.POINTER(P)]
         L.tpt_grav_plan_destroy.argtypes = [P]
