@@ -318,6 +318,15 @@ int tpt_batch_profile_phases(tpt_batch *batch, uint32_t ticks,
 
 /* ---- diagnostics ------------------------------------------------------- */
 
+/*
+ * Reads and clears the library's device error word on the current device:
+ * TPT_ERR_DEVICE_TIMEOUT if a bounded device-side wait (tensor-core
+ * pipeline barriers) gave up since the last call, TPT_OK otherwise. The
+ * kernel that timed out skipped its remaining work and released its
+ * resources, so the context stays usable. Synchronises the device.
+ */
+int tpt_check_device_errors(void);
+
 /* Message of the last failure on the calling thread ("" if none). */
 const char *tpt_last_error_string(void);
 /* Number of kernel launches this library has issued (all threads). */

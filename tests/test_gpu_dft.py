@@ -1,0 +1,92 @@
+"""GPU accuracy of the split-BF16 DFT-as-GEMM gravity (tcgen05) against the
+FP64 oracle. Bar (per result): max |g - g64| <= 1e-4 * max |g64| and the L2
+error normalised by ||g64|| <= 1e-4, for gx and gy; exact zeros outside the
+mask; no device-side wait timed out."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+def errors(g, ref):
+    g = g.astype(np.float64)
+    scale = max(np.abs(ref).max(), 1e-30)
+    return np.abs(g - ref).max() / scale, np.linalg.norm(g - ref) / max(np.linalg.norm(ref), 1e-30)
+
+
+def check_clean(tf):
+    rc = tf.lib().tpt_check_device_errors()
+    assert rc == 0, tf.lib().tpt_last_error_string().decode()
+
+
+@pytest.mark.parametrize("X,Y,kind", [(24, 24, "stress"), (37, 29, "stress"), (64, 48, "stress"),
+                                      (153, 96, "c1"), (400, 225, "c2"), (32, 130, "stress")])
+def test_split_bf16_plan_vs_fp64(cuda, tf, oracle, X, Y, kind):
+    import workloads as W
+    from test_gpu_grav import solve_gpu
+
+    if kind == "c1":
+        inst = W.config_instances(1)[0]
+    elif kind == "c2":
+        inst = W.config_instances(2)[0]
+    else:
+        inst = W.make_stress_instance(X, Y, 31 * X + Y)
+    gx, gy = solve_gpu(tf, cuda, X, Y, inst.gmask, inst.mass_fx, precision=tf.PRECISION_SPLIT_BF16)
+    check_clean(tf)
+    dx, dy = oracle.grav_solve(X, Y, inst.gmask, mass_fx=inst.mass_fx, dtype=np.float64)
+    for g, d in ((gx, dx), (gy, dy)):
+        emax, el2 = errors(g, d)
+        assert emax <= TOL and el2 <= TOL, (emax, el2)
+    assert np.all(gx[inst.gmask == 0] == 0) and np.all(gy[inst.gmask == 0] == 0)
+
+
+def test_split_bf16_c3_f32_mass(cuda, tf, oracle):
+    import workloads as W
+    from test_gpu_grav import solve_gpu
+
+    X = Y = 512
+    mass = W.clustered_mass(X, Y, W.instance_seed(3, 0))
+    mask = np.full(X * Y, 0xFFFFFFFF, np.uint32)
+    gx, gy = solve_gpu(tf, cuda, X, Y, mask, mass_f32=mass, precision=tf.PRECISION_SPLIT_BF16)
+    check_clean(tf)
+    dx, dy = oracle.grav_solve(X, Y, mask, mass_f32=mass, dtype=np.float64)
+    for g, d in ((gx, dx), (gy, dy)):
+        emax, el2 = errors(g, d)
+        assert emax <= TOL and el2 <= TOL, (emax, el2)
+
+
+def test_split_bf16_plan_dims_and_repeat(cuda, tf):
+    import workloads as W
+    from test_gpu_grav import solve_gpu
+
+    inst = W.config_instances(1)[0]
+    outs = solve_gpu(tf, cuda, 153, 96, inst.gmask, inst.mass_fx, precision=tf.PRECISION_SPLIT_BF16, repeat=2)
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    s = tf.GravityFft(tf.PRECISION_SPLIT_BF16)
+    s._ensure(153, 96)
+    assert s.padded_dims() == (306, 192)
+    s.close()
+
+
+def test_split_bf16_batch_mixed_shapes(cuda, tf, oracle):
+    """Equal-shape instances share one stacked GEMM per stage; singletons
+    run as their own groups; all in the same launches."""
+    import workloads as W
+
+    insts = W.config_instances(5, limit=3)  # three 400x225
+    insts += [W.make_instance(57, 36, 5, mass_density=0.02), W.make_instance(33, 151, 6, mass_density=0.02),
+              W.make_instance(57, 36, 7, mass_density=0.02)]
+    b = tf.Batch(insts, tf.PRECISION_SPLIT_BF16)
+    b.step(2)
+    cuda.cuda.synchronize()
+    check_clean(tf)
+    for i, inst in enumerate(insts):
+        st = b.state(i)
+        dx, dy = oracle.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx, dtype=np.float64)
+        for g, d in ((st["gx"], dx), (st["gy"], dy)):
+            emax, el2 = errors(g, d)
+            assert emax <= TOL and el2 <= TOL, (i, emax, el2)
+    b.close()

@@ -83,6 +83,15 @@ struct tpt_grav_plan {
 extern "C" {
 
 const char *tpt_last_error_string(void) { return g_err; }
+
+int tpt_check_device_errors(void) {
+    TPT_CUDA(cudaDeviceSynchronize());
+    uint32_t bits = 0;
+    int rc = dft::read_errors(&bits);
+    if (rc) return rc;
+    if (bits) TPT_FAIL(TPT_ERR_DEVICE_TIMEOUT, "a device-side wait timed out (error bits 0x%x)", bits);
+    return TPT_OK;
+}
 uint64_t tpt_kernel_launch_count(void) { return g_launches.load(); }
 const char *tpt_version(void) { return "tpt-field-b200 0.1.0 (sm_100a)"; }
 

@@ -1,31 +1,716 @@
-// grav_dft.cu -- split-BF16 DFT-as-GEMM gravity solve (tcgen05). Not built
-// yet: plans of this precision report TPT_ERR_UNSUPPORTED.
+// grav_dft.cu -- the gravity solve as split-BF16 DFT-as-GEMM on tcgen05.
+//
+// Same result as the FFT solve (crates/tpt-sim/src/gravity_gpu/mod.rs:204-278):
+// g = mask * (mass * K) for K(d) = -M_GRAV d / |d|^3, the linear convolution
+// of the X x Y mass grid, computed through an N1 x N2 = 2X x 2Y padded DFT.
+// The 1-D transforms are dense matrix products on the tensor cores:
+//
+//   R    A[y,kx]  = sum_x  m[y,x]   e^{-2 pi i kx x / N1}    kx < N1/2+1 (Hermitian half)
+//   C    B[ky,kx] = sum_y  F2[ky,y] A[y,kx]                  F2 = e^{-2 pi i ky y / N2}
+//        S_f      = B * i Ks_f[ky,kx]                         (kernel spectra are imaginary)
+//   C^-1 C_f[y,kx]= sum_ky G2[y,ky] S_f[ky,kx]               G2 = e^{+2 pi i y ky / N2}
+//   R^-1 g_f[y,x] = sum_kx Re(C_f[y,kx] w_kx e^{+2 pi i kx x / N1})   w = 1, 2, ..., 2, 1
+//
+// Every operand is stored as bf16 hi/lo planes (v = hi + lo, 16 significant
+// bits) and each product is the 3-term split hi*hi + hi*lo + lo*hi,
+// accumulated in FP32 in TMEM. Instances of equal shape form a group whose
+// data operands are stacked along M or N, so a group is four GEMMs; all
+// groups' tiles run in one persistent launch per stage. The kernel spectra
+// and DFT matrices are built once in FP64 on the device.
+//
+// GEMM kernel: 192 threads. Warp 0 issues TMA tile loads (64-byte swizzle,
+// 32-wide K tiles, no multicast) into a 3-stage shared-memory ring; warp 1
+// issues tcgen05.mma (M=128, N=256/128, K=16) into a double-buffered TMEM
+// accumulator; warps 2-5 read the accumulator with tcgen05.ld and run the
+// stage's epilogue, which writes the next stage's operand planes. Every
+// mbarrier wait is bounded (see tc.cuh).
+#include <cudaTypedefs.h>
+#include <math.h>
+
+#include <algorithm>
+#include <map>
+#include <vector>
+
 #include "grav_dft.hpp"
+#include "tc.cuh"
 
 namespace tpt {
 namespace dft {
 
-struct DftImpl {
-    std::vector<JobShape> shapes;
+using bf16 = __nv_bfloat16;
+
+constexpr int KT = 32;             // K elements per tile (64 bytes)
+constexpr int MT = 128;            // rows per M tile
+constexpr int NT = 128;            // complex columns per N tile
+constexpr int STAGES = 3;
+constexpr int TILE_BYTES = MT * KT * 2;  // one plane of one tile: 8 KB
+constexpr int STAGE_BYTES = 8 * TILE_BYTES;
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;
+constexpr int THREADS = 192;
+
+enum Stage : int { ST_R = 0, ST_C = 1, ST_CI = 2, ST_RI = 3 };
+
+__device__ uint32_t g_dft_err;
+
+// One group of equal-shape instances (device copy).
+struct Group {
+    uint32_t X, Y, N1, N2, N1h, G, inst0;
+    uint32_t kpR, kpC, kpCi, kpRi;       // K pitches (elements)
+    uint32_t rowsR, rowsC, rowsCi, rowsRi;  // rows per plane of the data operands
+    bf16 *aR, *bC, *bCi, *aRi;           // data operands (planes stacked)
+    const float *kxs, *kys;              // imaginary parts of the kernel spectra, [kx][ky]
 };
 
+struct InstIO {
+    const int32_t *mass_i;
+    const float *mass_f;
+    const uint32_t *mask;
+    float *gx, *gy;
+    float inv;
+};
+
+struct Problem {
+    const CUtensorMap *ta, *tb;
+    uint32_t group, M, N, ktiles, a_rows, b_rows;
+};
+
+struct Tile {
+    uint32_t problem;
+    uint16_t mt, nt;
+};
+
+// ---- helpers ---------------------------------------------------------------
+__device__ __forceinline__ void split_store(bf16 *hi, bf16 *lo, float v) {
+    bf16 h = __float2bfloat16_rn(v);
+    *hi = h;
+    *lo = __float2bfloat16_rn(v - __bfloat162float(h));
+}
+
+// ---- the GEMM kernel ---------------------------------------------------------
+template <int STAGE>
+__global__ void __launch_bounds__(THREADS, 1)
+    dft_gemm(const Problem *__restrict__ probs, const Tile *__restrict__ tiles, uint32_t ntiles,
+             const Group *__restrict__ groups, const InstIO *__restrict__ ios, InstIO io0, int io0_active,
+             uint32_t *err) {
+    constexpr bool A_COMPLEX = STAGE != ST_R;
+    constexpr bool OUT_COMPLEX = STAGE != ST_RI;
+    constexpr uint32_t A_PLANES = A_COMPLEX ? 4 : 2;
+    constexpr uint32_t TX_BYTES = (A_PLANES + 4) * TILE_BYTES;
+
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ uint64_t full_bar[STAGES], empty_bar[STAGES], acc_full[2], acc_empty[2];
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            tc::mbar_init(&full_bar[s], 1);
+            tc::mbar_init(&empty_bar[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            tc::mbar_init(&acc_full[a], 1);
+            tc::mbar_init(&acc_empty[a], 4);
+        }
+        abort_flag = 0;
+        tc::fence_mbar_init();
+    }
+    if (warp == 1) tc::tmem_alloc(&tmem_slot, 512);
+    tc::tc_fence_before();
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    if (warp == 0) {
+        // ---------------- TMA producer ----------------
+        if (lane == 0) {
+            uint32_t s = 0, ph = 0;
+            for (uint32_t t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x) {
+                const Tile T = tiles[t];
+                const Problem P = probs[T.problem];
+                const int32_t m0 = T.mt * MT, n0 = T.nt * NT;
+                for (uint32_t kt = 0; kt < P.ktiles; ++kt) {
+                    if (!tc::mbar_wait(&empty_bar[s], ph ^ 1u, err)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    uint8_t *st = smem + s * STAGE_BYTES;
+                    tc::mbar_arrive_expect_tx(&full_bar[s], TX_BYTES);
+                    const int32_t k0 = kt * KT;
+                    for (uint32_t p = 0; p < A_PLANES; ++p)
+                        tc::tma_load_2d(st + p * TILE_BYTES, P.ta, k0, (int32_t)(p * P.a_rows) + m0, &full_bar[s]);
+                    // B: hi block [r_hi | i_hi], lo block [r_lo | i_lo]
+                    uint8_t *bb = st + 4 * TILE_BYTES;
+                    tc::tma_load_2d(bb + 0 * TILE_BYTES, P.tb, k0, (int32_t)(0 * P.b_rows) + n0, &full_bar[s]);
+                    tc::tma_load_2d(bb + 1 * TILE_BYTES, P.tb, k0, (int32_t)(2 * P.b_rows) + n0, &full_bar[s]);
+                    tc::tma_load_2d(bb + 2 * TILE_BYTES, P.tb, k0, (int32_t)(1 * P.b_rows) + n0, &full_bar[s]);
+                    tc::tma_load_2d(bb + 3 * TILE_BYTES, P.tb, k0, (int32_t)(3 * P.b_rows) + n0, &full_bar[s]);
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer ----------------
+        if (lane == 0) {
+            constexpr uint32_t I256 = tc::idesc_bf16(128, 256), I128 = tc::idesc_bf16(128, 128);
+            constexpr uint32_t I128N = tc::idesc_bf16(128, 128, true);
+            uint32_t s = 0, ph = 0, acc = 0, acc_ph = 0;
+            for (uint32_t t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x) {
+                const Problem P = probs[tiles[t].problem];
+                if (!tc::mbar_wait(&acc_empty[acc], acc_ph ^ 1u, err)) {
+                    abort_flag = 1;
+                    break;
+                }
+                tc::tc_fence_after();
+                const uint32_t d = tmem + acc * 256;
+                for (uint32_t kt = 0; kt < P.ktiles; ++kt) {
+                    if (!tc::mbar_wait(&full_bar[s], ph, err)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    tc::tc_fence_after();
+                    const uint32_t st = tc::smem_u32(smem + s * STAGE_BYTES);
+                    const uint32_t arh = st, arl = st + TILE_BYTES, aih = st + 2 * TILE_BYTES,
+                                   ail = st + 3 * TILE_BYTES;
+                    const uint32_t bhi = st + 4 * TILE_BYTES, blo = st + 6 * TILE_BYTES;
+#pragma unroll
+                    for (int j = 0; j < KT / 16; ++j) {
+                        const uint32_t o = j * 32;  // 16 bf16 along K
+                        const uint32_t first = (kt == 0 && j == 0) ? 0u : 1u;
+                        if (OUT_COMPLEX) {
+                            // [Dr | Di] += Ar * [Br | Bi]
+                            tc::mma_bf16(d, tc::sdesc_k64(arh + o), tc::sdesc_k64(bhi + o), I256, first);
+                            tc::mma_bf16(d, tc::sdesc_k64(arh + o), tc::sdesc_k64(blo + o), I256, 1);
+                            tc::mma_bf16(d, tc::sdesc_k64(arl + o), tc::sdesc_k64(bhi + o), I256, 1);
+                            if (A_COMPLEX) {
+                                // Dr -= Ai * Bi ; Di += Ai * Br
+                                tc::mma_bf16(d, tc::sdesc_k64(aih + o), tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
+                                tc::mma_bf16(d, tc::sdesc_k64(aih + o), tc::sdesc_k64(blo + TILE_BYTES + o), I128N, 1);
+                                tc::mma_bf16(d, tc::sdesc_k64(ail + o), tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
+                                tc::mma_bf16(d + 128, tc::sdesc_k64(aih + o), tc::sdesc_k64(bhi + o), I128, 1);
+                                tc::mma_bf16(d + 128, tc::sdesc_k64(aih + o), tc::sdesc_k64(blo + o), I128, 1);
+                                tc::mma_bf16(d + 128, tc::sdesc_k64(ail + o), tc::sdesc_k64(bhi + o), I128, 1);
+                            }
+                        } else {
+                            // Dr = Ar * Br - Ai * Bi
+                            tc::mma_bf16(d, tc::sdesc_k64(arh + o), tc::sdesc_k64(bhi + o), I128, first);
+                            tc::mma_bf16(d, tc::sdesc_k64(arh + o), tc::sdesc_k64(blo + o), I128, 1);
+                            tc::mma_bf16(d, tc::sdesc_k64(arl + o), tc::sdesc_k64(bhi + o), I128, 1);
+                            tc::mma_bf16(d, tc::sdesc_k64(aih + o), tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
+                            tc::mma_bf16(d, tc::sdesc_k64(aih + o), tc::sdesc_k64(blo + TILE_BYTES + o), I128N, 1);
+                            tc::mma_bf16(d, tc::sdesc_k64(ail + o), tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
+                        }
+                    }
+                    tc::mma_commit(&empty_bar[s]);  // frees the stage when these MMAs finish
+                    if (++s == STAGES) {
+                        s = 0;
+                        ph ^= 1u;
+                    }
+                }
+                tc::mma_commit(&acc_full[acc]);
+                if (++acc == 2) {
+                    acc = 0;
+                    acc_ph ^= 1u;
+                }
+            }
+        }
+    } else {
+        // ---------------- epilogue (warps 2..5) ----------------
+        const uint32_t q = warp & 3;  // TMEM lane quarter this warp may access
+        uint32_t acc = 0, acc_ph = 0;
+        for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+            const Tile T = tiles[t];
+            const Problem P = probs[T.problem];
+            const Group Gp = groups[P.group];
+            if (!tc::mbar_wait(&acc_full[acc], acc_ph, err)) {
+                abort_flag = 1;
+                break;
+            }
+            tc::tc_fence_after();
+            const uint32_t m = T.mt * MT + q * 32 + lane;  // this thread's row
+            const uint32_t d = tmem + acc * 256 + ((q * 32u) << 16);
+            for (uint32_t c0 = 0; c0 < (uint32_t)NT; c0 += 32) {
+                float vr[32], vi[32];
+                tc::tmem_ld32(d + c0, vr);
+                if (OUT_COMPLEX) tc::tmem_ld32(d + 128 + c0, vi);
+                if (m >= P.M) continue;
+                const uint32_t nb = T.nt * NT + c0;
+                if (STAGE == ST_R) {
+                    // row m = (inst, y) ; col = kx -> B operand of C: row (inst, kx), k = y
+                    const uint32_t il = m / Gp.Y, y = m - il * Gp.Y;
+                    const size_t plane = (size_t)Gp.rowsC * Gp.kpC;
+                    bf16 *o = Gp.bC + (size_t)(il * Gp.N1h + nb) * Gp.kpC + y;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        if (nb + j < Gp.N1h) {
+                            split_store(o, o + plane, vr[j]);
+                            split_store(o + 2 * plane, o + 3 * plane, vi[j]);
+                        }
+                        o += Gp.kpC;
+                    }
+                } else if (STAGE == ST_C) {
+                    // row m = ky ; col = (inst, kx) -> B operand of C^-1: row (inst, f, kx), k = ky
+                    const size_t plane = (size_t)Gp.rowsCi * Gp.kpCi;
+                    uint32_t il = nb / Gp.N1h, kx = nb - il * Gp.N1h;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        if (il < Gp.G) {
+                            const float kxs = __ldg(Gp.kxs + (size_t)kx * Gp.N2 + m);
+                            const float kys = __ldg(Gp.kys + (size_t)kx * Gp.N2 + m);
+                            const float br = vr[j], bi = vi[j];
+                            bf16 *ox = Gp.bCi + (size_t)(il * 2 * Gp.N1h + kx) * Gp.kpCi + m;
+                            bf16 *oy = ox + (size_t)Gp.N1h * Gp.kpCi;
+                            split_store(ox, ox + plane, -bi * kxs);
+                            split_store(ox + 2 * plane, ox + 3 * plane, br * kxs);
+                            split_store(oy, oy + plane, -bi * kys);
+                            split_store(oy + 2 * plane, oy + 3 * plane, br * kys);
+                        }
+                        if (++kx == Gp.N1h) {
+                            kx = 0;
+                            ++il;
+                        }
+                    }
+                } else if (STAGE == ST_CI) {
+                    // row m = y ; col = (inst, f, kx) -> A operand of R^-1: row (inst, f, y), k = kx
+                    const size_t plane = (size_t)Gp.rowsRi * Gp.kpRi;
+                    uint32_t il = nb / (2 * Gp.N1h), rem = nb - il * 2 * Gp.N1h;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        if (il < Gp.G) {
+                            const uint32_t f = rem >= Gp.N1h ? 1u : 0u, kx = rem - f * Gp.N1h;
+                            bf16 *o = Gp.aRi + (size_t)((il * 2 + f) * Gp.Y + m) * Gp.kpRi + kx;
+                            split_store(o, o + plane, vr[j]);
+                            split_store(o + 2 * plane, o + 3 * plane, vi[j]);
+                        }
+                        if (++rem == 2 * Gp.N1h) {
+                            rem = 0;
+                            ++il;
+                        }
+                    }
+                } else {
+                    // row m = (inst, f, y) ; col = x -> g_f[y * X + x], masked
+                    const uint32_t il = m / (2 * Gp.Y), r2 = m - il * 2 * Gp.Y;
+                    const uint32_t f = r2 >= Gp.Y ? 1u : 0u, y = r2 - f * Gp.Y;
+                    const uint32_t inst = Gp.inst0 + il;
+                    const InstIO io = (io0_active && inst == 0) ? io0 : ios[inst];
+                    float *out = (f ? io.gy : io.gx) + (size_t)y * Gp.X;
+                    const uint32_t *mask = io.mask + (size_t)y * Gp.X;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const uint32_t x = nb + j;
+                        if (x < Gp.X) out[x] = __ldg(mask + x) != 0u ? vr[j] : 0.0f;
+                    }
+                }
+            }
+            tc::tc_fence_before();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(&acc_empty[acc]);
+            if (++acc == 2) {
+                acc = 0;
+                acc_ph ^= 1u;
+            }
+        }
+    }
+    tc::tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc::tc_fence_after();
+        tc::tmem_dealloc(tmem, 512);
+    }
+}
+
+// ---- per-solve input preparation: mass rows -> A operand of stage R --------
+struct PrepRef {
+    uint32_t group, row;  // row = inst_local * Y + y
+};
+
+__global__ void prep_mass(const Group *__restrict__ groups, const PrepRef *__restrict__ refs,
+                          const InstIO *__restrict__ ios, InstIO io0, int io0_active) {
+    const PrepRef r = refs[blockIdx.x];
+    const Group Gp = groups[r.group];
+    const uint32_t il = r.row / Gp.Y, y = r.row - il * Gp.Y, inst = Gp.inst0 + il;
+    const InstIO io = (io0_active && inst == 0) ? io0 : ios[inst];
+    const size_t plane = (size_t)Gp.rowsR * Gp.kpR;
+    bf16 *o = Gp.aR + (size_t)r.row * Gp.kpR;
+    for (uint32_t x = threadIdx.x; x < Gp.X; x += blockDim.x) {
+        size_t c = (size_t)y * Gp.X + x;
+        float v = 0.0f;
+        if (__ldg(io.mask + c) != 0u) v = io.mass_f ? __ldg(io.mass_f + c) : (float)__ldg(io.mass_i + c) * io.inv;
+        split_store(o + x, o + plane + x, v);
+    }
+}
+
+// ---- FP64 precompute ---------------------------------------------------------
+__device__ __forceinline__ void split_store_d(bf16 *hi, bf16 *lo, double v) {
+    bf16 h = __double2bfloat16(v);
+    *hi = h;
+    *lo = __double2bfloat16(v - (double)__bfloat162float(h));
+}
+
+// Complex DFT matrix into 4 planes: rows r < rows, k < kvalid,
+// value = w(k) * exp(sign * 2 pi i * (r * k mod n) / n). `weights` = 1 gives
+// the Hermitian weights w = 1 (k == 0 or 2k == n) else 2 (on k).
+__global__ void dft_matrix(bf16 *out, uint32_t rows, uint32_t kvalid, uint32_t kpitch, uint32_t n, int sign,
+                           int weights) {
+    size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (size_t)rows * kvalid) return;
+    uint32_t r = (uint32_t)(id / kvalid), k = (uint32_t)(id - (size_t)r * kvalid);
+    uint64_t t = ((uint64_t)r * k) % n;
+    double s, c;
+    sincospi(2.0 * (double)t / (double)n, &s, &c);
+    double w = 1.0;
+    if (weights) w = (k == 0 || 2 * k == n) ? 1.0 : 2.0;
+    const size_t plane = (size_t)rows * kpitch, e = (size_t)r * kpitch + k;
+    split_store_d(out + e, out + plane + e, w * c);
+    split_store_d(out + 2 * plane + e, out + 3 * plane + e, w * (double)sign * s);
+}
+
+// Imaginary parts of the x/y kernel spectra, first over x:
+// tx[j][kx] = sum_dx Kx(dx, dy_j) sin(2 pi kx dx / N1), ty = sum_dx Ky cos(..),
+// with K(d) = scale * d / |d|^3, d folded into (-N/2, N/2) (the +N/2 offset
+// is never used by the linear convolution and is left out, which makes Kx
+// exactly odd in x and Ky exactly odd in y).
+__global__ void spectra_x(double *tx, double *ty, uint32_t N1, uint32_t N2, uint32_t N1h, double scale) {
+    size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (size_t)N2 * N1h) return;
+    uint32_t j = (uint32_t)(id / N1h), kx = (uint32_t)(id - (size_t)j * N1h);
+    if (2 * j == N2) {
+        tx[id] = 0.0;
+        ty[id] = 0.0;
+        return;
+    }
+    double dy = 2 * j < N2 ? (double)j : (double)j - (double)N2;
+    double sx = 0.0, sy = 0.0;
+    for (uint32_t dxi = 0; dxi < N1; ++dxi) {
+        if (2 * dxi == N1) continue;
+        double dx = 2 * dxi < N1 ? (double)dxi : (double)dxi - (double)N1;
+        if (dx == 0.0 && dy == 0.0) continue;
+        double r2 = dx * dx + dy * dy, d = sqrt(r2);
+        double inv = scale / (r2 * d);
+        uint64_t t = ((uint64_t)kx * dxi) % N1;
+        double s, c;
+        sincospi(2.0 * (double)t / (double)N1, &s, &c);
+        sx += dx * inv * s;
+        sy += dy * inv * c;
+    }
+    tx[id] = sx;
+    ty[id] = sy;
+}
+
+// then over y: kxs = -sum_j tx[j] cos(2 pi ky j / N2), kys = -sum_j ty[j] sin(..)
+__global__ void spectra_y(const double *tx, const double *ty, float *kxs, float *kys, uint32_t N2, uint32_t N1h) {
+    size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (size_t)N2 * N1h) return;
+    uint32_t ky = (uint32_t)(id / N1h), kx = (uint32_t)(id - (size_t)ky * N1h);
+    double ax = 0.0, ay = 0.0;
+    for (uint32_t j = 0; j < N2; ++j) {
+        uint64_t t = ((uint64_t)ky * j) % N2;
+        double s, c;
+        sincospi(2.0 * (double)t / (double)N2, &s, &c);
+        ax += tx[(size_t)j * N1h + kx] * c;
+        ay += ty[(size_t)j * N1h + kx] * s;
+    }
+    kxs[(size_t)kx * N2 + ky] = (float)(-ax);
+    kys[(size_t)kx * N2 + ky] = (float)(-ay);
+}
+
+// ---- host ---------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+static uint32_t round_up(uint32_t v, uint32_t m) { return (v + m - 1) / m * m; }
+
+struct HostGroup {
+    Group g;
+    bf16 *f1 = nullptr, *f2 = nullptr, *g2 = nullptr, *g1 = nullptr;
+    uint32_t kpF1 = 0, kpF2 = 0, kpG2 = 0, kpG1 = 0;
+    float *kxs = nullptr;
+    double flops = 0;  // executed tensor flops of one solve of the group
+};
+
+struct DftImpl {
+    std::vector<JobShape> shapes;
+    std::vector<HostGroup> hg;
+    std::vector<void *> allocs;
+    Group *groups = nullptr;
+    InstIO *ios = nullptr;
+    std::vector<InstIO> ios_host;
+    std::vector<uint32_t> inst_group, inst_local;
+    CUtensorMap *tmaps = nullptr;
+    Problem *probs = nullptr;
+    Tile *tiles[4] = {};
+    uint32_t ntiles[4] = {};
+    PrepRef *prep = nullptr;
+    uint32_t nprep = 0;
+    uint32_t grid[4] = {};
+    double flops = 0;
+    uint32_t *err = nullptr;  // device address of g_dft_err
+    ~DftImpl() {
+        for (void *p : allocs) cudaFree(p);
+    }
+    template <typename T> int alloc(T **p, size_t n) {
+        void *q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+        if (e != cudaSuccess) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "split-BF16 gravity: allocation failed");
+        e = cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T));
+        if (e != cudaSuccess) TPT_FAIL(TPT_ERR_CUDA, "cudaMemset failed: %s", cudaGetErrorString(e));
+        allocs.push_back(q);
+        *p = static_cast<T *>(q);
+        return TPT_OK;
+    }
+};
+
+static int make_tmap(CUtensorMap *out, const bf16 *base, uint32_t kpitch, uint32_t rows_total) {
+    auto fn = encode_fn();
+    if (!fn) TPT_FAIL(TPT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available from the driver");
+    cuuint64_t dims[2] = {kpitch, rows_total};
+    cuuint64_t strides[1] = {(cuuint64_t)kpitch * 2};
+    cuuint32_t box[2] = {KT, MT};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) TPT_FAIL(TPT_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return TPT_OK;
+}
+
+static int init_attrs() {
+    static bool done = false;
+    if (done) return TPT_OK;
+    TPT_CUDA(cudaFuncSetAttribute(dft_gemm<ST_R>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    TPT_CUDA(cudaFuncSetAttribute(dft_gemm<ST_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    TPT_CUDA(cudaFuncSetAttribute(dft_gemm<ST_CI>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    TPT_CUDA(cudaFuncSetAttribute(dft_gemm<ST_RI>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    done = true;
+    return TPT_OK;
+}
+
 int DftSet::create(const std::vector<JobShape> &shapes) {
-    (void)shapes;
-    TPT_FAIL(TPT_ERR_UNSUPPORTED, "split-BF16 gravity is not available in this build");
+    destroy();
+    int rc = init_attrs();
+    if (rc) return rc;
+    if (!encode_fn()) TPT_FAIL(TPT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available from the driver");
+    DftImpl *I = new (std::nothrow) DftImpl();
+    if (!I) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "host allocation failed");
+    impl = I;
+    I->shapes = shapes;
+    TPT_CUDA(cudaGetSymbolAddress((void **)&I->err, g_dft_err));
+    const uint32_t n = (uint32_t)shapes.size();
+    // group instances by shape, keeping first-seen order
+    std::map<std::pair<uint32_t, uint32_t>, uint32_t> gid;
+    std::vector<std::vector<uint32_t>> members;
+    for (uint32_t i = 0; i < n; ++i) {
+        auto key = std::make_pair(shapes[i].X, shapes[i].Y);
+        auto it = gid.find(key);
+        if (it == gid.end()) {
+            gid[key] = (uint32_t)members.size();
+            members.push_back({});
+            it = gid.find(key);
+        }
+        members[it->second].push_back(i);
+    }
+    // instance order = grouped order; instance IO table is indexed by the
+    // position in that order (inst0 + local)
+    std::vector<uint32_t> order;
+    for (auto &mv : members) order.insert(order.end(), mv.begin(), mv.end());
+    I->inst_group.resize(n);
+    I->inst_local.resize(n);
+    I->hg.resize(members.size());
+    uint32_t inst0 = 0;
+    for (size_t gi = 0; gi < members.size(); ++gi) {
+        HostGroup &H = I->hg[gi];
+        Group &g = H.g;
+        g.X = shapes[members[gi][0]].X;
+        g.Y = shapes[members[gi][0]].Y;
+        g.N1 = 2 * g.X;
+        g.N2 = 2 * g.Y;
+        g.N1h = g.N1 / 2 + 1;
+        g.G = (uint32_t)members[gi].size();
+        g.inst0 = inst0;
+        for (uint32_t l = 0; l < g.G; ++l) {
+            I->inst_group[members[gi][l]] = (uint32_t)gi;
+            I->inst_local[members[gi][l]] = inst0 + l;
+        }
+        inst0 += g.G;
+        g.kpR = round_up(g.X, KT);
+        g.kpC = round_up(g.Y, KT);
+        g.kpCi = round_up(g.N2, KT);
+        g.kpRi = round_up(g.N1h, KT);
+        g.rowsR = g.G * g.Y;
+        g.rowsC = g.G * g.N1h;
+        g.rowsCi = 2 * g.G * g.N1h;
+        g.rowsRi = 2 * g.G * g.Y;
+        H.kpF1 = g.kpR;   // F1: N1h rows, K = x
+        H.kpF2 = g.kpC;   // F2: N2 rows, K = y
+        H.kpG2 = g.kpCi;  // G2: Y rows, K = ky
+        H.kpG1 = g.kpRi;  // G1: X rows, K = kx
+        if ((rc = I->alloc(&g.aR, (size_t)2 * g.rowsR * g.kpR))) return rc;
+        if ((rc = I->alloc(&g.bC, (size_t)4 * g.rowsC * g.kpC))) return rc;
+        if ((rc = I->alloc(&g.bCi, (size_t)4 * g.rowsCi * g.kpCi))) return rc;
+        if ((rc = I->alloc(&g.aRi, (size_t)4 * g.rowsRi * g.kpRi))) return rc;
+        if ((rc = I->alloc(&H.f1, (size_t)4 * g.N1h * H.kpF1))) return rc;
+        if ((rc = I->alloc(&H.f2, (size_t)4 * g.N2 * H.kpF2))) return rc;
+        if ((rc = I->alloc(&H.g2, (size_t)4 * g.Y * H.kpG2))) return rc;
+        if ((rc = I->alloc(&H.g1, (size_t)4 * g.X * H.kpG1))) return rc;
+        if ((rc = I->alloc(&H.kxs, (size_t)2 * g.N2 * g.N1h))) return rc;
+        g.kxs = H.kxs;
+        g.kys = H.kxs + (size_t)g.N2 * g.N1h;
+        // constants in FP64, rounded once to the hi/lo planes
+        auto blocks = [](size_t cnt) { return (unsigned)((cnt + 255) / 256); };
+        dft_matrix<<<blocks((size_t)g.N1h * g.X), 256>>>(H.f1, g.N1h, g.X, H.kpF1, g.N1, -1, 0);
+        dft_matrix<<<blocks((size_t)g.N2 * g.Y), 256>>>(H.f2, g.N2, g.Y, H.kpF2, g.N2, -1, 0);
+        dft_matrix<<<blocks((size_t)g.Y * g.N2), 256>>>(H.g2, g.Y, g.N2, H.kpG2, g.N2, +1, 0);
+        dft_matrix<<<blocks((size_t)g.X * g.N1h), 256>>>(H.g1, g.X, g.N1h, H.kpG1, g.N1, +1, 1);
+        for (int k = 0; k < 4; ++k) count_launch();
+        double *tx = nullptr;
+        TPT_CUDA(cudaMalloc(&tx, (size_t)2 * g.N2 * g.N1h * sizeof(double)));
+        const double scale = -(double)6.673e-1f / ((double)g.N1 * (double)g.N2);
+        spectra_x<<<blocks((size_t)g.N2 * g.N1h), 256>>>(tx, tx + (size_t)g.N2 * g.N1h, g.N1, g.N2, g.N1h, scale);
+        spectra_y<<<blocks((size_t)g.N2 * g.N1h), 256>>>(tx, tx + (size_t)g.N2 * g.N1h, H.kxs,
+                                                         H.kxs + (size_t)g.N2 * g.N1h, g.N2, g.N1h);
+        count_launch();
+        count_launch();
+        cudaError_t e = cudaDeviceSynchronize();
+        cudaFree(tx);
+        if (e != cudaSuccess) TPT_FAIL(TPT_ERR_CUDA, "split-BF16 precompute failed: %s", cudaGetErrorString(e));
+        // executed tensor flops (3-term split, padded tiles)
+        auto tiles_of = [](uint32_t v, uint32_t t) { return (double)((v + t - 1) / t) * t; };
+        double fR = 2.0 * tiles_of(g.rowsR, MT) * tiles_of(g.N1h, NT) * 2 * g.kpR * 3;
+        double fC = 2.0 * tiles_of(g.N2, MT) * tiles_of(g.rowsC, NT) * 4 * g.kpC * 3;
+        double fCi = 2.0 * tiles_of(g.Y, MT) * tiles_of(g.rowsCi, NT) * 4 * g.kpCi * 3;
+        double fRi = 2.0 * tiles_of(g.rowsRi, MT) * tiles_of(g.X, NT) * 2 * g.kpRi * 3;
+        H.flops = fR + fC + fCi + fRi;
+        I->flops += H.flops;
+    }
+    // device tables: groups, tensor maps, problems, tiles
+    const size_t ng = I->hg.size();
+    if ((rc = I->alloc(&I->groups, ng))) return rc;
+    std::vector<Group> gh(ng);
+    for (size_t gi = 0; gi < ng; ++gi) gh[gi] = I->hg[gi].g;
+    TPT_CUDA(cudaMemcpy(I->groups, gh.data(), ng * sizeof(Group), cudaMemcpyHostToDevice));
+    std::vector<CUtensorMap> tm(8 * ng);
+    std::vector<Problem> pr(4 * ng);
+    if ((rc = I->alloc(&I->tmaps, tm.size()))) return rc;
+    std::vector<Tile> tl[4];
+    std::vector<PrepRef> pref;
+    for (size_t gi = 0; gi < ng; ++gi) {
+        const HostGroup &H = I->hg[gi];
+        const Group &g = H.g;
+        CUtensorMap *tmd = I->tmaps + 8 * gi;
+        // stage R: A = aR (2 planes), B = F1
+        if ((rc = make_tmap(&tm[8 * gi + 0], g.aR, g.kpR, 2 * g.rowsR))) return rc;
+        if ((rc = make_tmap(&tm[8 * gi + 1], H.f1, H.kpF1, 4 * g.N1h))) return rc;
+        // stage C: A = F2, B = bC
+        if ((rc = make_tmap(&tm[8 * gi + 2], H.f2, H.kpF2, 4 * g.N2))) return rc;
+        if ((rc = make_tmap(&tm[8 * gi + 3], g.bC, g.kpC, 4 * g.rowsC))) return rc;
+        // stage C^-1: A = G2, B = bCi
+        if ((rc = make_tmap(&tm[8 * gi + 4], H.g2, H.kpG2, 4 * g.Y))) return rc;
+        if ((rc = make_tmap(&tm[8 * gi + 5], g.bCi, g.kpCi, 4 * g.rowsCi))) return rc;
+        // stage R^-1: A = aRi, B = G1
+        if ((rc = make_tmap(&tm[8 * gi + 6], g.aRi, g.kpRi, 4 * g.rowsRi))) return rc;
+        if ((rc = make_tmap(&tm[8 * gi + 7], H.g1, H.kpG1, 4 * g.X))) return rc;
+        const uint32_t gi32 = (uint32_t)gi;
+        pr[4 * gi + 0] = {tmd + 0, tmd + 1, gi32, g.rowsR, g.N1h, g.kpR / KT, g.rowsR, g.N1h};
+        pr[4 * gi + 1] = {tmd + 2, tmd + 3, gi32, g.N2, g.rowsC, g.kpC / KT, g.N2, g.rowsC};
+        pr[4 * gi + 2] = {tmd + 4, tmd + 5, gi32, g.Y, g.rowsCi, g.kpCi / KT, g.Y, g.rowsCi};
+        pr[4 * gi + 3] = {tmd + 6, tmd + 7, gi32, g.rowsRi, g.X, g.kpRi / KT, g.rowsRi, g.X};
+        for (int st = 0; st < 4; ++st) {
+            const Problem &P = pr[4 * gi + st];
+            // M tiles fastest so consecutive CTAs share the B tile (L2 reuse)
+            for (uint32_t nt = 0; nt * NT < P.N; ++nt)
+                for (uint32_t mt = 0; mt * MT < P.M; ++mt)
+                    tl[st].push_back({(uint32_t)(4 * gi + st), (uint16_t)mt, (uint16_t)nt});
+        }
+        for (uint32_t r = 0; r < g.rowsR; ++r) pref.push_back({gi32, r});
+    }
+    TPT_CUDA(cudaMemcpy(I->tmaps, tm.data(), tm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
+    if ((rc = I->alloc(&I->probs, pr.size()))) return rc;
+    TPT_CUDA(cudaMemcpy(I->probs, pr.data(), pr.size() * sizeof(Problem), cudaMemcpyHostToDevice));
+    int sms = 148, dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    for (int st = 0; st < 4; ++st) {
+        if ((rc = I->alloc(&I->tiles[st], tl[st].size()))) return rc;
+        TPT_CUDA(cudaMemcpy(I->tiles[st], tl[st].data(), tl[st].size() * sizeof(Tile), cudaMemcpyHostToDevice));
+        I->ntiles[st] = (uint32_t)tl[st].size();
+        I->grid[st] = std::min<uint32_t>(I->ntiles[st], (uint32_t)sms);
+    }
+    if ((rc = I->alloc(&I->prep, pref.size()))) return rc;
+    TPT_CUDA(cudaMemcpy(I->prep, pref.data(), pref.size() * sizeof(PrepRef), cudaMemcpyHostToDevice));
+    I->nprep = (uint32_t)pref.size();
+    I->ios_host.assign(n, InstIO{});
+    if ((rc = I->alloc(&I->ios, n))) return rc;
+    return TPT_OK;
 }
-void DftSet::dims(size_t, uint32_t *n1, uint32_t *n2) const {
-    *n1 = 0;
-    *n2 = 0;
+
+void DftSet::dims(size_t j, uint32_t *n1, uint32_t *n2) const {
+    const JobShape &s = impl->shapes[j];
+    *n1 = 2 * s.X;
+    *n2 = 2 * s.Y;
 }
-int DftSet::set_io(size_t, const SolveIO &) { TPT_FAIL(TPT_ERR_UNSUPPORTED, "split-BF16 gravity unavailable"); }
-int DftSet::launch(cudaStream_t, const SolveIO *) const {
-    TPT_FAIL(TPT_ERR_UNSUPPORTED, "split-BF16 gravity unavailable");
+
+int DftSet::set_io(size_t j, const SolveIO &io) {
+    DftImpl *I = impl;
+    uint32_t pos = I->inst_local[j];
+    I->ios_host[pos] = InstIO{io.mass_i, io.mass_f, io.mask, io.gx, io.gy, io.mass_scale_inv};
+    TPT_CUDA(cudaMemcpy(I->ios + pos, &I->ios_host[pos], sizeof(InstIO), cudaMemcpyHostToDevice));
+    return TPT_OK;
 }
-uint32_t DftSet::launches() const { return 0; }
-double DftSet::flops() const { return 0.0; }
+
+int DftSet::launch(cudaStream_t st, const SolveIO *io) const {
+    const DftImpl *I = impl;
+    InstIO io0{};
+    int act = 0;
+    if (io) {
+        io0 = InstIO{io->mass_i, io->mass_f, io->mask, io->gx, io->gy, io->mass_scale_inv};
+        act = 1;
+    }
+    uint32_t *err = I->err;
+    prep_mass<<<I->nprep, 128, 0, st>>>(I->groups, I->prep, I->ios, io0, act);
+    TPT_LAUNCHED();
+    dft_gemm<ST_R><<<I->grid[0], THREADS, SMEM_BYTES, st>>>(I->probs, I->tiles[0], I->ntiles[0], I->groups, I->ios,
+                                                            io0, act, err);
+    TPT_LAUNCHED();
+    dft_gemm<ST_C><<<I->grid[1], THREADS, SMEM_BYTES, st>>>(I->probs, I->tiles[1], I->ntiles[1], I->groups, I->ios,
+                                                            io0, act, err);
+    TPT_LAUNCHED();
+    dft_gemm<ST_CI><<<I->grid[2], THREADS, SMEM_BYTES, st>>>(I->probs, I->tiles[2], I->ntiles[2], I->groups, I->ios,
+                                                             io0, act, err);
+    TPT_LAUNCHED();
+    dft_gemm<ST_RI><<<I->grid[3], THREADS, SMEM_BYTES, st>>>(I->probs, I->tiles[3], I->ntiles[3], I->groups, I->ios,
+                                                             io0, act, err);
+    TPT_LAUNCHED();
+    return TPT_OK;
+}
+
+uint32_t DftSet::launches() const { return 5; }
+double DftSet::flops() const { return impl ? impl->flops : 0.0; }
+
 void DftSet::destroy() {
     delete impl;
     impl = nullptr;
+}
+
+// Reads and clears the device error word of the tensor-core kernels.
+int read_errors(uint32_t *out) {
+    uint32_t v = 0, z = 0;
+    TPT_CUDA(cudaMemcpyFromSymbol(&v, g_dft_err, sizeof(v)));
+    TPT_CUDA(cudaMemcpyToSymbol(g_dft_err, &z, sizeof(z)));
+    *out = v;
+    return TPT_OK;
 }
 
 }  // namespace dft

@@ -38,3 +38,10 @@ struct DftSet {
 
 }  // namespace dft
 }  // namespace tpt
+
+namespace tpt {
+namespace dft {
+// Reads and clears the device error word of the tensor-core kernels.
+int read_errors(uint32_t *out);
+}  // namespace dft
+}  // namespace tpt

@@ -47,7 +47,8 @@ EXPORTS = [
     "tpt_grav_plan_destroy", "tpt_grav_plan_dims", "tpt_grav_solve", "tpt_grav_solve_f32",
     "tpt_grav_mask_rebuild", "tpt_mass_to_fixed", "tpt_batch_create", "tpt_batch_destroy", "tpt_batch_fields",
     "tpt_batch_write", "tpt_batch_read", "tpt_batch_step", "tpt_batch_tune", "tpt_batch_get_tuning",
-    "tpt_batch_set_tuning", "tpt_batch_profile_phases", "tpt_last_error_string", "tpt_kernel_launch_count", "tpt_version",
+    "tpt_batch_set_tuning", "tpt_batch_profile_phases", "tpt_check_device_errors", "tpt_last_error_string",
+    "tpt_kernel_launch_count", "tpt_version",
 ]
 
 
