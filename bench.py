@@ -194,6 +194,39 @@ def cpu_rate(insts, target_s: float, threads: int | None = None):
 
 # ------------------------------------------------------------------ ours --
 
+def run_plain(ticks: int):
+    """The plain FP32 single-instance form: one 400x225 grid (C2) stepped
+    through the reference-shaped calls, step_air_gpu + GravityFft.solve
+    (FP32) once per tick, stream ordered, no graph. Device time, inputs
+    resident. Returns (cell-ticks/s, ms per tick)."""
+    import torch
+
+    import tpt_field as tf
+    import workloads as W
+
+    inst = W.config_instances(2)[0]
+    b = tf.SimBuffers.from_instance(inst)
+    solver = tf.GravityFft(tf.PRECISION_FP32)
+    stream = torch.cuda.current_stream()
+
+    def tick():
+        tf.step_air_gpu(b, stream)
+        solver.solve(b, b.grav_mass_prev, 1.0 / 65536.0, stream)
+
+    for _ in range(20):
+        tick()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(ticks):
+        tick()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    solver.close()
+    return inst.cells * ticks / (ms / 1e3), ms / ticks
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -292,6 +325,13 @@ def run_ours(args, rank, world, local):
     launches = (prof.air_launches_per_tick + prof.grav_launches_per_tick) * ticks * args.steps + \
         (args.steps if ticks % 2 else 0)
 
+    plain = None
+    if rank == 0 and world == 1 and args.plain_ticks > 0:
+        p_rate, p_ms = run_plain(args.plain_ticks)
+        plain = {"workload": WORKLOAD_NAMES[2] + ", one instance, step_air_gpu + GravityFft.solve per tick",
+                 "value": p_rate, "unit": "cell-ticks/s", "ms_per_tick": p_ms, "ticks": args.plain_ticks,
+                 "speedup_of_this_line": value / world / p_rate}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, desc = cpu_rate(insts, args.cpu_seconds)
@@ -314,6 +354,7 @@ def run_ours(args, rank, world, local):
             "roofline_phases": {"air": roof_air, "gravity": roof_grav, **phases},
             "clocks": clk,
             "cpu_baseline": cpu,
+            "plain_fp32_single_instance": plain,
         }
         print(json.dumps(line), flush=True)
     batch.close()
@@ -348,8 +389,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--workload", type=int, choices=(1, 2, 4, 5), default=4)
+    ap.add_argument("--workload", type=int, choices=(1, 2, 4, 5), default=5)
     ap.add_argument("--ticks", type=int, default=0)
+    ap.add_argument("--plain-ticks", type=int, default=500, help="ticks of the plain FP32 comparison (0 = skip)")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer run (profiling captures)")

@@ -232,9 +232,11 @@ typedef struct tpt_instance_desc {
     uint32_t newton_grav; /* 0/1: solve gravity every tick (config flag) */
 } tpt_instance_desc;
 
-/* Device pointers of one instance's grids inside a batch's arenas. The
- * layout of each grid is the reference's (`cy * xcells + cx`), so any
- * reference-layout kernel can read or edit them between steps. */
+/* Device pointers of one instance's grids inside a batch's arenas. Every
+ * grid has `ycells` rows of `pitch` elements (pitch = xcells rounded up to
+ * 32, so each row starts on a 128-byte boundary): cell (cx, cy) is at
+ * cy * pitch + cx. tpt_batch_write / tpt_batch_read convert from/to the
+ * reference's dense layout (`cy * xcells + cx`). */
 typedef struct tpt_instance_fields {
     float *pv, *vx, *vy, *hv;
     uint32_t *block_air, *block_airh, *wall_bmap, *wall_emap;
@@ -243,6 +245,7 @@ typedef struct tpt_instance_fields {
     int32_t *grav_mass;  /* fixed-point mass the solve reads            */
     uint32_t *grav_mask; /* gravity propagation mask                     */
     float *gx, *gy;      /* solve output                                 */
+    uint32_t pitch;      /* row stride of every grid above (elements)    */
 } tpt_instance_fields;
 
 /* Grid ids for tpt_batch_write / tpt_batch_read. */

@@ -1,5 +1,5 @@
-// air.cu -- launches of the air step (single grid and batched instances).
-// Compiled with -fmad=false: see air.cuh.
+// air.cu -- the one-grid air step (tpt_air_step and its static-scratch
+// variant). Compiled with -fmad=false: see air.cuh.
 #include <algorithm>
 #include <mutex>
 
@@ -9,27 +9,43 @@
 namespace tpt {
 namespace air {
 
-// Tile of a batched launch: instance index and tile origin in cells.
-__device__ __forceinline__ void tile_of(const TileRef *tiles, uint32_t t, uint32_t &inst, int &x0, int &y0) {
-    TileRef r = tiles[t];
-    inst = r.inst;
-    x0 = (int)r.tx * TX;
-    y0 = (int)r.ty * TY;
-}
-
-// ---- single grid: one CTA per tile, the instance by value -----------------
+// Pass A of one tile, staged by plain loads (the caller's grids may have any
+// row length, so no TMA).
 __global__ void __launch_bounds__(NT) k_pressure_velocity(const AirInst I) {
-    __shared__ SmemA S;
-    tile_pressure_velocity(I, blockIdx.x * TX, blockIdx.y * TY, S);
+    __shared__ LayoutA1 S;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    stage_flag<3>(S.b, I.bair, 0xFFFFFFFFu, I, x0, y0);
+    stage<float, 2>(S.vx, I.vx, I, x0, y0);
+    stage<float, 2>(S.vy, I.vy, I, x0, y0);
+    stage<float, 1>(S.pv, I.pv, I, x0, y0);
+    __syncthreads();
+    pass_a(I, x0, y0, S);
 }
 
+// Pass B of one tile.
 __global__ void __launch_bounds__(NT) k_advect_heat(const AirInst I) {
-    __shared__ SmemB S;
-    tile_advect_heat(I, blockIdx.x * TX, blockIdx.y * TY, S);
+    __shared__ LayoutB1 S;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    if (I.air_mode != 4u) {
+        stage_flag<3>(S.b, I.bair, 0xFFFFFFFFu, I, x0, y0);
+        stage<float, 3>(S.ovx, I.ovx, I, x0, y0);
+        stage<float, 3>(S.ovy, I.ovy, I, x0, y0);
+        stage<float, 2>(S.opv, I.opv, I, x0, y0);
+    } else {
+        stage<float, 1>(S.nvx, I.vx, I, x0, y0);
+        stage<float, 1>(S.nvy, I.vy, I, x0, y0);
+    }
+    if (I.aheat) {
+        stage_flag<1>(S.bh, I.bairh, 0x8u, I, x0, y0);
+        stage<float, 1>(S.hv, I.hv, I, x0, y0);
+    }
+    __syncthreads();
+    pass_b(I, x0, y0, S);
 }
 
 // Settle pass: new heat -> hv, NoUpdate convection -> vx/vy, wall masks
-// (settle.rs:50-93) and the optional HotAir pass (settle.rs:118-161).
+// (settle.rs:50-93) and the optional HotAir pass (settle.rs:118-161). The
+// grid is dense here (pitch == X).
 __global__ void k_settle(const AirInst I, const uint32_t *__restrict__ pmap, const uint32_t *__restrict__ props,
                          uint32_t nprops, uint32_t xres, uint32_t yres) {
     const size_t n = (size_t)I.X * I.Y;
@@ -85,105 +101,6 @@ int launch_single(const AirInst &I, const uint32_t *pmap, const uint32_t *props,
     size_t n = (size_t)I.X * I.Y;
     unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 16);
     k_settle<<<blocks, 256, 0, st>>>(I, pmap, props, nprops, xres, yres);
-    TPT_LAUNCHED();
-    return TPT_OK;
-}
-
-// ---- batched instances: persistent CTAs over a tile list ------------------
-__global__ void __launch_bounds__(NT) kb_pressure_velocity(const AirInst *__restrict__ insts,
-                                                           const TileRef *__restrict__ tiles, uint32_t ntiles,
-                                                           uint32_t parity) {
-    __shared__ SmemA S;
-    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        uint32_t i;
-        int x0, y0;
-        tile_of(tiles, t, i, x0, y0);
-        AirInst I = insts[2 * i + parity];
-        if (I.air_mode == 4u) continue;
-        tile_pressure_velocity(I, x0, y0, S);
-        __syncthreads();
-    }
-}
-
-// The batched B pass also rebuilds the masks of its tile into the other
-// half of the mask ping-pong (read by the next tick), so a tick is two
-// launches. The heat result goes to the other half of the hv ping-pong.
-__global__ void __launch_bounds__(NT) kb_advect_heat(const AirInst *__restrict__ insts,
-                                                     const TileRef *__restrict__ tiles, uint32_t ntiles,
-                                                     uint32_t parity) {
-    __shared__ SmemB S;
-    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        uint32_t i;
-        int x0, y0;
-        tile_of(tiles, t, i, x0, y0);
-        const AirInst I = insts[2 * i + parity];
-        if (I.air_mode != 4u || I.aheat) tile_advect_heat(I, x0, y0, S);
-        const int gx = x0 + (int)(threadIdx.x % TX), gy = y0 + (int)(threadIdx.x / TX);
-        if (in_grid(gx, gy, I)) {
-            size_t g = (size_t)gy * I.X + gx;
-            uint32_t ba, bh;
-            masks_cell(I, g, ba, bh);
-            I.bair_out[g] = ba;
-            I.bairh_out[g] = bh;
-            if (!I.aheat && I.hv_out != I.hv) I.hv_out[g] = I.hv[g];
-        }
-        __syncthreads();
-    }
-}
-
-// NoUpdate + ambient heat writes its convected velocity to ovx/ovy; a batch
-// with such an instance copies it back after the B pass.
-__global__ void kb_noupdate_settle(const AirInst *__restrict__ insts, const TileRef *__restrict__ tiles,
-                                   uint32_t ntiles, uint32_t parity) {
-    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        uint32_t i;
-        int x0, y0;
-        tile_of(tiles, t, i, x0, y0);
-        const AirInst I = insts[2 * i + parity];
-        if (!(I.air_mode == 4u && I.aheat)) continue;
-        const int gx = x0 + (int)(threadIdx.x % TX), gy = y0 + (int)(threadIdx.x / TX);
-        if (in_grid(gx, gy, I)) {
-            size_t g = (size_t)gy * I.X + gx;
-            I.vx[g] = I.ovx[g];
-            I.vy[g] = I.ovy[g];
-        }
-    }
-}
-
-int launch_batch_tick(const AirInst *insts, const TileRef *tiles, uint32_t ntiles, uint32_t grid, uint32_t parity,
-                      bool any_noupdate_heat, cudaStream_t st) {
-    kb_pressure_velocity<<<grid, NT, 0, st>>>(insts, tiles, ntiles, parity);
-    TPT_LAUNCHED();
-    kb_advect_heat<<<grid, NT, 0, st>>>(insts, tiles, ntiles, parity);
-    TPT_LAUNCHED();
-    if (any_noupdate_heat) {
-        kb_noupdate_settle<<<grid, NT, 0, st>>>(insts, tiles, ntiles, parity);
-        TPT_LAUNCHED();
-    }
-    return TPT_OK;
-}
-
-// Copies the ping-pong halves that hold the newest state back to the
-// instance's canonical buffers (after an odd number of ticks).
-__global__ void kb_copy_back(const AirInst *__restrict__ insts, const TileRef *__restrict__ tiles, uint32_t ntiles) {
-    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-        uint32_t i;
-        int x0, y0;
-        tile_of(tiles, t, i, x0, y0);
-        const AirInst C = insts[2 * i + 0];  // parity 0 reads canonical
-        const AirInst O = insts[2 * i + 1];  // parity 1 reads the other half
-        const int gx = x0 + (int)(threadIdx.x % TX), gy = y0 + (int)(threadIdx.x / TX);
-        if (in_grid(gx, gy, C)) {
-            size_t g = (size_t)gy * C.X + gx;
-            C.hv[g] = O.hv[g];
-            C.bair[g] = O.bair[g];
-            C.bairh[g] = O.bairh[g];
-        }
-    }
-}
-
-int launch_copy_back(const AirInst *insts, const TileRef *tiles, uint32_t ntiles, uint32_t grid, cudaStream_t st) {
-    kb_copy_back<<<grid, NT, 0, st>>>(insts, tiles, ntiles);
     TPT_LAUNCHED();
     return TPT_OK;
 }

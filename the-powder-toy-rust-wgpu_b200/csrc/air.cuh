@@ -2,25 +2,30 @@
 //
 // The arithmetic restates the reference kernels operation by operation
 // (crates/tpt-sim/src/air_kernel/pressure.rs, advect.rs, heat.rs, settle.rs)
-// and this file is compiled with -fmad=false, so every f32 operation is
-// rounded separately exactly as in the reference's source: the FP32 results
-// are bit-identical to the CPU restatement of those kernels.
+// and the files that include it are compiled with -fmad=false, so every f32
+// operation is rounded separately exactly as in the reference's source: the
+// FP32 results are bit-identical to the CPU restatement of those kernels.
 //
-// The seven reference launches become two tile kernels and a settle pass:
+// The seven reference launches become two tile passes and a settle pass:
 //
-//   A  pressure + velocity   (pressure.rs:173-299)
-//      tile + 3-cell halo of block_air, + 2 of vx/vy, + 1 of pv staged in
-//      shared memory; effective velocities on the +2 ring, pressure on the
-//      +1 ring, velocity on the tile. Writes opv/ovx/ovy.
-//   B  smooth/advect/vorticity/fans (advect.rs:174-360) on the tile + 1
-//      ring, then ambient heat + convection (heat.rs:31-253) on the tile.
-//      The far-advection walks and bilinear samples read global memory
-//      (read-only in this launch). Writes vx/vy/pv and the new heat.
+//   A  pressure + velocity   (pressure.rs:173-299): effective velocities on
+//      the tile's +2 ring, pressure on the +1 ring, velocity on the tile.
+//      Needs block_air with a 3-cell halo, vx/vy with 2, pv with 1.
+//   B  smooth/advect/vorticity/fans (advect.rs:174-360) on the tile's +1
+//      ring (vorticity precomputed on the +2 ring), then ambient heat and
+//      convection (heat.rs:31-253) on the tile. Needs ovx/ovy and block_air
+//      with a 3-cell halo, opv with 2, hv and block_airh with 1. The
+//      far-advection walks and bilinear samples read global memory.
 //   S  settle: heat copy-back (settle.rs:21-27), wall masks (settle.rs:
 //      50-93) and HotAir (settle.rs:118-161), elementwise.
 //
 // The one global dependency of a tick is between A and B: the far-advection
 // sample can reach any cell of ovx/ovy (0.7*|v| <= 179 cells).
+//
+// The tile code is written once over a shared-memory layout policy `L`:
+// the single-grid kernels stage each array with its own halo (Reg<H>); the
+// batched kernels stage every array as one TMA box of the tile plus a
+// 4-cell (x) by 3-cell (y) halo.
 #pragma once
 
 #include "common.cuh"
@@ -30,14 +35,23 @@ namespace air {
 
 constexpr int TX = AIR_TX, TY = AIR_TY, NT = TX * TY;
 
-// Shared-memory region of the tile plus an H-cell halo.
+// Tile plus an H-cell halo on every side.
 template <int H> struct Reg {
     static constexpr int W = TX + 2 * H;
     static constexpr int HGT = TY + 2 * H;
     static constexpr int N = W * HGT;
-    // (gx, gy) global -> flat index; caller guarantees it is in the region.
     __device__ static __forceinline__ int at(int gx, int gy, int x0, int y0) {
         return (gy - y0 + H) * W + (gx - x0 + H);
+    }
+};
+
+// The TMA box of the batched kernels: x halo 4 (keeps the box start 16-byte
+// aligned), y halo 3.
+struct Box {
+    static constexpr int HX = 4, HY = 3, W = TX + 2 * HX, HGT = TY + 2 * HY, N = W * HGT;
+    static constexpr int NP = (N + 31) / 32 * 32;  // array stride: TMA destinations are 128-byte aligned
+    __device__ static __forceinline__ int at(int gx, int gy, int x0, int y0) {
+        return (gy - y0 + HY) * W + (gx - x0 + HX);
     }
 };
 
@@ -54,41 +68,111 @@ __device__ __forceinline__ bool interior(uint32_t x, uint32_t y, uint32_t X, uin
     return x >= 1u && y >= 1u && x + 1u < X && y + 1u < Y;
 }
 
-// Staged block_air (nonzero test only) with a 3-cell halo; out-of-grid = 0,
-// which is what `blocked_at` returns there (pressure.rs:30-36).
-struct BlockView {
-    const uint8_t *s;
-    int x0, y0;
-    __device__ __forceinline__ bool at(int x, int y) const { return s[Reg<3>::at(x, y, x0, y0)] != 0; }
+// mod.rs:92-102 (compare and assign; keeps NaN and -0 as the reference does).
+__device__ __forceinline__ float clampf(float v, float lo, float hi) {
+    float out = v;
+    if (out < lo) out = lo;
+    if (out > hi) out = hi;
+    return out;
+}
+
+// Smoothing weight of tap (dx, dy) (advect.rs:215-225).
+__device__ __forceinline__ float smooth_w(int dx, int dy) {
+    float w = 0.01831564f;
+    if (dx == 1) w = 0.13533528f;
+    if (dy == 1) w = 0.13533528f;
+    if (dx == 1 && dy == 1) w = 1.0f;
+    return w;
+}
+
+// ---- shared-memory layouts ---------------------------------------------------
+// Pass A working set. `vx`/`vy` hold the raw velocity, then the effective
+// velocity; `pv` the raw pressure; `opv` the new pressure.
+struct LayoutA1 {  // single grid: per-array halos, masks as flags
+    uint8_t b[Reg<3>::N];
+    float vx[Reg<2>::N], vy[Reg<2>::N];
+    float pv[Reg<1>::N], opv[Reg<1>::N];
+    __device__ __forceinline__ bool blk(int x, int y, int x0, int y0) const { return b[Reg<3>::at(x, y, x0, y0)] != 0; }
+    __device__ __forceinline__ float &VX(int x, int y, int x0, int y0) { return vx[Reg<2>::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &VY(int x, int y, int x0, int y0) { return vy[Reg<2>::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float PV(int x, int y, int x0, int y0) const { return pv[Reg<1>::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &OPV(int x, int y, int x0, int y0) { return opv[Reg<1>::at(x, y, x0, y0)]; }
 };
 
-// pressure.rs:43-62
-__device__ __forceinline__ bool wall_cleared_vx(const BlockView &b, uint32_t x, uint32_t y, uint32_t X, uint32_t Y) {
-    bool out = false;
-    if (y >= 1u && y + 1u < Y) {
-        if (x >= 1u && x + 1u < X && b.at(x, y)) out = true;
-        if (x >= 2u && b.at((int)x - 1, y)) out = true;
-        if (x + 2u < X && b.at((int)x + 1, y)) out = true;
-    }
-    return out;
-}
-// pressure.rs:65-85
-__device__ __forceinline__ bool wall_cleared_vy(const BlockView &b, uint32_t x, uint32_t y, uint32_t X, uint32_t Y) {
-    bool out = false;
-    if (x >= 1u && x + 1u < X) {
-        if (y >= 1u && y + 1u < Y && b.at(x, y)) out = true;
-        if (y >= 2u && b.at(x, (int)y - 1)) out = true;
-        if (y + 2u < Y && b.at(x, (int)y + 1)) out = true;
-    }
-    return out;
-}
+struct __align__(128) BoxA {  // batched: one TMA box per array
+    float pv[Box::NP];
+    float vx[Box::NP];
+    float vy[Box::NP];
+    uint32_t b[Box::NP];
+};
+struct LayoutA2 {
+    BoxA *in;
+    float *opv;  // Box::N
+    __device__ __forceinline__ bool blk(int x, int y, int x0, int y0) const { return in->b[Box::at(x, y, x0, y0)] != 0u; }
+    __device__ __forceinline__ float &VX(int x, int y, int x0, int y0) { return in->vx[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &VY(int x, int y, int x0, int y0) { return in->vy[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float PV(int x, int y, int x0, int y0) const { return in->pv[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &OPV(int x, int y, int x0, int y0) { return opv[Box::at(x, y, x0, y0)]; }
+};
 
+// Pass B working set: staged ovx/ovy/opv/hv, the two masks, and the
+// computed vorticity (+2 ring) and smoothed/advected velocity and pressure
+// (+1 ring).
+struct LayoutB1 {
+    uint8_t b[Reg<3>::N];
+    uint8_t bh[Reg<1>::N];
+    float ovx[Reg<3>::N], ovy[Reg<3>::N];
+    float opv[Reg<2>::N];
+    float hv[Reg<1>::N];
+    float vort[Reg<2>::N];
+    float nvx[Reg<1>::N], nvy[Reg<1>::N], npv[Reg<1>::N];
+    __device__ __forceinline__ bool blk(int x, int y, int x0, int y0) const { return b[Reg<3>::at(x, y, x0, y0)] != 0; }
+    __device__ __forceinline__ bool hblk(int x, int y, int x0, int y0) const { return bh[Reg<1>::at(x, y, x0, y0)] != 0; }
+    __device__ __forceinline__ float OVX(int x, int y, int x0, int y0) const { return ovx[Reg<3>::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float OVY(int x, int y, int x0, int y0) const { return ovy[Reg<3>::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float OPV(int x, int y, int x0, int y0) const { return opv[Reg<2>::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float HV(int x, int y, int x0, int y0) const { return hv[Reg<1>::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &VORT(int x, int y, int x0, int y0) { return vort[Reg<2>::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &NVX(int x, int y, int x0, int y0) { return nvx[Reg<1>::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &NVY(int x, int y, int x0, int y0) { return nvy[Reg<1>::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &NPV(int x, int y, int x0, int y0) { return npv[Reg<1>::at(x, y, x0, y0)]; }
+};
+
+struct __align__(128) BoxB {  // batched: one TMA box per array
+    float ovx[Box::NP];  // ovx (or vx when the pressure/velocity pass is off)
+    float ovy[Box::NP];
+    float opv[Box::NP];
+    float hv[Box::NP];
+    uint32_t b[Box::NP];
+    uint32_t bh[Box::NP];
+};
+struct WorkB2 {
+    float vort[Box::N], nvx[Box::N], nvy[Box::N], npv[Box::N];
+};
+struct LayoutB2 {
+    BoxB *in;
+    WorkB2 *w;
+    __device__ __forceinline__ bool blk(int x, int y, int x0, int y0) const { return in->b[Box::at(x, y, x0, y0)] != 0u; }
+    __device__ __forceinline__ bool hblk(int x, int y, int x0, int y0) const {
+        return (in->bh[Box::at(x, y, x0, y0)] & 0x8u) != 0u;
+    }
+    __device__ __forceinline__ float OVX(int x, int y, int x0, int y0) const { return in->ovx[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float OVY(int x, int y, int x0, int y0) const { return in->ovy[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float OPV(int x, int y, int x0, int y0) const { return in->opv[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float HV(int x, int y, int x0, int y0) const { return in->hv[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &VORT(int x, int y, int x0, int y0) { return w->vort[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &NVX(int x, int y, int x0, int y0) { return w->nvx[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &NVY(int x, int y, int x0, int y0) { return w->nvy[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &NPV(int x, int y, int x0, int y0) { return w->npv[Box::at(x, y, x0, y0)]; }
+};
+
+// ---- staging by loads (single-grid path) -------------------------------------
 template <typename T, int H>
 __device__ __forceinline__ void stage(T *s, const T *g, const AirInst &I, int x0, int y0) {
     for (int i = threadIdx.x; i < Reg<H>::N; i += NT) {
         int ly = i / Reg<H>::W, lx = i - ly * Reg<H>::W;
         int gx = x0 - H + lx, gy = y0 - H + ly;
-        s[i] = in_grid(gx, gy, I) ? __ldg(g + (size_t)gy * I.X + gx) : T(0);
+        s[i] = in_grid(gx, gy, I) ? __ldg(g + (size_t)gy * I.pitch + gx) : T(0);
     }
 }
 template <int H>
@@ -97,91 +181,103 @@ __device__ __forceinline__ void stage_flag(uint8_t *s, const uint32_t *g, uint32
     for (int i = threadIdx.x; i < Reg<H>::N; i += NT) {
         int ly = i / Reg<H>::W, lx = i - ly * Reg<H>::W;
         int gx = x0 - H + lx, gy = y0 - H + ly;
-        s[i] = in_grid(gx, gy, I) ? ((__ldg(g + (size_t)gy * I.X + gx) & bitmask) != 0u) : 0;
+        s[i] = in_grid(gx, gy, I) ? ((__ldg(g + (size_t)gy * I.pitch + gx) & bitmask) != 0u) : 0;
     }
 }
 
-// ---------------------------------------------------------------- A ----
-struct SmemA {
-    uint8_t b[Reg<3>::N];
-    float vx[Reg<2>::N], vy[Reg<2>::N];  // raw, then effective velocity
-    float pv[Reg<1>::N];                 // raw, then opv
-};
+// Calls f(gx, gy) for every in-grid cell of the tile's +R ring (R = 0: the
+// tile), spread over the block's threads.
+template <int R, typename F>
+__device__ __forceinline__ void for_ring(const AirInst &I, int x0, int y0, F &&f) {
+    constexpr int W = TX + 2 * R, N = W * (TY + 2 * R);
+    for (int i = threadIdx.x; i < N; i += NT) {
+        int ly = i / W, lx = i - ly * W;
+        int gx = x0 - R + lx, gy = y0 - R + ly;
+        if (in_grid(gx, gy, I)) f(gx, gy);
+    }
+}
 
-__device__ __forceinline__ void tile_pressure_velocity(const AirInst &I, int x0, int y0, SmemA &S) {
+// ---- pass A ------------------------------------------------------------------
+// pressure.rs:43-85: the three-cell wall velocity clear.
+template <class L>
+__device__ __forceinline__ bool wall_cleared_vx(const L &S, uint32_t x, uint32_t y, uint32_t X, uint32_t Y, int x0, int y0) {
+    bool out = false;
+    if (y >= 1u && y + 1u < Y) {
+        if (x >= 1u && x + 1u < X && S.blk(x, y, x0, y0)) out = true;
+        if (x >= 2u && S.blk((int)x - 1, y, x0, y0)) out = true;
+        if (x + 2u < X && S.blk((int)x + 1, y, x0, y0)) out = true;
+    }
+    return out;
+}
+template <class L>
+__device__ __forceinline__ bool wall_cleared_vy(const L &S, uint32_t x, uint32_t y, uint32_t X, uint32_t Y, int x0, int y0) {
+    bool out = false;
+    if (x >= 1u && x + 1u < X) {
+        if (y >= 1u && y + 1u < Y && S.blk(x, y, x0, y0)) out = true;
+        if (y >= 2u && S.blk(x, (int)y - 1, x0, y0)) out = true;
+        if (y + 2u < Y && S.blk(x, (int)y + 1, x0, y0)) out = true;
+    }
+    return out;
+}
+
+// The compute of pass A once the tile is staged in S. Writes opv, ovx, ovy.
+template <class L> __device__ __forceinline__ void pass_a(const AirInst &I, int x0, int y0, L &S) {
     const uint32_t X = I.X, Y = I.Y;
-    stage_flag<3>(S.b, I.bair, 0xFFFFFFFFu, I, x0, y0);
-    stage<float, 2>(S.vx, I.vx, I, x0, y0);
-    stage<float, 2>(S.vy, I.vy, I, x0, y0);
-    stage<float, 1>(S.pv, I.pv, I, x0, y0);
-    __syncthreads();
-    const BlockView B{S.b, x0, y0};
-    // effective_vx/vy (pressure.rs:119-157) on the +2 ring; this is also the
-    // velocity pass's pre-gradient value (pressure.rs:265-276).
-    for (int i = threadIdx.x; i < Reg<2>::N; i += NT) {
-        int ly = i / Reg<2>::W, lx = i - ly * Reg<2>::W;
-        int gx = x0 - 2 + lx, gy = y0 - 2 + ly;
-        if (!in_grid(gx, gy, I)) continue;
-        float vx = S.vx[i], vy = S.vy[i];
+    // effective_vx/vy (pressure.rs:119-157) on the +2 ring, in place; this
+    // is also the velocity pass's pre-gradient value (pressure.rs:265-276).
+    // Every thread reads only its own cells' velocities, so no barrier is
+    // needed between the reads and the in-place writes.
+    for_ring<2>(I, x0, y0, [&](int gx, int gy) {
+        float vx = S.VX(gx, gy, x0, y0), vy = S.VY(gx, gy, x0, y0);
         if (in_border(gx, gy, X, Y)) {
             vx = I.evx + (vx - I.evx) * 0.9f;
             vy = I.evy + (vy - I.evy) * 0.9f;
         }
-        if (wall_cleared_vx(B, gx, gy, X, Y)) vx = 0.0f;
-        if (wall_cleared_vy(B, gx, gy, X, Y)) vy = 0.0f;
-        S.vx[i] = vx;
-        S.vy[i] = vy;
-    }
+        if (wall_cleared_vx(S, gx, gy, X, Y, x0, y0)) vx = 0.0f;
+        if (wall_cleared_vy(S, gx, gy, X, Y, x0, y0)) vy = 0.0f;
+        S.VX(gx, gy, x0, y0) = vx;
+        S.VY(gx, gy, x0, y0) = vy;
+    });
     __syncthreads();
     // air_pressure_kernel (pressure.rs:186-237) on the +1 ring.
-    float opv_ring[2];
-    int nring = 0;
-    for (int i = threadIdx.x; i < Reg<1>::N; i += NT, ++nring) {
-        int ly = i / Reg<1>::W, lx = i - ly * Reg<1>::W;
-        int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
-        float next = 0.0f;
-        if (in_grid(gx, gy, I)) {
-            float cur = S.pv[i];
-            if (in_border(gx, gy, X, Y)) cur = I.ep + (cur - I.ep) * 0.8f;
-            next = cur;
-            if (interior(gx, gy, X, Y)) {
-                float dp = S.vx[Reg<2>::at(gx - 1, gy, x0, y0)] - S.vx[Reg<2>::at(gx + 1, gy, x0, y0)] +
-                           S.vy[Reg<2>::at(gx, gy - 1, x0, y0)] - S.vy[Reg<2>::at(gx, gy + 1, x0, y0)];
-                next = I.ep + (cur - I.ep) * 0.9999f + dp * 0.15f;
-            }
+    for_ring<1>(I, x0, y0, [&](int gx, int gy) {
+        float cur = S.PV(gx, gy, x0, y0);
+        if (in_border(gx, gy, X, Y)) cur = I.ep + (cur - I.ep) * 0.8f;
+        float next = cur;
+        if (interior(gx, gy, X, Y)) {
+            float dp = S.VX(gx - 1, gy, x0, y0) - S.VX(gx + 1, gy, x0, y0) + S.VY(gx, gy - 1, x0, y0) -
+                       S.VY(gx, gy + 1, x0, y0);
+            next = I.ep + (cur - I.ep) * 0.9999f + dp * 0.15f;
         }
-        opv_ring[nring] = next;
-    }
-    __syncthreads();
-    nring = 0;
-    for (int i = threadIdx.x; i < Reg<1>::N; i += NT, ++nring) S.pv[i] = opv_ring[nring];
+        S.OPV(gx, gy, x0, y0) = next;
+    });
     __syncthreads();
     // air_velocity_kernel (pressure.rs:260-298) on the tile.
     const int gx = x0 + (int)(threadIdx.x % TX), gy = y0 + (int)(threadIdx.x / TX);
     if (in_grid(gx, gy, I)) {
-        const int c2 = Reg<2>::at(gx, gy, x0, y0);
-        float nx = S.vx[c2], ny = S.vy[c2];
+        float nx = S.VX(gx, gy, x0, y0), ny = S.VY(gx, gy, x0, y0);
         if (interior(gx, gy, X, Y)) {
-            float dx = S.pv[Reg<1>::at(gx - 1, gy, x0, y0)] - S.pv[Reg<1>::at(gx + 1, gy, x0, y0)];
-            float dy = S.pv[Reg<1>::at(gx, gy - 1, x0, y0)] - S.pv[Reg<1>::at(gx, gy + 1, x0, y0)];
+            float dx = S.OPV(gx - 1, gy, x0, y0) - S.OPV(gx + 1, gy, x0, y0);
+            float dy = S.OPV(gx, gy - 1, x0, y0) - S.OPV(gx, gy + 1, x0, y0);
             nx = I.evx + (nx - I.evx) * 0.999f + dx * 0.2f;
             ny = I.evy + (ny - I.evy) * 0.999f + dy * 0.2f;
             // adjacent_blocked_x/y (pressure.rs:92-114)
-            if (B.at(gx - 1, gy) || B.at(gx, gy) || B.at(gx + 1, gy)) nx = 0.0f;
-            if (B.at(gx, gy - 1) || B.at(gx, gy) || B.at(gx, gy + 1)) ny = 0.0f;
+            if (S.blk(gx - 1, gy, x0, y0) || S.blk(gx, gy, x0, y0) || S.blk(gx + 1, gy, x0, y0)) nx = 0.0f;
+            if (S.blk(gx, gy - 1, x0, y0) || S.blk(gx, gy, x0, y0) || S.blk(gx, gy + 1, x0, y0)) ny = 0.0f;
         }
-        size_t g = (size_t)gy * X + gx;
+        size_t g = (size_t)gy * I.pitch + gx;
         I.ovx[g] = nx;
         I.ovy[g] = ny;
-        I.opv[g] = S.pv[Reg<1>::at(gx, gy, x0, y0)];
+        I.opv[g] = S.OPV(gx, gy, x0, y0);
     }
 }
 
-// ---------------------------------------------------------------- B ----
+// ---- pass B ------------------------------------------------------------------
 // advect.rs:66-152. `blk` is the mask the walk tests: block_air (heat=false)
 // or block_airh & 0x8 (heat=true).
 __device__ __forceinline__ void far_advect_target(uint32_t x, uint32_t y, float dx, float dy, const uint32_t *blk,
-                                                  uint32_t X, uint32_t Y, bool heat, float &otx, float &oty) {
+                                                  uint32_t X, uint32_t Y, uint32_t pitch, bool heat, float &otx,
+                                                  float &oty) {
     float tx = (float)x - dx * 0.7f;
     float ty = (float)y - dy * 0.7f;
     float adx = dx * 0.7f;
@@ -213,7 +309,7 @@ __device__ __forceinline__ void far_advect_target(uint32_t x, uint32_t y, float 
             int cy = (int)(ty + 0.5f);
             bool hit = true;
             if (cx >= 0 && cy >= 0 && cx < (int)X && cy < (int)Y) {
-                uint32_t v = __ldg(blk + (size_t)cy * X + cx);
+                uint32_t v = __ldg(blk + (size_t)cy * pitch + cx);
                 hit = (heat ? (v & 0x8u) : v) != 0u;
             }
             if (hit) {
@@ -232,54 +328,28 @@ __device__ __forceinline__ void far_advect_target(uint32_t x, uint32_t y, float 
     oty = ty;
 }
 
-// mod.rs:92-102 (compare and assign; keeps NaN and -0 as the reference does).
-__device__ __forceinline__ float clampf(float v, float lo, float hi) {
-    float out = v;
-    if (out < lo) out = lo;
-    if (out > hi) out = hi;
-    return out;
-}
-
-// Smoothing weight of tap (dx, dy) (advect.rs:215-225).
-__device__ __forceinline__ float smooth_w(int dx, int dy) {
-    float w = 0.01831564f;
-    if (dx == 1) w = 0.13533528f;
-    if (dy == 1) w = 0.13533528f;
-    if (dx == 1 && dy == 1) w = 1.0f;
-    return w;
-}
-
-struct SmemB {
-    uint8_t b[Reg<3>::N];               // block_air != 0
-    uint8_t bh[Reg<1>::N];              // block_airh & 0x8
-    float ovx[Reg<3>::N], ovy[Reg<3>::N];
-    float opv[Reg<2>::N];
-    float hv[Reg<1>::N];
-    float nvx[Reg<1>::N], nvy[Reg<1>::N], npv[Reg<1>::N];
-};
-
-// advect.rs:10-42, on staged ovx/ovy (cell and its +-1 neighbours staged).
-__device__ __forceinline__ float vorticity_bmap(const SmemB &S, const BlockView &B, uint32_t x, uint32_t y,
-                                                uint32_t X, uint32_t Y, int x0, int y0) {
+// vorticity_bmap (advect.rs:10-42) of cell (x, y) from the staged ovx/ovy.
+template <class L>
+__device__ __forceinline__ float vorticity_bmap(const L &S, uint32_t x, uint32_t y, uint32_t X, uint32_t Y, int x0, int y0) {
     float out = 0.0f;
     if (x > 1u && x + 2u < X && y > 1u && y + 2u < Y) {
-        bool here = B.at(x, y);
-        float dvydx = S.ovy[Reg<3>::at(x + 1, y, x0, y0)] - S.ovy[Reg<3>::at(x - 1, y, x0, y0)];
-        if (here || B.at(x + 1, y) || B.at(x - 1, y)) dvydx = 0.0f;
-        float dvxdy = S.ovx[Reg<3>::at(x, y + 1, x0, y0)] - S.ovx[Reg<3>::at(x, y - 1, x0, y0)];
-        if (here || B.at(x, y + 1) || B.at(x, y - 1)) dvxdy = 0.0f;
+        bool here = S.blk(x, y, x0, y0);
+        float dvydx = S.OVY(x + 1, y, x0, y0) - S.OVY(x - 1, y, x0, y0);
+        if (here || S.blk(x + 1, y, x0, y0) || S.blk(x - 1, y, x0, y0)) dvydx = 0.0f;
+        float dvxdy = S.OVX(x, y + 1, x0, y0) - S.OVX(x, y - 1, x0, y0);
+        if (here || S.blk(x, y + 1, x0, y0) || S.blk(x, y - 1, x0, y0)) dvxdy = 0.0f;
         out = (dvydx - dvxdy) * 0.5f;
     }
     return out;
 }
 
-// air_smooth_advect_kernel body (advect.rs:192-358) for one cell.
-__device__ __forceinline__ void smooth_advect_cell(const AirInst &I, const SmemB &S, const BlockView &B, int x,
-                                                   int y, int x0, int y0, float &out_vx, float &out_vy,
-                                                   float &out_pv) {
+// air_smooth_advect_kernel body (advect.rs:192-358) for one cell, with the
+// vorticity of the cell and its neighbours taken from S.VORT.
+template <class L>
+__device__ __forceinline__ void smooth_advect_cell(const AirInst &I, L &S, int x, int y, int x0, int y0, float &out_vx,
+                                                   float &out_vy, float &out_pv) {
     const uint32_t X = I.X, Y = I.Y;
-    const int c3 = Reg<3>::at(x, y, x0, y0);
-    const float cvx = S.ovx[c3], cvy = S.ovy[c3], cpv = S.opv[Reg<2>::at(x, y, x0, y0)];
+    const float cvx = S.OVX(x, y, x0, y0), cvy = S.OVY(x, y, x0, y0), cpv = S.OPV(x, y, x0, y0);
     float sx = 0.0f, sy = 0.0f, sp = 0.0f, ws = 0.0f;
 #pragma unroll
     for (int dyy = 0; dyy < 3; ++dyy) {
@@ -292,11 +362,10 @@ __device__ __forceinline__ void smooth_advect_cell(const AirInst &I, const SmemB
             float w = smooth_w(dxx, dyy);
             bool itap = nx >= 1u && ny >= 1u && nx + 1u < X && ny + 1u < Y;
             float tx = cvx, ty = cvy, tp = cpv;
-            if (itap && !B.at(nx, ny)) {
-                int n3 = Reg<3>::at(nx, ny, x0, y0);
-                tx = S.ovx[n3];
-                ty = S.ovy[n3];
-                tp = S.opv[Reg<2>::at(nx, ny, x0, y0)];
+            if (itap && !S.blk(nx, ny, x0, y0)) {
+                tx = S.OVX(nx, ny, x0, y0);
+                ty = S.OVY(nx, ny, x0, y0);
+                tp = S.OPV(nx, ny, x0, y0);
             }
             sx += tx * w;
             sy += ty * w;
@@ -307,11 +376,11 @@ __device__ __forceinline__ void smooth_advect_cell(const AirInst &I, const SmemB
     float nvx = sx / ws, nvy = sy / ws, npv = sp / ws;
 
     float tx0, ty0;
-    far_advect_target(x, y, nvx, nvy, I.bair, X, Y, false, tx0, ty0);
+    far_advect_target(x, y, nvx, nvy, I.bair, X, Y, I.pitch, false, tx0, ty0);
     int i0 = (int)tx0, j0 = (int)ty0;
     float fx = tx0 - (float)i0, fy = ty0 - (float)j0;
-    if (!B.at(x, y) && i0 >= 2 && i0 < (int)X - 3 && j0 >= 2 && j0 < (int)Y - 3 && fx >= 0.0f && fy >= 0.0f) {
-        size_t r0 = (size_t)j0 * X + i0, r1 = r0 + X;
+    if (!S.blk(x, y, x0, y0) && i0 >= 2 && i0 < (int)X - 3 && j0 >= 2 && j0 < (int)Y - 3 && fx >= 0.0f && fy >= 0.0f) {
+        size_t r0 = (size_t)j0 * I.pitch + i0, r1 = r0 + I.pitch;
         float w00 = (1.0f - fx) * (1.0f - fy);
         float w10 = fx * (1.0f - fy);
         float w01 = (1.0f - fx) * fy;
@@ -323,11 +392,11 @@ __device__ __forceinline__ void smooth_advect_cell(const AirInst &I, const SmemB
     }
     // advect.rs:297-328
     if (I.vcoef > 0.0f && (uint32_t)x > 1u && (uint32_t)x + 2u < X && (uint32_t)y > 1u && (uint32_t)y + 2u < Y) {
-        float w = vorticity_bmap(S, B, x, y, X, Y, x0, y0);
-        float wxp = vorticity_bmap(S, B, x + 1, y, X, Y, x0, y0);
-        float wxm = vorticity_bmap(S, B, x - 1, y, X, Y, x0, y0);
-        float wyp = vorticity_bmap(S, B, x, y + 1, X, Y, x0, y0);
-        float wym = vorticity_bmap(S, B, x, y - 1, X, Y, x0, y0);
+        float w = S.VORT(x, y, x0, y0);
+        float wxp = S.VORT(x + 1, y, x0, y0);
+        float wxm = S.VORT(x - 1, y, x0, y0);
+        float wyp = S.VORT(x, y + 1, x0, y0);
+        float wym = S.VORT(x, y - 1, x0, y0);
         if (wxp < 0.0f) wxp = 0.0f - wxp;
         if (wxm < 0.0f) wxm = 0.0f - wxm;
         if (wyp < 0.0f) wyp = 0.0f - wyp;
@@ -339,7 +408,7 @@ __device__ __forceinline__ void smooth_advect_cell(const AirInst &I, const SmemB
         nvx += k * dwy / (norm + 0.001f) * w;
         nvy += k * (0.0f - dwx) / (norm + 0.001f) * w;
     }
-    size_t g = (size_t)y * X + x;
+    size_t g = (size_t)y * I.pitch + x;
     if (__ldg(I.wall + g) == 5u) {  // WL_FAN, advect.rs:331-334
         nvx += __ldg(I.fvx + g);
         nvy += __ldg(I.fvy + g);
@@ -356,13 +425,13 @@ __device__ __forceinline__ void smooth_advect_cell(const AirInst &I, const SmemB
 }
 
 // air_heat_convect_kernel (heat.rs:46-251) for one tile cell; vx/vy of the
-// cell and its neighbours come from the staged smoothing/advection output
-// (read-before-write semantics). Returns the new heat; updates v in place.
-__device__ __forceinline__ float heat_cell(const AirInst &I, const SmemB &S, int x, int y, int x0, int y0,
-                                           float &vx_io, float &vy_io) {
+// cell and its neighbours come from S.NVX/NVY (read-before-write
+// semantics). Returns the new heat; updates v in place.
+template <class L>
+__device__ __forceinline__ float heat_cell(const AirInst &I, L &S, int x, int y, int x0, int y0, float &vx_io,
+                                           float &vy_io) {
     const uint32_t X = I.X, Y = I.Y;
-    const int c1 = Reg<1>::at(x, y, x0, y0);
-    const float ch = S.hv[c1], cvx = S.nvx[c1], cvy = S.nvy[c1];
+    const float ch = S.HV(x, y, x0, y0), cvx = S.NVX(x, y, x0, y0), cvy = S.NVY(x, y, x0, y0);
     float sh = 0.0f, sx = 0.0f, sy = 0.0f, ws = 0.0f;
 #pragma unroll
     for (int dyy = 0; dyy < 3; ++dyy) {
@@ -375,13 +444,10 @@ __device__ __forceinline__ float heat_cell(const AirInst &I, const SmemB &S, int
             float w = smooth_w(dxx, dyy);
             bool itap = nx >= 1u && ny >= 1u && nx + 1u < X && ny + 1u < Y;
             float th = ch, tx = cvx, ty = cvy;
-            if (itap) {
-                int n1 = Reg<1>::at(nx, ny, x0, y0);
-                if (!S.bh[n1]) {
-                    th = S.hv[n1];
-                    tx = S.nvx[n1];
-                    ty = S.nvy[n1];
-                }
+            if (itap && !S.hblk(nx, ny, x0, y0)) {
+                th = S.HV(nx, ny, x0, y0);
+                tx = S.NVX(nx, ny, x0, y0);
+                ty = S.NVY(nx, ny, x0, y0);
             }
             sh += th * w;
             sx += tx * w;
@@ -392,12 +458,12 @@ __device__ __forceinline__ float heat_cell(const AirInst &I, const SmemB &S, int
     float dh = sh / ws;
     float svx = sx / ws, svy = sy / ws;
     float tx, ty;
-    far_advect_target(x, y, svx, svy, I.bairh, X, Y, true, tx, ty);
+    far_advect_target(x, y, svx, svy, I.bairh, X, Y, I.pitch, true, tx, ty);
     int i0 = (int)tx, j0 = (int)ty;
     float fx = tx - (float)i0, fy = ty - (float)j0;
-    const bool here_blocked = S.bh[c1] != 0;
+    const bool here_blocked = S.hblk(x, y, x0, y0);
     if (!here_blocked && i0 >= 0 && i0 < (int)X - 1 && j0 >= 0 && j0 < (int)Y - 1 && fx >= 0.0f && fy >= 0.0f) {
-        size_t r0 = (size_t)j0 * X + i0, r1 = r0 + X;
+        size_t r0 = (size_t)j0 * I.pitch + i0, r1 = r0 + I.pitch;
         float s00 = (__ldg(I.bairh + r0) & 0x8u) ? dh : __ldg(I.hv + r0);
         float s10 = (__ldg(I.bairh + r0 + 1) & 0x8u) ? dh : __ldg(I.hv + r0 + 1);
         float s01 = (__ldg(I.bairh + r1) & 0x8u) ? dh : __ldg(I.hv + r1);
@@ -433,9 +499,8 @@ __device__ __forceinline__ float heat_cell(const AirInst &I, const SmemB &S, int
         float convx = 0.0f - gxv, convy = 0.0f - gyv;
         float nx = cvx, ny = cvy;
         if (I.conv == 1u) {
-            float weight = ((ch - S.hv[Reg<1>::at(x - 1, y, x0, y0)]) * convx +
-                            (ch - S.hv[Reg<1>::at(x, y - 1, x0, y0)]) * convy) / 5000.0f;
-            if (weight > 0.0f && !S.bh[Reg<1>::at(x, y - 1, x0, y0)]) {
+            float weight = ((ch - S.HV(x - 1, y, x0, y0)) * convx + (ch - S.HV(x, y - 1, x0, y0)) * convy) / 5000.0f;
+            if (weight > 0.0f && !S.hblk(x, y - 1, x0, y0)) {
                 nx += weight * convx;
                 ny += weight * convy;
             }
@@ -458,49 +523,44 @@ __device__ __forceinline__ float heat_cell(const AirInst &I, const SmemB &S, int
     return dh;
 }
 
-// Kernel B body. With air_mode == NoUpdate the smoothing/advection pass is
-// skipped (mod.rs:150) and the heat pass reads the stored vx/vy; its
-// convected velocity then goes to ovx/ovy (unused scratch in that mode) so
-// no CTA writes a vx/vy cell another CTA may still stage.
-__device__ __forceinline__ void tile_advect_heat(const AirInst &I, int x0, int y0, SmemB &S) {
-    const uint32_t X = I.X;
+// The compute of pass B once the tile is staged in S. With air_mode ==
+// NoUpdate the smoothing/advection pass is skipped (mod.rs:150) and S.NVX/
+// NVY already hold the stored vx/vy (staged by the caller); the convected
+// velocity then goes to ovx/ovy (unused scratch in that mode) so that no CTA
+// writes a vx/vy cell another CTA may still stage.
+template <class L> __device__ __forceinline__ void pass_b(const AirInst &I, int x0, int y0, L &S) {
+    const uint32_t X = I.X, Y = I.Y;
     const bool update = I.air_mode != 4u;
     if (update) {
-        stage_flag<3>(S.b, I.bair, 0xFFFFFFFFu, I, x0, y0);
-        stage<float, 3>(S.ovx, I.ovx, I, x0, y0);
-        stage<float, 3>(S.ovy, I.ovy, I, x0, y0);
-        stage<float, 2>(S.opv, I.opv, I, x0, y0);
-    } else {
-        stage<float, 1>(S.nvx, I.vx, I, x0, y0);
-        stage<float, 1>(S.nvy, I.vy, I, x0, y0);
-    }
-    if (I.aheat) {
-        stage_flag<1>(S.bh, I.bairh, 0x8u, I, x0, y0);
-        stage<float, 1>(S.hv, I.hv, I, x0, y0);
-    }
-    __syncthreads();
-    if (update) {
-        const BlockView B{S.b, x0, y0};
-        for (int i = threadIdx.x; i < Reg<1>::N; i += NT) {
-            int ly = i / Reg<1>::W, lx = i - ly * Reg<1>::W;
-            int gx = x0 - 1 + lx, gy = y0 - 1 + ly;
-            if (!in_grid(gx, gy, I)) continue;
-            // the ring outside the tile is needed only as heat-smoothing taps
-            bool need = (lx >= 1 && lx <= TX && ly >= 1 && ly <= TY) || I.aheat;
-            if (!need) continue;
-            float a, b, c;
-            smooth_advect_cell(I, S, B, gx, gy, x0, y0, a, b, c);
-            S.nvx[i] = a;
-            S.nvy[i] = b;
-            S.npv[i] = c;
+        if (I.vcoef > 0.0f) {
+            for_ring<2>(I, x0, y0,
+                        [&](int gx, int gy) { S.VORT(gx, gy, x0, y0) = vorticity_bmap(S, gx, gy, X, Y, x0, y0); });
+            __syncthreads();
+        }
+        // the +1 ring outside the tile is needed only as heat-smoothing taps
+        if (I.aheat) {
+            for_ring<1>(I, x0, y0, [&](int gx, int gy) {
+                float a, b, c;
+                smooth_advect_cell(I, S, gx, gy, x0, y0, a, b, c);
+                S.NVX(gx, gy, x0, y0) = a;
+                S.NVY(gx, gy, x0, y0) = b;
+                S.NPV(gx, gy, x0, y0) = c;
+            });
+        } else {
+            for_ring<0>(I, x0, y0, [&](int gx, int gy) {
+                float a, b, c;
+                smooth_advect_cell(I, S, gx, gy, x0, y0, a, b, c);
+                S.NVX(gx, gy, x0, y0) = a;
+                S.NVY(gx, gy, x0, y0) = b;
+                S.NPV(gx, gy, x0, y0) = c;
+            });
         }
         __syncthreads();
     }
     const int gx = x0 + (int)(threadIdx.x % TX), gy = y0 + (int)(threadIdx.x / TX);
     if (!in_grid(gx, gy, I)) return;
-    const int c1 = Reg<1>::at(gx, gy, x0, y0);
-    const size_t g = (size_t)gy * X + gx;
-    float vx = S.nvx[c1], vy = S.nvy[c1];
+    const size_t g = (size_t)gy * I.pitch + gx;
+    float vx = S.NVX(gx, gy, x0, y0), vy = S.NVY(gx, gy, x0, y0);
     if (I.aheat) {
         float h = heat_cell(I, S, gx, gy, x0, y0, vx, vy);
         I.hv_out[g] = h;
@@ -508,14 +568,14 @@ __device__ __forceinline__ void tile_advect_heat(const AirInst &I, int x0, int y
     if (update) {
         I.vx[g] = vx;
         I.vy[g] = vy;
-        I.pv[g] = S.npv[c1];
+        I.pv[g] = S.NPV(gx, gy, x0, y0);
     } else if (I.aheat) {
         I.ovx[g] = vx;
         I.ovy[g] = vy;
     }
 }
 
-// ---------------------------------------------------------------- S ----
+// ---- settle --------------------------------------------------------------------
 // settle.rs:50-93 for one cell: emap decay and the two masks.
 __device__ __forceinline__ void masks_cell(const AirInst &I, size_t g, uint32_t &bair, uint32_t &bairh) {
     uint32_t w = __ldg(I.wall + g) & 0xFFu;

@@ -5,11 +5,13 @@
 #include <string.h>
 
 #include <atomic>
+#include <mutex>
 #include <vector>
 
 #include "air_launch.hpp"
 #include "grav_dft.hpp"
 #include "grav_plan.hpp"
+#include "tmap.hpp"
 
 namespace tpt {
 
@@ -37,6 +39,35 @@ int require_sm100() {
     return TPT_OK;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+int make_grid_tmap(CUtensorMap *out, const void *base, bool is_float, uint32_t cols, uint32_t rows, uint32_t pitch,
+                   uint32_t box_cols, uint32_t box_rows) {
+    auto fn = tensor_map_encoder();
+    if (!fn) TPT_FAIL(TPT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available from the driver");
+    cuuint64_t dims[2] = {cols, rows};
+    cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
+    cuuint32_t box[2] = {box_cols, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(out, is_float ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT32, 2,
+                    const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) TPT_FAIL(TPT_ERR_CUDA, "cuTensorMapEncodeTiled (grid %ux%u pitch %u) failed (%d)", cols, rows,
+                                    pitch, (int)r);
+    return TPT_OK;
+}
+
 static int check_dims(uint32_t X, uint32_t Y) {
     if (X > TPT_MAX_CELLS_PER_SIDE || Y > TPT_MAX_CELLS_PER_SIDE)
         TPT_FAIL(TPT_ERR_INVALID_DIMS, "grid %ux%u exceeds %u cells per side", X, Y, TPT_MAX_CELLS_PER_SIDE);
@@ -55,6 +86,7 @@ AirInst make_air_inst(const tpt_air_params &p) {
     AirInst I{};
     I.X = p.xcells;
     I.Y = p.ycells;
+    I.pitch = p.xcells;
     I.air_mode = p.air_mode;
     I.aheat = p.aheat_enable;
     I.conv = p.convection_mode;
@@ -86,9 +118,12 @@ const char *tpt_last_error_string(void) { return g_err; }
 
 int tpt_check_device_errors(void) {
     TPT_CUDA(cudaDeviceSynchronize());
-    uint32_t bits = 0;
+    uint32_t bits = 0, abits = 0;
     int rc = dft::read_errors(&bits);
     if (rc) return rc;
+    rc = air::read_errors(&abits);
+    if (rc) return rc;
+    bits |= abits;
     if (bits) TPT_FAIL(TPT_ERR_DEVICE_TIMEOUT, "a device-side wait timed out (error bits 0x%x)", bits);
     return TPT_OK;
 }
@@ -258,7 +293,7 @@ static int grav_solve_any(tpt_grav_plan *p, const int32_t *mi, const float *mf, 
         gfft::JobIO io{mi, mf, mask, gx, gy, inv, 1};
         return p->fft.launch((cudaStream_t)stream, &io);
     }
-    dft::SolveIO io{mi, mf, mask, gx, gy, inv};
+    dft::SolveIO io{mi, mf, mask, gx, gy, inv, p->X};
     return p->dft->launch((cudaStream_t)stream, &io);
 }
 

@@ -1,8 +1,9 @@
 // batch.cu -- many independent sandbox instances stepped together.
 //
 // Layout: every grid of every instance lives in one of three packed device
-// arenas (f32, u32, i32); each instance's grid is contiguous in the
-// reference layout (`cy * xcells + cx`) and starts on a 256-byte boundary.
+// arenas (f32, u32, i32). Instance i's grids are `ycells` rows of
+// `pitch_i` elements (pitch = xcells rounded up to 32, so rows start on
+// 128-byte boundaries as TMA needs); cell (cx, cy) is at cy * pitch + cx.
 // Ambient heat and the two wall masks have a second copy (ping-pong), so a
 // tick is two air launches over a tile list of all instances (no settle
 // pass); after an odd tick count one copy-back restores the canonical
@@ -22,34 +23,33 @@
 #include "air_launch.hpp"
 #include "grav_dft.hpp"
 #include "grav_plan.hpp"
-
-namespace tpt {
-AirInst make_air_inst(const tpt_air_params &p);
-}
+#include "tmap.hpp"
 
 using namespace tpt;
 
 namespace {
 constexpr uint32_t CHUNK = 50;  // ticks per captured graph (even)
-constexpr size_t ALIGN = 64;    // elements (256 B)
+constexpr size_t ALIGN = 64;    // elements (256 B) between instances
 
 enum F32 { F_PV, F_VX, F_VY, F_HV, F_HV2, F_OPV, F_OVX, F_OVY, F_FVX, F_FVY, F_GX, F_GY, F_N32 };
 enum U32 { U_BA, U_BH, U_BA2, U_BH2, U_WALL, U_EMAP, U_EA, U_EH, U_GMASK, U_NU32 };
 
-size_t round_up(size_t v) { return (v + ALIGN - 1) / ALIGN * ALIGN; }
+size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
 }  // namespace
 
 struct tpt_batch {
     uint32_t n = 0;
     int precision = TPT_PRECISION_FP32;
     std::vector<tpt_instance_desc> descs;
-    std::vector<size_t> off;  // per-instance element offset (same in all arenas)
-    size_t stride = 0;        // elements per grid slot of the arenas
+    std::vector<size_t> off;       // per-instance element offset (same in all arenas)
+    std::vector<uint32_t> pitch;   // per-instance row stride (elements)
+    size_t stride = 0;             // elements per grid slot of the arenas
     float *f32 = nullptr;
     uint32_t *u32 = nullptr;
     int32_t *i32 = nullptr;
     std::vector<AirInst> insts_host;
     AirInst *insts = nullptr;
+    CUtensorMap *tmaps = nullptr;
     air::TileRef *tiles = nullptr;
     uint32_t ntiles = 0;
     bool any_noupdate_heat = false;
@@ -64,7 +64,15 @@ struct tpt_batch {
 
     float *f(int field, uint32_t i) const { return f32 + (size_t)field * stride + off[i]; }
     uint32_t *u(int field, uint32_t i) const { return u32 + (size_t)field * stride + off[i]; }
-    uint32_t grid() const { return std::min<uint32_t>(ntiles, (uint32_t)sms * std::max<uint32_t>(tuning.ctas_per_sm, 1)); }
+    uint32_t grid() const {
+        return std::min<uint32_t>(ntiles, (uint32_t)sms * std::max<uint32_t>(tuning.ctas_per_sm, 1));
+    }
+    int air_tick(uint32_t parity, cudaStream_t st) const {
+        return air::launch_batch_tick(insts, tmaps, tiles, ntiles, grid(), parity, any_noupdate_heat, st);
+    }
+    int grav_solve(cudaStream_t st) const {
+        return precision == TPT_PRECISION_FP32 ? fft.launch(st) : dft.launch(st);
+    }
 
     void drop_graphs() {
         for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
@@ -76,6 +84,7 @@ struct tpt_batch {
         cudaFree(u32);
         cudaFree(i32);
         cudaFree(insts);
+        cudaFree(tmaps);
         cudaFree(tiles);
         if (side) cudaStreamDestroy(side);
         if (fork) cudaEventDestroy(fork);
@@ -91,12 +100,12 @@ static int record_ticks(tpt_batch *b, uint32_t ticks, cudaStream_t st) {
         TPT_CUDA(cudaEventRecord(b->fork, st));
         TPT_CUDA(cudaStreamWaitEvent(b->side, b->fork, 0));
         for (uint32_t t = 0; t < ticks; ++t) {
-            rc = b->precision == TPT_PRECISION_FP32 ? b->fft.launch(b->side) : b->dft.launch(b->side);
+            rc = b->grav_solve(b->side);
             if (rc) return rc;
         }
     }
     for (uint32_t t = 0; t < ticks; ++t) {
-        rc = air::launch_batch_tick(b->insts, b->tiles, b->ntiles, b->grid(), t & 1u, b->any_noupdate_heat, st);
+        rc = b->air_tick(t & 1u, st);
         if (rc) return rc;
     }
     if (ticks & 1u) {
@@ -167,6 +176,32 @@ static int field_ptr(tpt_batch *b, uint32_t i, int field, void **p) {
     return TPT_OK;
 }
 
+// Saved copy of the state arenas, for the calls that run trial ticks.
+struct StateCopy {
+    float *f = nullptr;
+    uint32_t *u = nullptr;
+    size_t fbytes = 0, ubytes = 0;
+    int save(const tpt_batch *b, cudaStream_t st) {
+        fbytes = b->stride * F_N32 * sizeof(float);
+        ubytes = b->stride * U_NU32 * sizeof(uint32_t);
+        TPT_CUDA(cudaMalloc(&f, fbytes));
+        TPT_CUDA(cudaMalloc(&u, ubytes));
+        TPT_CUDA(cudaMemcpyAsync(f, b->f32, fbytes, cudaMemcpyDeviceToDevice, st));
+        TPT_CUDA(cudaMemcpyAsync(u, b->u32, ubytes, cudaMemcpyDeviceToDevice, st));
+        return TPT_OK;
+    }
+    int restore(tpt_batch *b, cudaStream_t st) {
+        TPT_CUDA(cudaMemcpyAsync(b->f32, f, fbytes, cudaMemcpyDeviceToDevice, st));
+        TPT_CUDA(cudaMemcpyAsync(b->u32, u, ubytes, cudaMemcpyDeviceToDevice, st));
+        TPT_CUDA(cudaStreamSynchronize(st));
+        return TPT_OK;
+    }
+    ~StateCopy() {
+        cudaFree(f);
+        cudaFree(u);
+    }
+};
+
 extern "C" {
 
 int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, tpt_batch **out) {
@@ -186,6 +221,7 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     }
     int rc = require_sm100();
     if (rc) return rc;
+    if (!tensor_map_encoder()) TPT_FAIL(TPT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available");
     tpt_batch *b = new (std::nothrow) tpt_batch();
     if (!b) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "host allocation failed");
     auto bail = [&](int code) {
@@ -200,9 +236,11 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
     size_t total = 0;
     b->off.resize(n);
+    b->pitch.resize(n);
     for (uint32_t i = 0; i < n; ++i) {
+        b->pitch[i] = (uint32_t)round_up(descs[i].air.xcells, 32);
         b->off[i] = total;
-        total += round_up((size_t)descs[i].air.xcells * descs[i].air.ycells);
+        total += round_up((size_t)b->pitch[i] * descs[i].air.ycells, ALIGN);
     }
     b->stride = total;
     cudaError_t e = cudaMalloc(&b->f32, total * F_N32 * sizeof(float));
@@ -211,6 +249,7 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     if (e == cudaSuccess) e = cudaMemset(b->f32, 0, total * F_N32 * sizeof(float));
     if (e == cudaSuccess) e = cudaMemset(b->u32, 0, total * U_NU32 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(b->i32, 0, total * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b->tmaps, (size_t)n * air::TM_COUNT * sizeof(CUtensorMap));
     if (e != cudaSuccess) {
         set_error("batch arena allocation (%zu cells) failed: %s", total, cudaGetErrorString(e));
         return bail(e == cudaErrorMemoryAllocation ? TPT_ERR_OUT_OF_MEMORY : TPT_ERR_CUDA);
@@ -218,12 +257,14 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     // two AirInst per instance: parity 0 reads canonical hv/masks and writes
     // the second copies; parity 1 the reverse.
     std::vector<air::TileRef> tiles;
+    std::vector<CUtensorMap> tm((size_t)n * air::TM_COUNT);
     b->insts_host.resize(2 * (size_t)n);
     std::vector<JobShape> gshapes;
     std::vector<uint32_t> gidx;
     for (uint32_t i = 0; i < n; ++i) {
         const tpt_air_params &p = descs[i].air;
         AirInst I = make_air_inst(p);
+        I.pitch = b->pitch[i];
         I.pv = b->f(F_PV, i);
         I.vx = b->f(F_VX, i);
         I.vy = b->f(F_VY, i);
@@ -251,6 +292,27 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
             J.bairh_out = b->u(par ? U_BH : U_BH2, i);
             b->insts_host[2 * (size_t)i + par] = J;
         }
+        // tensor maps of the grids the two passes stage (box = tile + halo)
+        CUtensorMap *m = &tm[(size_t)i * air::TM_COUNT];
+        const uint32_t X = p.xcells, Y = p.ycells, P = b->pitch[i];
+        const uint32_t BW = AIR_TX + 8, BH = AIR_TY + 6;
+        struct Slot {
+            int slot;
+            const void *base;
+            bool f;
+        } slots[] = {
+            {air::TM_PV, b->f(F_PV, i), true},        {air::TM_VX, b->f(F_VX, i), true},
+            {air::TM_VY, b->f(F_VY, i), true},        {air::TM_OVX, b->f(F_OVX, i), true},
+            {air::TM_OVY, b->f(F_OVY, i), true},      {air::TM_OPV, b->f(F_OPV, i), true},
+            {air::TM_BA0, b->u(U_BA, i), false},      {air::TM_BA1, b->u(U_BA2, i), false},
+            {air::TM_BH0, b->u(U_BH, i), false},      {air::TM_BH1, b->u(U_BH2, i), false},
+            {air::TM_HV0, b->insts_host[2 * (size_t)i].hv, true},
+            {air::TM_HV1, b->insts_host[2 * (size_t)i + 1].hv, true},
+        };
+        for (const Slot &s : slots) {
+            rc = make_grid_tmap(&m[s.slot], s.base, s.f, X, Y, P, BW, BH);
+            if (rc) return bail(rc);
+        }
         if (p.air_mode == 4u && p.aheat_enable) b->any_noupdate_heat = true;
         for (uint32_t ty = 0; ty * AIR_TY < p.ycells; ++ty)
             for (uint32_t tx = 0; tx * AIR_TX < p.xcells; ++tx) tiles.push_back({i, (uint16_t)tx, (uint16_t)ty});
@@ -266,6 +328,7 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
         e = cudaMemcpy(b->insts, b->insts_host.data(), b->insts_host.size() * sizeof(AirInst), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(b->tiles, tiles.data(), tiles.size() * sizeof(air::TileRef), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->tmaps, tm.data(), tm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
@@ -281,7 +344,7 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
             for (size_t j = 0; j < gidx.size(); ++j) {
                 uint32_t i = gidx[j];
                 b->fft.set_io(j, b->i32 + b->off[i], nullptr, 1.0f / 65536.0f, b->u(U_GMASK, i), b->f(F_GX, i),
-                              b->f(F_GY, i));
+                              b->f(F_GY, i), b->pitch[i]);
             }
             rc = b->fft.upload_jobs();
         } else {
@@ -289,7 +352,7 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
             for (size_t j = 0; rc == TPT_OK && j < gidx.size(); ++j) {
                 uint32_t i = gidx[j];
                 dft::SolveIO io{b->i32 + b->off[i], nullptr, b->u(U_GMASK, i), b->f(F_GX, i), b->f(F_GY, i),
-                                1.0f / 65536.0f};
+                                1.0f / 65536.0f, b->pitch[i]};
                 rc = b->dft.set_io(j, io);
             }
         }
@@ -323,31 +386,35 @@ int tpt_batch_fields(tpt_batch *b, uint32_t i, tpt_instance_fields *o) {
     o->grav_mask = b->u(U_GMASK, i);
     o->gx = b->f(F_GX, i);
     o->gy = b->f(F_GY, i);
+    o->pitch = b->pitch[i];
+    return TPT_OK;
+}
+
+// Copies between a dense host grid (xcells per row) and the pitched grid.
+static int batch_copy(tpt_batch *b, uint32_t i, int field, void *host, size_t bytes, bool to_device,
+                      tpt_stream_t stream) {
+    if (!b || !host) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_%s: NULL pointer", to_device ? "write" : "read");
+    if (i >= b->n) TPT_FAIL(TPT_ERR_INVALID_ARG, "instance %u out of range", i);
+    const size_t X = b->descs[i].air.xcells, Y = b->descs[i].air.ycells;
+    if (bytes != X * Y * 4) TPT_FAIL(TPT_ERR_INVALID_ARG, "bytes %zu != %zu cells * 4", bytes, X * Y);
+    void *p;
+    int rc = field_ptr(b, i, field, &p);
+    if (rc) return rc;
+    const size_t dpitch = (size_t)b->pitch[i] * 4;
+    if (to_device) {
+        TPT_CUDA(cudaMemcpy2DAsync(p, dpitch, host, X * 4, X * 4, Y, cudaMemcpyHostToDevice, (cudaStream_t)stream));
+    } else {
+        TPT_CUDA(cudaMemcpy2DAsync(host, X * 4, p, dpitch, X * 4, Y, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    }
     return TPT_OK;
 }
 
 int tpt_batch_write(tpt_batch *b, uint32_t i, int field, const void *host, size_t bytes, tpt_stream_t stream) {
-    if (!b || !host) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_write: NULL pointer");
-    if (i >= b->n) TPT_FAIL(TPT_ERR_INVALID_ARG, "instance %u out of range", i);
-    size_t cells = (size_t)b->descs[i].air.xcells * b->descs[i].air.ycells;
-    if (bytes != cells * 4) TPT_FAIL(TPT_ERR_INVALID_ARG, "bytes %zu != %zu cells * 4", bytes, cells);
-    void *p;
-    int rc = field_ptr(b, i, field, &p);
-    if (rc) return rc;
-    TPT_CUDA(cudaMemcpyAsync(p, host, bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream));
-    return TPT_OK;
+    return batch_copy(b, i, field, const_cast<void *>(host), bytes, true, stream);
 }
 
 int tpt_batch_read(tpt_batch *b, uint32_t i, int field, void *host, size_t bytes, tpt_stream_t stream) {
-    if (!b || !host) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_read: NULL pointer");
-    if (i >= b->n) TPT_FAIL(TPT_ERR_INVALID_ARG, "instance %u out of range", i);
-    size_t cells = (size_t)b->descs[i].air.xcells * b->descs[i].air.ycells;
-    if (bytes != cells * 4) TPT_FAIL(TPT_ERR_INVALID_ARG, "bytes %zu != %zu cells * 4", bytes, cells);
-    void *p;
-    int rc = field_ptr(b, i, field, &p);
-    if (rc) return rc;
-    TPT_CUDA(cudaMemcpyAsync(host, p, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
-    return TPT_OK;
+    return batch_copy(b, i, field, host, bytes, false, stream);
 }
 
 int tpt_batch_step(tpt_batch *b, uint32_t ticks, tpt_stream_t stream) {
@@ -389,32 +456,6 @@ int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
     return TPT_OK;
 }
 
-// Saved copy of the state arenas, for the calls that run trial ticks.
-struct StateCopy {
-    float *f = nullptr;
-    uint32_t *u = nullptr;
-    size_t fbytes = 0, ubytes = 0;
-    int save(const tpt_batch *b, cudaStream_t st) {
-        fbytes = b->stride * F_N32 * sizeof(float);
-        ubytes = b->stride * U_NU32 * sizeof(uint32_t);
-        TPT_CUDA(cudaMalloc(&f, fbytes));
-        TPT_CUDA(cudaMalloc(&u, ubytes));
-        TPT_CUDA(cudaMemcpyAsync(f, b->f32, fbytes, cudaMemcpyDeviceToDevice, st));
-        TPT_CUDA(cudaMemcpyAsync(u, b->u32, ubytes, cudaMemcpyDeviceToDevice, st));
-        return TPT_OK;
-    }
-    int restore(tpt_batch *b, cudaStream_t st) {
-        TPT_CUDA(cudaMemcpyAsync(b->f32, f, fbytes, cudaMemcpyDeviceToDevice, st));
-        TPT_CUDA(cudaMemcpyAsync(b->u32, u, ubytes, cudaMemcpyDeviceToDevice, st));
-        TPT_CUDA(cudaStreamSynchronize(st));
-        return TPT_OK;
-    }
-    ~StateCopy() {
-        cudaFree(f);
-        cudaFree(u);
-    }
-};
-
 int tpt_batch_profile_phases(tpt_batch *b, uint32_t ticks, tpt_stream_t stream, tpt_batch_profile *out) {
     if (!b || !out) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_profile_phases: NULL pointer");
     if (ticks == 0 || (ticks & 1u)) TPT_FAIL(TPT_ERR_INVALID_ARG, "ticks must be even and > 0");
@@ -436,14 +477,11 @@ int tpt_batch_profile_phases(tpt_batch *b, uint32_t ticks, tpt_stream_t stream, 
     TPT_CUDA(cudaEventCreate(&e0));
     TPT_CUDA(cudaEventCreate(&e1));
     TPT_CUDA(cudaEventCreate(&e2));
-    for (uint32_t t = 0; t < 2 && rc == TPT_OK; ++t)  // warm-up
-        rc = air::launch_batch_tick(b->insts, b->tiles, b->ntiles, b->grid(), t, b->any_noupdate_heat, st);
+    for (uint32_t t = 0; t < 2 && rc == TPT_OK; ++t) rc = b->air_tick(t, st);  // warm-up
     cudaEventRecord(e0, st);
-    for (uint32_t t = 0; t < ticks && rc == TPT_OK; ++t)
-        rc = air::launch_batch_tick(b->insts, b->tiles, b->ntiles, b->grid(), t & 1u, b->any_noupdate_heat, st);
+    for (uint32_t t = 0; t < ticks && rc == TPT_OK; ++t) rc = b->air_tick(t & 1u, st);
     cudaEventRecord(e1, st);
-    for (uint32_t t = 0; t < ticks && rc == TPT_OK && b->any_grav; ++t)
-        rc = b->precision == TPT_PRECISION_FP32 ? b->fft.launch(st) : b->dft.launch(st);
+    for (uint32_t t = 0; t < ticks && rc == TPT_OK && b->any_grav; ++t) rc = b->grav_solve(st);
     cudaEventRecord(e2, st);
     if (rc == TPT_OK) {
         cudaEventSynchronize(e2);
@@ -466,7 +504,7 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const uint32_t cands[] = {1, 2, 4, 8};
+    const uint32_t cands[] = {1, 2, 3, 4, 6, 8};
     tpt_batch_tuning best = b->tuning;
     float best_ms = 1e30f;
     int rc = TPT_OK;
@@ -478,8 +516,7 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
         const uint32_t trial = 20;
         for (int rep = 0; rep < 2 && rc == TPT_OK; ++rep) {  // warm-up, then timed
             cudaEventRecord(e0, st);
-            for (uint32_t k = 0; k < trial && rc == TPT_OK; ++k)
-                rc = air::launch_batch_tick(b->insts, b->tiles, b->ntiles, b->grid(), k & 1u, b->any_noupdate_heat, st);
+            for (uint32_t k = 0; k < trial && rc == TPT_OK; ++k) rc = b->air_tick(k & 1u, st);
             cudaEventRecord(e1, st);
         }
         if (rc) break;

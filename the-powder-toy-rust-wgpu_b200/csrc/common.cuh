@@ -50,6 +50,7 @@ int require_sm100();
 // Everything one air step of one instance needs, in device-visible form.
 struct AirInst {
     uint32_t X, Y;
+    uint32_t pitch;  // row stride (elements) of every grid of the instance
     uint32_t air_mode, aheat, conv, gmode;
     float ep, evx, evy, amb, vcoef, cgx, cgy;
     float *pv, *vx, *vy, *hv;

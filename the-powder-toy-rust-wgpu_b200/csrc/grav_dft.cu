@@ -67,6 +67,7 @@ struct InstIO {
     const uint32_t *mask;
     float *gx, *gy;
     float inv;
+    uint32_t pitch;  // row stride of the four grids
 };
 
 struct Problem {
@@ -297,8 +298,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const uint32_t f = r2 >= Gp.Y ? 1u : 0u, y = r2 - f * Gp.Y;
                     const uint32_t inst = Gp.inst0 + il;
                     const InstIO io = (io0_active && inst == 0) ? io0 : ios[inst];
-                    float *out = (f ? io.gy : io.gx) + (size_t)y * Gp.X;
-                    const uint32_t *mask = io.mask + (size_t)y * Gp.X;
+                    float *out = (f ? io.gy : io.gx) + (size_t)y * io.pitch;
+                    const uint32_t *mask = io.mask + (size_t)y * io.pitch;
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
                         const uint32_t x = nb + j;
@@ -337,7 +338,7 @@ __global__ void prep_mass(const Group *__restrict__ groups, const PrepRef *__res
     const size_t plane = (size_t)Gp.rowsR * Gp.kpR;
     bf16 *o = Gp.aR + (size_t)r.row * Gp.kpR;
     for (uint32_t x = threadIdx.x; x < Gp.X; x += blockDim.x) {
-        size_t c = (size_t)y * Gp.X + x;
+        size_t c = (size_t)y * io.pitch + x;
         float v = 0.0f;
         if (__ldg(io.mask + c) != 0u) v = io.mass_f ? __ldg(io.mass_f + c) : (float)__ldg(io.mass_i + c) * io.inv;
         split_store(o + x, o + plane + x, v);
@@ -665,7 +666,7 @@ void DftSet::dims(size_t j, uint32_t *n1, uint32_t *n2) const {
 int DftSet::set_io(size_t j, const SolveIO &io) {
     DftImpl *I = impl;
     uint32_t pos = I->inst_local[j];
-    I->ios_host[pos] = InstIO{io.mass_i, io.mass_f, io.mask, io.gx, io.gy, io.mass_scale_inv};
+    I->ios_host[pos] = InstIO{io.mass_i, io.mass_f, io.mask, io.gx, io.gy, io.mass_scale_inv, io.pitch};
     TPT_CUDA(cudaMemcpy(I->ios + pos, &I->ios_host[pos], sizeof(InstIO), cudaMemcpyHostToDevice));
     return TPT_OK;
 }
@@ -675,7 +676,7 @@ int DftSet::launch(cudaStream_t st, const SolveIO *io) const {
     InstIO io0{};
     int act = 0;
     if (io) {
-        io0 = InstIO{io->mass_i, io->mass_f, io->mask, io->gx, io->gy, io->mass_scale_inv};
+        io0 = InstIO{io->mass_i, io->mass_f, io->mask, io->gx, io->gy, io->mass_scale_inv, io->pitch};
         act = 1;
     }
     uint32_t *err = I->err;

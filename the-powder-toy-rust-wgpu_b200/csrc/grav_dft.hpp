@@ -16,6 +16,7 @@ struct SolveIO {
     const uint32_t *mask;
     float *gx, *gy;
     float mass_scale_inv;
+    uint32_t pitch;  // row stride (elements) of mass, mask, gx, gy
 };
 
 struct DftImpl;

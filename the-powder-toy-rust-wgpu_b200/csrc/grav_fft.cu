@@ -23,7 +23,7 @@ __global__ void __launch_bounds__(NT) rows_forward(const Job *__restrict__ jobs,
     for (uint32_t i = threadIdx.x; i < J.n1; i += NT) sm2[i] = make_float2(0.f, 0.f);
     __syncthreads();
     for (uint32_t x = threadIdx.x; x < J.X; x += NT) {
-        size_t c = (size_t)y * J.X + x;
+        size_t c = (size_t)y * J.pitch + x;
         float v = 0.0f;
         if (__ldg(J.mask + c) != 0u) v = J.mass_f ? __ldg(J.mass_f + c) : (float)__ldg(J.mass_i + c) * J.mass_scale_inv;
         sm2[bitrev(x, J.l1)] = make_float2(v, 0.f);
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(NT) rows_inverse(const Job *__restrict__ jobs,
     fft_dif(sm2, (int)J.n1, J.l1, 1, J.tw1, true);
     float *out = field ? J.gy : J.gx;
     for (uint32_t x = threadIdx.x; x < J.X; x += NT) {
-        size_t c = (size_t)y * J.X + x;
+        size_t c = (size_t)y * J.pitch + x;
         out[c] = __ldg(J.mask + c) != 0u ? sm2[bitrev(x, J.l1)].x : 0.0f;
     }
 }
@@ -275,6 +275,7 @@ int FftSet::create(const std::vector<JobShape> &shapes) {
         Job &J = jobs_host[j];
         J = Job{};
         J.X = s.X;
+        J.pitch = s.X;
         J.Y = s.Y;
         J.n1 = next_pow2(2 * s.X);
         J.n2 = next_pow2(2 * s.Y);
@@ -332,8 +333,9 @@ int FftSet::upload_jobs() {
 }
 
 int FftSet::set_io(size_t j, const int32_t *mass_i, const float *mass_f, float inv, const uint32_t *mask, float *gx,
-                   float *gy) {
+                   float *gy, uint32_t pitch) {
     Job &J = jobs_host[j];
+    J.pitch = pitch;
     bool changed = J.mass_i != mass_i || J.mass_f != mass_f || J.mass_scale_inv != inv || J.mask != mask ||
                    J.gx != gx || J.gy != gy;
     J.mass_i = mass_i;

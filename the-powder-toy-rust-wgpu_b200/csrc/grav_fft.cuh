@@ -100,6 +100,7 @@ __device__ void fft_dif(T2 *s, int n, int log2n, int ncols, const T2 *__restrict
 struct Job {
     uint32_t X, Y, n1, n2;
     int l1, l2;                   // log2(n1), log2(n2)
+    uint32_t pitch;               // row stride (elements) of mass, mask, gx, gy
     const int32_t *mass_i;        // fixed-point mass, or
     const float *mass_f;          // f32 mass (one of the two is set)
     float mass_scale_inv;

@@ -30,7 +30,7 @@ struct FftSet {
     // Points job j at its inputs/outputs; returns 1 if anything changed
     // (the caller then re-uploads with upload_jobs()).
     int set_io(size_t j, const int32_t *mass_i, const float *mass_f, float inv, const uint32_t *mask, float *gx,
-               float *gy);
+               float *gy, uint32_t pitch);
     int upload_jobs();
     // io != null: a one-job set solving on per-call pointers.
     int launch(cudaStream_t st, const JobIO *io = nullptr) const;

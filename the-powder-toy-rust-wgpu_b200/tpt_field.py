@@ -83,7 +83,7 @@ class InstanceDesc(ctypes.Structure):
 class InstanceFields(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in (
         "pv", "vx", "vy", "hv", "block_air", "block_airh", "wall_bmap", "wall_emap", "elem_block_air",
-        "elem_block_airh", "fan_vx", "fan_vy", "grav_mass", "grav_mask", "gx", "gy")]
+        "elem_block_airh", "fan_vx", "fan_vy", "grav_mass", "grav_mask", "gx", "gy")] + [("pitch", ctypes.c_uint32)]
 
 
 class BatchProfile(ctypes.Structure):
