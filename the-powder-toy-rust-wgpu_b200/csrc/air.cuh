@@ -126,6 +126,13 @@ struct LayoutB1 {
     float hv[Reg<1>::N];
     float vort[Reg<2>::N];
     float nvx[Reg<1>::N], nvy[Reg<1>::N], npv[Reg<1>::N];
+    // staged regions: b/ovx/ovy cover the +3 ring, bh/hv the +1 ring
+    __device__ __forceinline__ static bool has3(int x, int y, int x0, int y0) {
+        return x >= x0 - 3 && x < x0 + TX + 3 && y >= y0 - 3 && y < y0 + TY + 3;
+    }
+    __device__ __forceinline__ static bool hasH(int x, int y, int x0, int y0) {
+        return x >= x0 - 1 && x < x0 + TX + 1 && y >= y0 - 1 && y < y0 + TY + 1;
+    }
     __device__ __forceinline__ bool blk(int x, int y, int x0, int y0) const { return b[Reg<3>::at(x, y, x0, y0)] != 0; }
     __device__ __forceinline__ bool hblk(int x, int y, int x0, int y0) const { return bh[Reg<1>::at(x, y, x0, y0)] != 0; }
     __device__ __forceinline__ float OVX(int x, int y, int x0, int y0) const { return ovx[Reg<3>::at(x, y, x0, y0)]; }
@@ -152,6 +159,11 @@ struct WorkB2 {
 struct LayoutB2 {
     BoxB *in;
     WorkB2 *w;
+    // every staged grid covers the whole box
+    __device__ __forceinline__ static bool has3(int x, int y, int x0, int y0) {
+        return x >= x0 - Box::HX && x < x0 + TX + Box::HX && y >= y0 - Box::HY && y < y0 + TY + Box::HY;
+    }
+    __device__ __forceinline__ static bool hasH(int x, int y, int x0, int y0) { return has3(x, y, x0, y0); }
     __device__ __forceinline__ bool blk(int x, int y, int x0, int y0) const { return in->b[Box::at(x, y, x0, y0)] != 0u; }
     __device__ __forceinline__ bool hblk(int x, int y, int x0, int y0) const {
         return (in->bh[Box::at(x, y, x0, y0)] & 0x8u) != 0u;
@@ -273,11 +285,12 @@ template <class L> __device__ __forceinline__ void pass_a(const AirInst &I, int 
 }
 
 // ---- pass B ------------------------------------------------------------------
-// advect.rs:66-152. `blk` is the mask the walk tests: block_air (heat=false)
-// or block_airh & 0x8 (heat=true).
-__device__ __forceinline__ void far_advect_target(uint32_t x, uint32_t y, float dx, float dy, const uint32_t *blk,
-                                                  uint32_t X, uint32_t Y, uint32_t pitch, bool heat, float &otx,
-                                                  float &oty) {
+// advect.rs:66-152. `blocked(cx, cy)` is the mask the walk tests for an
+// in-grid cell: block_air != 0 (velocity walk) or block_airh & 0x8 (heat
+// walk), read from shared memory when the cell is staged.
+template <typename B>
+__device__ __forceinline__ void far_advect_target(uint32_t x, uint32_t y, float dx, float dy, B &&blocked, uint32_t X,
+                                                  uint32_t Y, float &otx, float &oty) {
     float tx = (float)x - dx * 0.7f;
     float ty = (float)y - dy * 0.7f;
     float adx = dx * 0.7f;
@@ -308,10 +321,7 @@ __device__ __forceinline__ void far_advect_target(uint32_t x, uint32_t y, float 
             int cx = (int)(tx + 0.5f);
             int cy = (int)(ty + 0.5f);
             bool hit = true;
-            if (cx >= 0 && cy >= 0 && cx < (int)X && cy < (int)Y) {
-                uint32_t v = __ldg(blk + (size_t)cy * pitch + cx);
-                hit = (heat ? (v & 0x8u) : v) != 0u;
-            }
+            if (cx >= 0 && cy >= 0 && cx < (int)X && cy < (int)Y) hit = blocked(cx, cy);
             if (hit) {
                 tx -= step_x;
                 ty -= step_y;
@@ -376,19 +386,43 @@ __device__ __forceinline__ void smooth_advect_cell(const AirInst &I, L &S, int x
     float nvx = sx / ws, nvy = sy / ws, npv = sp / ws;
 
     float tx0, ty0;
-    far_advect_target(x, y, nvx, nvy, I.bair, X, Y, I.pitch, false, tx0, ty0);
+    far_advect_target(
+        x, y, nvx, nvy,
+        [&](int cx, int cy) -> bool {
+            if (S.has3(cx, cy, x0, y0)) return S.blk(cx, cy, x0, y0);
+            return __ldg(I.bair + (size_t)cy * I.pitch + cx) != 0u;
+        },
+        X, Y, tx0, ty0);
     int i0 = (int)tx0, j0 = (int)ty0;
     float fx = tx0 - (float)i0, fy = ty0 - (float)j0;
     if (!S.blk(x, y, x0, y0) && i0 >= 2 && i0 < (int)X - 3 && j0 >= 2 && j0 < (int)Y - 3 && fx >= 0.0f && fy >= 0.0f) {
-        size_t r0 = (size_t)j0 * I.pitch + i0, r1 = r0 + I.pitch;
         float w00 = (1.0f - fx) * (1.0f - fy);
         float w10 = fx * (1.0f - fy);
         float w01 = (1.0f - fx) * fy;
         float w11 = fx * fy;
-        nvx = nvx * 0.7f + 0.3f * (__ldg(I.ovx + r0) * w00 + __ldg(I.ovx + r0 + 1) * w10 + __ldg(I.ovx + r1) * w01 +
-                                   __ldg(I.ovx + r1 + 1) * w11);
-        nvy = nvy * 0.7f + 0.3f * (__ldg(I.ovy + r0) * w00 + __ldg(I.ovy + r0 + 1) * w10 + __ldg(I.ovy + r1) * w01 +
-                                   __ldg(I.ovy + r1 + 1) * w11);
+        float a00, a10, a01, a11, b00, b10, b01, b11;
+        if (S.has3(i0, j0, x0, y0) && S.has3(i0 + 1, j0 + 1, x0, y0)) {  // sample inside the staged box
+            a00 = S.OVX(i0, j0, x0, y0);
+            a10 = S.OVX(i0 + 1, j0, x0, y0);
+            a01 = S.OVX(i0, j0 + 1, x0, y0);
+            a11 = S.OVX(i0 + 1, j0 + 1, x0, y0);
+            b00 = S.OVY(i0, j0, x0, y0);
+            b10 = S.OVY(i0 + 1, j0, x0, y0);
+            b01 = S.OVY(i0, j0 + 1, x0, y0);
+            b11 = S.OVY(i0 + 1, j0 + 1, x0, y0);
+        } else {
+            size_t r0 = (size_t)j0 * I.pitch + i0, r1 = r0 + I.pitch;
+            a00 = __ldg(I.ovx + r0);
+            a10 = __ldg(I.ovx + r0 + 1);
+            a01 = __ldg(I.ovx + r1);
+            a11 = __ldg(I.ovx + r1 + 1);
+            b00 = __ldg(I.ovy + r0);
+            b10 = __ldg(I.ovy + r0 + 1);
+            b01 = __ldg(I.ovy + r1);
+            b11 = __ldg(I.ovy + r1 + 1);
+        }
+        nvx = nvx * 0.7f + 0.3f * (a00 * w00 + a10 * w10 + a01 * w01 + a11 * w11);
+        nvy = nvy * 0.7f + 0.3f * (b00 * w00 + b10 * w10 + b01 * w01 + b11 * w11);
     }
     // advect.rs:297-328
     if (I.vcoef > 0.0f && (uint32_t)x > 1u && (uint32_t)x + 2u < X && (uint32_t)y > 1u && (uint32_t)y + 2u < Y) {
@@ -458,16 +492,30 @@ __device__ __forceinline__ float heat_cell(const AirInst &I, L &S, int x, int y,
     float dh = sh / ws;
     float svx = sx / ws, svy = sy / ws;
     float tx, ty;
-    far_advect_target(x, y, svx, svy, I.bairh, X, Y, I.pitch, true, tx, ty);
+    far_advect_target(
+        x, y, svx, svy,
+        [&](int cx, int cy) -> bool {
+            if (S.hasH(cx, cy, x0, y0)) return S.hblk(cx, cy, x0, y0);
+            return (__ldg(I.bairh + (size_t)cy * I.pitch + cx) & 0x8u) != 0u;
+        },
+        X, Y, tx, ty);
     int i0 = (int)tx, j0 = (int)ty;
     float fx = tx - (float)i0, fy = ty - (float)j0;
     const bool here_blocked = S.hblk(x, y, x0, y0);
     if (!here_blocked && i0 >= 0 && i0 < (int)X - 1 && j0 >= 0 && j0 < (int)Y - 1 && fx >= 0.0f && fy >= 0.0f) {
-        size_t r0 = (size_t)j0 * I.pitch + i0, r1 = r0 + I.pitch;
-        float s00 = (__ldg(I.bairh + r0) & 0x8u) ? dh : __ldg(I.hv + r0);
-        float s10 = (__ldg(I.bairh + r0 + 1) & 0x8u) ? dh : __ldg(I.hv + r0 + 1);
-        float s01 = (__ldg(I.bairh + r1) & 0x8u) ? dh : __ldg(I.hv + r1);
-        float s11 = (__ldg(I.bairh + r1 + 1) & 0x8u) ? dh : __ldg(I.hv + r1 + 1);
+        float s00, s10, s01, s11;
+        if (S.hasH(i0, j0, x0, y0) && S.hasH(i0 + 1, j0 + 1, x0, y0)) {  // sample inside the staged box
+            s00 = S.hblk(i0, j0, x0, y0) ? dh : S.HV(i0, j0, x0, y0);
+            s10 = S.hblk(i0 + 1, j0, x0, y0) ? dh : S.HV(i0 + 1, j0, x0, y0);
+            s01 = S.hblk(i0, j0 + 1, x0, y0) ? dh : S.HV(i0, j0 + 1, x0, y0);
+            s11 = S.hblk(i0 + 1, j0 + 1, x0, y0) ? dh : S.HV(i0 + 1, j0 + 1, x0, y0);
+        } else {
+            size_t r0 = (size_t)j0 * I.pitch + i0, r1 = r0 + I.pitch;
+            s00 = (__ldg(I.bairh + r0) & 0x8u) ? dh : __ldg(I.hv + r0);
+            s10 = (__ldg(I.bairh + r0 + 1) & 0x8u) ? dh : __ldg(I.hv + r0 + 1);
+            s01 = (__ldg(I.bairh + r1) & 0x8u) ? dh : __ldg(I.hv + r1);
+            s11 = (__ldg(I.bairh + r1 + 1) & 0x8u) ? dh : __ldg(I.hv + r1 + 1);
+        }
         float w00 = (1.0f - fx) * (1.0f - fy);
         float w10 = fx * (1.0f - fy);
         float w01 = (1.0f - fx) * fy;

@@ -45,8 +45,10 @@ constexpr int NT = 128;            // complex columns per N tile
 constexpr int STAGES = 3;
 constexpr int TILE_BYTES = MT * KT * 2;  // one plane of one tile: 8 KB
 constexpr int STAGE_BYTES = 8 * TILE_BYTES;
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024;
-constexpr int THREADS = 192;
+constexpr int EPI_WARPS = 8;             // two per TMEM lane quarter, one column half each
+constexpr int XPOSE_BYTES = 32 * 33 * 4; // per epilogue warp: a 32x32 f32 transpose buffer
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + EPI_WARPS * XPOSE_BYTES;
+constexpr int THREADS = 64 + 32 * EPI_WARPS;
 
 enum Stage : int { ST_R = 0, ST_C = 1, ST_CI = 2, ST_RI = 3 };
 
@@ -55,6 +57,7 @@ __device__ uint32_t g_dft_err;
 // One group of equal-shape instances (device copy).
 struct Group {
     uint32_t X, Y, N1, N2, N1h, G, inst0;
+    uint32_t N1hp;                       // N1h rounded up to 32: per-instance column stride of C and C^-1
     uint32_t kpR, kpC, kpCi, kpRi;       // K pitches (elements)
     uint32_t rowsR, rowsC, rowsCi, rowsRi;  // rows per plane of the data operands
     bf16 *aR, *bC, *bCi, *aRi;           // data operands (planes stacked)
@@ -112,7 +115,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         }
         for (int a = 0; a < 2; ++a) {
             tc::mbar_init(&acc_full[a], 1);
-            tc::mbar_init(&acc_empty[a], 4);
+            tc::mbar_init(&acc_empty[a], EPI_WARPS);
         }
         abort_flag = 0;
         tc::fence_mbar_init();
@@ -220,8 +223,13 @@ __global__ void __launch_bounds__(THREADS, 1)
             }
         }
     } else {
-        // ---------------- epilogue (warps 2..5) ----------------
-        const uint32_t q = warp & 3;  // TMEM lane quarter this warp may access
+        // ---------------- epilogue (warps 2..9) ----------------
+        // Warp e reads TMEM lane quarter warp%4 (the only lanes it may
+        // access) and the e/4-th half of the tile's columns, in 32-column
+        // chunks; C and C^-1 columns are padded per instance to N1hp, so a
+        // chunk never straddles an instance or field.
+        const uint32_t ew = warp - 2, q = warp & 3, half = ew >> 2;
+        float *xbuf = reinterpret_cast<float *>(smem + STAGES * STAGE_BYTES) + ew * (32 * 33);
         uint32_t acc = 0, acc_ph = 0;
         for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
             const Tile T = tiles[t];
@@ -232,19 +240,71 @@ __global__ void __launch_bounds__(THREADS, 1)
                 break;
             }
             tc::tc_fence_after();
-            const uint32_t m = T.mt * MT + q * 32 + lane;  // this thread's row
+            const uint32_t mrow0 = T.mt * MT + q * 32;  // first row of this warp
+            const uint32_t m = mrow0 + lane;            // this thread's row
             const uint32_t d = tmem + acc * 256 + ((q * 32u) << 16);
-            for (uint32_t c0 = 0; c0 < (uint32_t)NT; c0 += 32) {
+            for (uint32_t c0 = half * (NT / 2); c0 < (half + 1) * (NT / 2); c0 += 32) {
+                const uint32_t nb = T.nt * NT + c0;
+                const bool row_ok = m < P.M;
+                if constexpr (STAGE == ST_C) {
+                    // row m = ky ; col = (inst, kx) -> B operand of C^-1: row (inst, f, kx), k = ky.
+                    // S_f = B * i Ks_f: real = -Bi Ks, imag = Br Ks. Each part is
+                    // transposed through shared memory so each lane writes one
+                    // destination row's 32 consecutive ky as 16-byte stores.
+                    const uint32_t il = nb / Gp.N1hp, kx0 = nb - il * Gp.N1hp;
+                    if (mrow0 >= P.M || il >= Gp.G) continue;  // warp-uniform
+                    const size_t plane = (size_t)Gp.rowsCi * Gp.kpCi;
+                    const uint32_t kx = kx0 + lane;  // after the transpose
+#pragma unroll 1
+                    for (int part = 0; part < 2; ++part) {
+                        float v[32];
+                        tc::tmem_ld32(d + (part ? 0u : 128u) + c0, v);  // part 0 needs Bi, part 1 Br
+#pragma unroll 1
+                        for (int f = 0; f < 2; ++f) {
+                            const float *ks = f ? Gp.kys : Gp.kxs;
+                            const float sgn = part ? 1.0f : -1.0f;
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) {
+                                const float kv =
+                                    (row_ok && kx0 + j < Gp.N1h) ? __ldg(ks + (size_t)(kx0 + j) * Gp.N2 + m) : 0.0f;
+                                xbuf[lane * 33 + j] = sgn * v[j] * kv;
+                            }
+                            __syncwarp();
+                            if (kx < Gp.N1h) {
+                                bf16 *o = Gp.bCi + (size_t)((il * 2 + f) * Gp.N1hp + kx) * Gp.kpCi + mrow0 +
+                                          (size_t)(2 * part) * plane;
+                                uint32_t hw[16], lw[16];
+#pragma unroll
+                                for (int i = 0; i < 16; ++i) {
+                                    const float v0 = xbuf[(2 * i) * 33 + lane], v1 = xbuf[(2 * i + 1) * 33 + lane];
+                                    const bf16 h0 = __float2bfloat16_rn(v0), h1 = __float2bfloat16_rn(v1);
+                                    const bf16 l0 = __float2bfloat16_rn(v0 - __bfloat162float(h0));
+                                    const bf16 l1 = __float2bfloat16_rn(v1 - __bfloat162float(h1));
+                                    hw[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+                                    lw[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+                                }
+                                uint4 *oh = reinterpret_cast<uint4 *>(o), *ol = reinterpret_cast<uint4 *>(o + plane);
+#pragma unroll
+                                for (int i = 0; i < 4; ++i) {
+                                    oh[i] = make_uint4(hw[4 * i], hw[4 * i + 1], hw[4 * i + 2], hw[4 * i + 3]);
+                                    ol[i] = make_uint4(lw[4 * i], lw[4 * i + 1], lw[4 * i + 2], lw[4 * i + 3]);
+                                }
+                            }
+                            __syncwarp();
+                        }
+                    }
+                    continue;
+                }
                 float vr[32], vi[32];
                 tc::tmem_ld32(d + c0, vr);
                 if (OUT_COMPLEX) tc::tmem_ld32(d + 128 + c0, vi);
-                if (m >= P.M) continue;
-                const uint32_t nb = T.nt * NT + c0;
+                if (mrow0 >= P.M) continue;  // warp-uniform
                 if (STAGE == ST_R) {
                     // row m = (inst, y) ; col = kx -> B operand of C: row (inst, kx), k = y
+                    if (!row_ok) continue;
                     const uint32_t il = m / Gp.Y, y = m - il * Gp.Y;
                     const size_t plane = (size_t)Gp.rowsC * Gp.kpC;
-                    bf16 *o = Gp.bC + (size_t)(il * Gp.N1h + nb) * Gp.kpC + y;
+                    bf16 *o = Gp.bC + (size_t)(il * Gp.N1hp + nb) * Gp.kpC + y;
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
                         if (nb + j < Gp.N1h) {
@@ -253,57 +313,59 @@ __global__ void __launch_bounds__(THREADS, 1)
                         }
                         o += Gp.kpC;
                     }
-                } else if (STAGE == ST_C) {
-                    // row m = ky ; col = (inst, kx) -> B operand of C^-1: row (inst, f, kx), k = ky
-                    const size_t plane = (size_t)Gp.rowsCi * Gp.kpCi;
-                    uint32_t il = nb / Gp.N1h, kx = nb - il * Gp.N1h;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        if (il < Gp.G) {
-                            const float kxs = __ldg(Gp.kxs + (size_t)kx * Gp.N2 + m);
-                            const float kys = __ldg(Gp.kys + (size_t)kx * Gp.N2 + m);
-                            const float br = vr[j], bi = vi[j];
-                            bf16 *ox = Gp.bCi + (size_t)(il * 2 * Gp.N1h + kx) * Gp.kpCi + m;
-                            bf16 *oy = ox + (size_t)Gp.N1h * Gp.kpCi;
-                            split_store(ox, ox + plane, -bi * kxs);
-                            split_store(ox + 2 * plane, ox + 3 * plane, br * kxs);
-                            split_store(oy, oy + plane, -bi * kys);
-                            split_store(oy + 2 * plane, oy + 3 * plane, br * kys);
-                        }
-                        if (++kx == Gp.N1h) {
-                            kx = 0;
-                            ++il;
-                        }
-                    }
                 } else if (STAGE == ST_CI) {
-                    // row m = y ; col = (inst, f, kx) -> A operand of R^-1: row (inst, f, y), k = kx
+                    // row m = y ; col = (inst, f, kx) -> A operand of R^-1: row (inst, f, y), k = kx.
+                    // Each lane writes its own row's 32 consecutive kx as 16-byte stores.
+                    const uint32_t il = nb / (2 * Gp.N1hp), rem = nb - il * 2 * Gp.N1hp;
+                    if (il >= Gp.G || !row_ok) continue;
+                    const uint32_t f = rem >= Gp.N1hp ? 1u : 0u, kx0 = rem - f * Gp.N1hp;
                     const size_t plane = (size_t)Gp.rowsRi * Gp.kpRi;
-                    uint32_t il = nb / (2 * Gp.N1h), rem = nb - il * 2 * Gp.N1h;
+                    bf16 *o = Gp.aRi + (size_t)((il * 2 + f) * Gp.Y + m) * Gp.kpRi + kx0;
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        if (il < Gp.G) {
-                            const uint32_t f = rem >= Gp.N1h ? 1u : 0u, kx = rem - f * Gp.N1h;
-                            bf16 *o = Gp.aRi + (size_t)((il * 2 + f) * Gp.Y + m) * Gp.kpRi + kx;
-                            split_store(o, o + plane, vr[j]);
-                            split_store(o + 2 * plane, o + 3 * plane, vi[j]);
+                    for (int part = 0; part < 2; ++part) {
+                        const float *v = part ? vi : vr;
+                        uint32_t hw[16], lw[16];
+#pragma unroll
+                        for (int i = 0; i < 16; ++i) {
+                            const bf16 h0 = __float2bfloat16_rn(v[2 * i]), h1 = __float2bfloat16_rn(v[2 * i + 1]);
+                            const bf16 l0 = __float2bfloat16_rn(v[2 * i] - __bfloat162float(h0));
+                            const bf16 l1 = __float2bfloat16_rn(v[2 * i + 1] - __bfloat162float(h1));
+                            hw[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+                            lw[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
                         }
-                        if (++rem == 2 * Gp.N1h) {
-                            rem = 0;
-                            ++il;
+                        uint4 *oh = reinterpret_cast<uint4 *>(o + (size_t)(2 * part) * plane);
+                        uint4 *ol = reinterpret_cast<uint4 *>(o + (size_t)(2 * part + 1) * plane);
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            oh[i] = make_uint4(hw[4 * i], hw[4 * i + 1], hw[4 * i + 2], hw[4 * i + 3]);
+                            ol[i] = make_uint4(lw[4 * i], lw[4 * i + 1], lw[4 * i + 2], lw[4 * i + 3]);
                         }
                     }
                 } else {
-                    // row m = (inst, f, y) ; col = x -> g_f[y * X + x], masked
+                    // row m = (inst, f, y) ; col = x -> g_f[y * pitch + x], masked
+                    if (!row_ok) continue;
                     const uint32_t il = m / (2 * Gp.Y), r2 = m - il * 2 * Gp.Y;
                     const uint32_t f = r2 >= Gp.Y ? 1u : 0u, y = r2 - f * Gp.Y;
                     const uint32_t inst = Gp.inst0 + il;
                     const InstIO io = (io0_active && inst == 0) ? io0 : ios[inst];
                     float *out = (f ? io.gy : io.gx) + (size_t)y * io.pitch;
                     const uint32_t *mask = io.mask + (size_t)y * io.pitch;
+                    if (nb + 32 <= Gp.X && ((reinterpret_cast<uintptr_t>(out + nb) | reinterpret_cast<uintptr_t>(mask + nb)) & 15u) == 0u) {
+                        // whole chunk, 16-byte aligned
+                        const uint4 *mk = reinterpret_cast<const uint4 *>(mask + nb);
+                        float4 *o4 = reinterpret_cast<float4 *>(out + nb);
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const uint32_t x = nb + j;
-                        if (x < Gp.X) out[x] = __ldg(mask + x) != 0u ? vr[j] : 0.0f;
+                        for (int i = 0; i < 8; ++i) {
+                            const uint4 mm = __ldg(mk + i);
+                            o4[i] = make_float4(mm.x ? vr[4 * i] : 0.0f, mm.y ? vr[4 * i + 1] : 0.0f,
+                                                mm.z ? vr[4 * i + 2] : 0.0f, mm.w ? vr[4 * i + 3] : 0.0f);
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const uint32_t x = nb + j;
+                            if (x < Gp.X) out[x] = __ldg(mask + x) != 0u ? vr[j] : 0.0f;
+                        }
                     }
                 }
             }
@@ -539,6 +601,7 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
         g.N1 = 2 * g.X;
         g.N2 = 2 * g.Y;
         g.N1h = g.N1 / 2 + 1;
+        g.N1hp = round_up(g.N1h, 32);
         g.G = (uint32_t)members[gi].size();
         g.inst0 = inst0;
         for (uint32_t l = 0; l < g.G; ++l) {
@@ -551,8 +614,8 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
         g.kpCi = round_up(g.N2, KT);
         g.kpRi = round_up(g.N1h, KT);
         g.rowsR = g.G * g.Y;
-        g.rowsC = g.G * g.N1h;
-        g.rowsCi = 2 * g.G * g.N1h;
+        g.rowsC = g.G * g.N1hp;
+        g.rowsCi = 2 * g.G * g.N1hp;
         g.rowsRi = 2 * g.G * g.Y;
         H.kpF1 = g.kpR;   // F1: N1h rows, K = x
         H.kpF2 = g.kpC;   // F2: N2 rows, K = y
