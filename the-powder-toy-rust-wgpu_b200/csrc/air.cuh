@@ -361,26 +361,46 @@ __device__ __forceinline__ void smooth_advect_cell(const AirInst &I, L &S, int x
     const uint32_t X = I.X, Y = I.Y;
     const float cvx = S.OVX(x, y, x0, y0), cvy = S.OVY(x, y, x0, y0), cpv = S.OPV(x, y, x0, y0);
     float sx = 0.0f, sy = 0.0f, sp = 0.0f, ws = 0.0f;
+    if ((uint32_t)x >= 2u && (uint32_t)x + 3u <= X && (uint32_t)y >= 2u && (uint32_t)y + 3u <= Y) {
+        // every tap is an interior cell: fixed offsets, no saturation
 #pragma unroll
-    for (int dyy = 0; dyy < 3; ++dyy) {
+        for (int dyy = 0; dyy < 3; ++dyy) {
 #pragma unroll
-        for (int dxx = 0; dxx < 3; ++dxx) {
-            uint32_t nx = (uint32_t)x + dxx;
-            nx = nx >= 1u ? nx - 1u : 0u;
-            uint32_t ny = (uint32_t)y + dyy;
-            ny = ny >= 1u ? ny - 1u : 0u;
-            float w = smooth_w(dxx, dyy);
-            bool itap = nx >= 1u && ny >= 1u && nx + 1u < X && ny + 1u < Y;
-            float tx = cvx, ty = cvy, tp = cpv;
-            if (itap && !S.blk(nx, ny, x0, y0)) {
-                tx = S.OVX(nx, ny, x0, y0);
-                ty = S.OVY(nx, ny, x0, y0);
-                tp = S.OPV(nx, ny, x0, y0);
+            for (int dxx = 0; dxx < 3; ++dxx) {
+                const int nx = x + dxx - 1, ny = y + dyy - 1;
+                const float w = smooth_w(dxx, dyy);
+                const bool open = !S.blk(nx, ny, x0, y0);
+                const float tx = open ? S.OVX(nx, ny, x0, y0) : cvx;
+                const float ty = open ? S.OVY(nx, ny, x0, y0) : cvy;
+                const float tp = open ? S.OPV(nx, ny, x0, y0) : cpv;
+                sx += tx * w;
+                sy += ty * w;
+                sp += tp * w;
+                ws += w;
             }
-            sx += tx * w;
-            sy += ty * w;
-            sp += tp * w;
-            ws += w;
+        }
+    } else {
+#pragma unroll
+        for (int dyy = 0; dyy < 3; ++dyy) {
+#pragma unroll
+            for (int dxx = 0; dxx < 3; ++dxx) {
+                uint32_t nx = (uint32_t)x + dxx;
+                nx = nx >= 1u ? nx - 1u : 0u;
+                uint32_t ny = (uint32_t)y + dyy;
+                ny = ny >= 1u ? ny - 1u : 0u;
+                float w = smooth_w(dxx, dyy);
+                bool itap = nx >= 1u && ny >= 1u && nx + 1u < X && ny + 1u < Y;
+                float tx = cvx, ty = cvy, tp = cpv;
+                if (itap && !S.blk(nx, ny, x0, y0)) {
+                    tx = S.OVX(nx, ny, x0, y0);
+                    ty = S.OVY(nx, ny, x0, y0);
+                    tp = S.OPV(nx, ny, x0, y0);
+                }
+                sx += tx * w;
+                sy += ty * w;
+                sp += tp * w;
+                ws += w;
+            }
         }
     }
     float nvx = sx / ws, nvy = sy / ws, npv = sp / ws;
@@ -467,26 +487,46 @@ __device__ __forceinline__ float heat_cell(const AirInst &I, L &S, int x, int y,
     const uint32_t X = I.X, Y = I.Y;
     const float ch = S.HV(x, y, x0, y0), cvx = S.NVX(x, y, x0, y0), cvy = S.NVY(x, y, x0, y0);
     float sh = 0.0f, sx = 0.0f, sy = 0.0f, ws = 0.0f;
+    if ((uint32_t)x >= 2u && (uint32_t)x + 3u <= X && (uint32_t)y >= 2u && (uint32_t)y + 3u <= Y) {
+        // every tap is an interior cell: fixed offsets, no saturation
 #pragma unroll
-    for (int dyy = 0; dyy < 3; ++dyy) {
+        for (int dyy = 0; dyy < 3; ++dyy) {
 #pragma unroll
-        for (int dxx = 0; dxx < 3; ++dxx) {
-            uint32_t nx = (uint32_t)x + dxx;
-            nx = nx >= 1u ? nx - 1u : 0u;
-            uint32_t ny = (uint32_t)y + dyy;
-            ny = ny >= 1u ? ny - 1u : 0u;
-            float w = smooth_w(dxx, dyy);
-            bool itap = nx >= 1u && ny >= 1u && nx + 1u < X && ny + 1u < Y;
-            float th = ch, tx = cvx, ty = cvy;
-            if (itap && !S.hblk(nx, ny, x0, y0)) {
-                th = S.HV(nx, ny, x0, y0);
-                tx = S.NVX(nx, ny, x0, y0);
-                ty = S.NVY(nx, ny, x0, y0);
+            for (int dxx = 0; dxx < 3; ++dxx) {
+                const int nx = x + dxx - 1, ny = y + dyy - 1;
+                const float w = smooth_w(dxx, dyy);
+                const bool open = !S.hblk(nx, ny, x0, y0);
+                const float th = open ? S.HV(nx, ny, x0, y0) : ch;
+                const float tx = open ? S.NVX(nx, ny, x0, y0) : cvx;
+                const float ty = open ? S.NVY(nx, ny, x0, y0) : cvy;
+                sh += th * w;
+                sx += tx * w;
+                sy += ty * w;
+                ws += w;
             }
-            sh += th * w;
-            sx += tx * w;
-            sy += ty * w;
-            ws += w;
+        }
+    } else {
+#pragma unroll
+        for (int dyy = 0; dyy < 3; ++dyy) {
+#pragma unroll
+            for (int dxx = 0; dxx < 3; ++dxx) {
+                uint32_t nx = (uint32_t)x + dxx;
+                nx = nx >= 1u ? nx - 1u : 0u;
+                uint32_t ny = (uint32_t)y + dyy;
+                ny = ny >= 1u ? ny - 1u : 0u;
+                float w = smooth_w(dxx, dyy);
+                bool itap = nx >= 1u && ny >= 1u && nx + 1u < X && ny + 1u < Y;
+                float th = ch, tx = cvx, ty = cvy;
+                if (itap && !S.hblk(nx, ny, x0, y0)) {
+                    th = S.HV(nx, ny, x0, y0);
+                    tx = S.NVX(nx, ny, x0, y0);
+                    ty = S.NVY(nx, ny, x0, y0);
+                }
+                sh += th * w;
+                sx += tx * w;
+                sy += ty * w;
+                ws += w;
+            }
         }
     }
     float dh = sh / ws;

@@ -693,10 +693,18 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
         pr[4 * gi + 3] = {tmd + 6, tmd + 7, gi32, g.rowsRi, g.X, g.kpRi / KT, g.rowsRi, g.X};
         for (int st = 0; st < 4; ++st) {
             const Problem &P = pr[4 * gi + st];
-            // M tiles fastest so consecutive CTAs share the B tile (L2 reuse)
-            for (uint32_t nt = 0; nt * NT < P.N; ++nt)
+            // Consecutive CTAs share the data operand's tile (L2 reuse): in C and
+            // C^-1 the data is B (M tiles fastest), in R and R^-1 it is A (N
+            // tiles fastest); the other operand is a small constant matrix.
+            if (st == ST_C || st == ST_CI) {
+                for (uint32_t nt = 0; nt * NT < P.N; ++nt)
+                    for (uint32_t mt = 0; mt * MT < P.M; ++mt)
+                        tl[st].push_back({(uint32_t)(4 * gi + st), (uint16_t)mt, (uint16_t)nt});
+            } else {
                 for (uint32_t mt = 0; mt * MT < P.M; ++mt)
-                    tl[st].push_back({(uint32_t)(4 * gi + st), (uint16_t)mt, (uint16_t)nt});
+                    for (uint32_t nt = 0; nt * NT < P.N; ++nt)
+                        tl[st].push_back({(uint32_t)(4 * gi + st), (uint16_t)mt, (uint16_t)nt});
+            }
         }
         for (uint32_t r = 0; r < g.rowsR; ++r) pref.push_back({gi32, r});
     }
