@@ -113,10 +113,7 @@ class ClockSampler:
 def workload(cid: int):
     import workloads as W
 
-    insts = W.config_instances(cid)
-    if cid == 5:
-        pass
-    return insts
+    return W.config_instances(cid)
 
 
 def dist_setup(gpus: int):
@@ -232,15 +229,23 @@ def run_ours(args, rank, world, local):
 
     import tpt_field as tf
 
+    import sharding
+
     tf.lib()
     cid = args.workload
     insts = workload(cid)
+    total_cells = sum(i.cells for i in insts)
+    if args.scaling == "strong" and world > 1:  # this rank's share, no exchange between ranks
+        insts = [insts[i] for i in sharding.shard_of([(i.xcells, i.ycells) for i in insts], rank, world)]
     ticks = args.ticks or (1000 if cid in (4, 5) else (1000 if cid == 1 else 10000))
     precision = tf.PRECISION_SPLIT_BF16 if cid == 5 else tf.PRECISION_FP32
     stream = torch.cuda.current_stream()
     batch = tf.Batch(insts, precision)
     batch.tune()
     cells = sum(i.cells for i in insts)
+    # cells all ranks advance per tick: every rank has a full copy (weak) or
+    # a share of one copy (strong)
+    job_cells = total_cells if args.scaling == "strong" else total_cells * world
 
     # device-timed: inputs resident
     for _ in range(args.warmup):
@@ -259,7 +264,7 @@ def run_ours(args, rank, world, local):
     clk = clocks.stop()
     barrier(world)
     ms = max_over_ranks(e0.elapsed_time(e1), world)
-    value = cells * ticks * args.steps * world / (ms / 1e3)
+    value = job_cells * ticks * args.steps / (ms / 1e3)
 
     # end to end through the C ABI with pinned host buffers
     names = [n for n, _ in tf.Batch.GRIDS]
@@ -301,7 +306,7 @@ def run_ours(args, rank, world, local):
         torch.cuda.synchronize()
         barrier(world)
         e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
-        e2e_value = cells * ticks * e2e_steps * world / (e2e_ms / 1e3)
+        e2e_value = job_cells * ticks * e2e_steps / (e2e_ms / 1e3)
 
     # per-phase device times for the roofline
     prof = batch.profile_phases(args.phase_ticks)
@@ -341,7 +346,7 @@ def run_ours(args, rank, world, local):
         line = {
             "metric": "cell-ticks/s", "value": value, "unit": "cell-ticks/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True, "scaling": args.scaling, "vs_baseline": None,
             "dtype": "f32" if precision == tf.PRECISION_FP32 else "f32 air + bf16x3 gravity (f32 accumulate)",
             "data": "synthetic (seeded sandboxes, workloads.py)",
             "config": {"workload": WORKLOAD_NAMES[cid], "instances": len(insts), "cells": cells,
@@ -392,6 +397,8 @@ def main():
     ap.add_argument("--workload", type=int, choices=(1, 2, 4, 5), default=5)
     ap.add_argument("--ticks", type=int, default=0)
     ap.add_argument("--plain-ticks", type=int, default=500, help="ticks of the plain FP32 comparison (0 = skip)")
+    ap.add_argument("--scaling", choices=("weak", "strong"), default="weak",
+                    help="weak: every rank steps a full copy; strong: ranks split one copy's instances")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer run (profiling captures)")
