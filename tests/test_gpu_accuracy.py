@@ -1,0 +1,86 @@
+"""Error figures of every measured workload against the FP64 oracle, checked
+against the stated bars and written out (JSON) when TPT_REPORT_DIR is set.
+
+  gravity  gx/gy rel-max = max|g - g64| / max|g64|, rel-L2 = ||g - g64|| /
+           ||g64||; bar 1e-4 (split-BF16) and 1e-5 (FP32 plan)
+  air      100 ticks on the GPU (bit-identical to the FP32 restatement of
+           the reference kernels) against the FP64 twin: rel-L2 of pv, vx,
+           vy, hv -- the reference algorithm's own FP32 error, reported; the
+           GPU-vs-FP32-reference bar (bit-exact) is in test_gpu_air.py
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+REPORT = {}
+
+
+def _err(g, ref):
+    g = g.astype(np.float64)
+    return (float(np.abs(g - ref).max() / max(np.abs(ref).max(), 1e-30)),
+            float(np.linalg.norm(g - ref) / max(np.linalg.norm(ref), 1e-30)))
+
+
+def _dump():
+    d = os.environ.get("TPT_REPORT_DIR")
+    if d:
+        os.makedirs(d, exist_ok=True)
+        with open(os.path.join(d, "accuracy.json"), "w") as f:
+            json.dump(REPORT, f, indent=1, sort_keys=True)
+
+
+@pytest.mark.parametrize("case", ["C1", "C2", "C3", "C5-400x225", "C5-small"])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_gravity_error_vs_fp64(cuda, tf, oracle, case, precision):
+    import workloads as W
+    from test_gpu_grav import solve_gpu
+
+    mass_fx = mass_f = None
+    if case == "C3":
+        X = Y = 512
+        mass_f = W.clustered_mass(X, Y, W.instance_seed(3, 0))
+        mask = np.full(X * Y, 0xFFFFFFFF, np.uint32)
+    else:
+        if case == "C1":
+            inst = W.config_instances(1)[0]
+        elif case == "C2":
+            inst = W.config_instances(2)[0]
+        elif case == "C5-400x225":
+            inst = W.config_instances(5, limit=1)[0]
+        else:
+            inst = W.config_instances(5)[70]
+        X, Y, mask, mass_fx = inst.xcells, inst.ycells, inst.gmask, inst.mass_fx
+    gx, gy = solve_gpu(tf, cuda, X, Y, mask, mass_fx, mass_f, precision=precision)
+    assert tf.lib().tpt_check_device_errors() == 0
+    dx, dy = oracle.grav_solve(X, Y, mask, mass_fx=mass_fx, mass_f32=mass_f, dtype=np.float64)
+    ex, ey = _err(gx, dx), _err(gy, dy)
+    name = "split_bf16" if precision else "fp32"
+    REPORT[f"gravity/{name}/{case} ({X}x{Y})"] = {"gx_relmax": ex[0], "gx_relL2": ex[1], "gy_relmax": ey[0],
+                                                  "gy_relL2": ey[1]}
+    _dump()
+    bar = 1e-4 if precision else 1e-5
+    assert max(ex + ey) <= bar
+
+
+@pytest.mark.parametrize("case", ["C1", "C2"])
+def test_air_100_ticks_vs_fp64(cuda, tf, oracle, case):
+    import workloads as W
+
+    inst = W.config_instances(1 if case == "C1" else 2)[0]
+    b = tf.SimBuffers.from_instance(inst)
+    for _ in range(100):
+        tf.step_air_gpu(b)
+    cuda.cuda.synchronize()
+    got = b.air_state()
+    want32 = oracle.air_steps(inst, 100)
+    want64 = oracle.air_steps(inst, 100, dtype=np.float64)
+    rec = {}
+    for k in ("pv", "vx", "vy", "hv"):
+        assert np.array_equal(got[k].view(np.uint32), want32[k].view(np.uint32)), k
+        rec[f"{k}_relL2"] = float(np.linalg.norm(got[k] - want64[k]) / max(np.linalg.norm(want64[k]), 1e-30))
+        rec[f"{k}_relmax"] = float(np.abs(got[k] - want64[k]).max() / max(np.abs(want64[k]).max(), 1e-30))
+    REPORT[f"air/100 ticks/{case} ({inst.xcells}x{inst.ycells}) vs fp64"] = rec
+    _dump()
