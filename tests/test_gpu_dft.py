@@ -90,3 +90,61 @@ def test_split_bf16_batch_mixed_shapes(cuda, tf, oracle):
             emax, el2 = errors(g, d)
             assert emax <= TOL and el2 <= TOL, (i, emax, el2)
     b.close()
+
+
+@pytest.mark.parametrize("ymode", ["toeplitz", "dft"])
+@pytest.mark.parametrize("X,Y,kind", [(37, 29, "stress"), (153, 96, "c1"), (400, 225, "c2"), (32, 130, "stress"),
+                                      (130, 33, "stress")])
+def test_split_bf16_forced_y_form_vs_fp64(cuda, tf, oracle, monkeypatch, ymode, X, Y, kind):
+    """Both forms of the y stage (y DFT pair, or direct Toeplitz GEMM per x
+    frequency with an MN-major R^-1 operand) meet the bar on their own."""
+    import workloads as W
+    from test_gpu_grav import solve_gpu
+
+    monkeypatch.setenv("TPT_SPLIT_BF16_Y_STAGE", ymode)
+    if kind == "c1":
+        inst = W.config_instances(1)[0]
+    elif kind == "c2":
+        inst = W.config_instances(2)[0]
+    else:
+        inst = W.make_stress_instance(X, Y, 17 * X + Y)
+    gx, gy = solve_gpu(tf, cuda, X, Y, inst.gmask, inst.mass_fx, precision=tf.PRECISION_SPLIT_BF16)
+    check_clean(tf)
+    dx, dy = oracle.grav_solve(X, Y, inst.gmask, mass_fx=inst.mass_fx, dtype=np.float64)
+    for g, d in ((gx, dx), (gy, dy)):
+        emax, el2 = errors(g, d)
+        assert emax <= TOL and el2 <= TOL, (ymode, emax, el2)
+    assert np.all(gx[inst.gmask == 0] == 0) and np.all(gy[inst.gmask == 0] == 0)
+
+
+@pytest.mark.parametrize("ymode", ["toeplitz:2", "toeplitz", "auto"])
+def test_split_bf16_batch_mixed_y_forms(cuda, tf, oracle, monkeypatch, ymode):
+    """One set whose groups use different y forms: the pair of 400x225 and
+    the pair of 57x36 go through T (toeplitz:2), the singletons through the
+    y DFT, with both y stages launched in the same solve. Repeating the
+    solve gives identical fields."""
+    import workloads as W
+
+    monkeypatch.setenv("TPT_SPLIT_BF16_Y_STAGE", ymode)
+    insts = W.config_instances(5, limit=2)  # two 400x225
+    insts += [W.make_instance(57, 36, 5, mass_density=0.02), W.make_instance(33, 151, 6, mass_density=0.02),
+              W.make_instance(57, 36, 7, mass_density=0.02), W.make_instance(200, 40, 8, mass_density=0.02)]
+    b = tf.Batch(insts, tf.PRECISION_SPLIT_BF16)
+    prof = b.profile_phases(2)
+    if ymode == "toeplitz:2":
+        assert prof.grav_launches_per_tick == 6  # prep, R, C, C^-1, T, R^-1
+    b.step(2)
+    cuda.cuda.synchronize()
+    check_clean(tf)
+    first = [b.state(i) for i in range(len(insts))]
+    b.step(1)
+    cuda.cuda.synchronize()
+    for i, inst in enumerate(insts):
+        st = b.state(i)
+        dx, dy = oracle.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx, dtype=np.float64)
+        for g, d in ((st["gx"], dx), (st["gy"], dy)):
+            emax, el2 = errors(g, d)
+            assert emax <= TOL and el2 <= TOL, (ymode, i, emax, el2)
+        # gravity reads the previous tick's mass, which the air step leaves alone
+        assert np.array_equal(st["gx"], first[i]["gx"]) and np.array_equal(st["gy"], first[i]["gy"])
+    b.close()

@@ -18,14 +18,29 @@
 // groups' tiles run in one persistent launch per stage. The kernel spectra
 // and DFT matrices are built once in FP64 on the device.
 //
-// GEMM kernel: 192 threads. Warp 0 issues TMA tile loads (64-byte swizzle,
+// Groups with many instances replace the C / C^-1 pair by one direct
+// (Toeplitz) convolution along y per x frequency, which needs no padding to
+// 2Y and no y spectrum:
+//
+//   T    C_f[y,kx] = sum_y' Tf_kx[y - y'] A[y',kx]     Tf_kx(dy) = sum_dx K_f(dx,dy) e^{-2 pi i kx dx/N1} / N1
+//
+// Tx is purely imaginary (Kx is odd in dx) and Ty real (Ky is even in dx),
+// so T is a real GEMM per (f, kx): M = Y, K = Y, N = the group's instances'
+// real and imaginary parts. Its epilogue writes R^-1's A operand M-major
+// ([kx][inst*Y + y]), which R^-1 reads as an MN-major tcgen05 operand. A
+// cost model picks the form per group (many instances amortise the Y x Y
+// matrices; a lone instance is cheaper through the y DFT).
+//
+// GEMM kernel: 320 threads. Warp 0 issues TMA tile loads (64-byte swizzle,
 // 32-wide K tiles, no multicast) into a 3-stage shared-memory ring; warp 1
-// issues tcgen05.mma (M=128, N=256/128, K=16) into a double-buffered TMEM
-// accumulator; warps 2-5 read the accumulator with tcgen05.ld and run the
+// issues tcgen05.mma (M=128, N<=256, K=16) into a double-buffered TMEM
+// accumulator; warps 2-9 read the accumulator with tcgen05.ld and run the
 // stage's epilogue, which writes the next stage's operand planes. Every
 // mbarrier wait is bounded (see tc.cuh).
 #include <cudaTypedefs.h>
 #include <math.h>
+#include <stdlib.h>
+#include <string.h>
 
 #include <algorithm>
 #include <map>
@@ -50,7 +65,7 @@ constexpr int XPOSE_BYTES = 32 * 33 * 4; // per epilogue warp: a 32x32 f32 trans
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + EPI_WARPS * XPOSE_BYTES;
 constexpr int THREADS = 64 + 32 * EPI_WARPS;
 
-enum Stage : int { ST_R = 0, ST_C = 1, ST_CI = 2, ST_RI = 3 };
+enum Stage : int { ST_R = 0, ST_C = 1, ST_CI = 2, ST_RI = 3, ST_T = 4 };
 
 __device__ uint32_t g_dft_err;
 
@@ -60,7 +75,12 @@ struct Group {
     uint32_t N1hp;                       // N1h rounded up to 32: per-instance column stride of C and C^-1
     uint32_t kpR, kpC, kpCi, kpRi;       // K pitches (elements)
     uint32_t rowsR, rowsC, rowsCi, rowsRi;  // rows per plane of the data operands
-    bf16 *aR, *bC, *bCi, *aRi;           // data operands (planes stacked)
+    uint32_t toe;                        // 1: y stage is the Toeplitz GEMM T
+    uint32_t rowsT;                      // T: rows per plane of B (N1h * 2G)
+    uint32_t nT;                         // T: MMA N (2G rounded up to 16, at most NT)
+    uint32_t MpT;                        // T: row length of aRiT (G*Y rounded up to 32)
+    bf16 *aR, *bC, *bCi, *aRi;           // data operands (planes stacked), DFT form
+    bf16 *bT, *aRiT;                     // T's B operand; R^-1's A operand [plane][f][kx][inst*Y + y]
     const float *kxs, *kys;              // imaginary parts of the kernel spectra, [kx][ky]
 };
 
@@ -76,11 +96,13 @@ struct InstIO {
 struct Problem {
     const CUtensorMap *ta, *tb;
     uint32_t group, M, N, ktiles, a_rows, b_rows;
+    uint32_t a_mn;  // R^-1 of a Toeplitz group: A is MN-major (aRiT), field f = a_mn - 1
 };
 
 struct Tile {
     uint32_t problem;
     uint16_t mt, nt;
+    uint32_t sub;  // Toeplitz stage: f * N1h + kx (the matrix of this tile)
 };
 
 // ---- helpers ---------------------------------------------------------------
@@ -96,10 +118,12 @@ __global__ void __launch_bounds__(THREADS, 1)
     dft_gemm(const Problem *__restrict__ probs, const Tile *__restrict__ tiles, uint32_t ntiles,
              const Group *__restrict__ groups, const InstIO *__restrict__ ios, InstIO io0, int io0_active,
              uint32_t *err) {
-    constexpr bool A_COMPLEX = STAGE != ST_R;
-    constexpr bool OUT_COMPLEX = STAGE != ST_RI;
+    constexpr bool A_COMPLEX = STAGE != ST_R && STAGE != ST_T;
+    constexpr bool B_COMPLEX = STAGE != ST_T;
+    constexpr bool OUT_COMPLEX = STAGE != ST_RI && STAGE != ST_T;
     constexpr uint32_t A_PLANES = A_COMPLEX ? 4 : 2;
-    constexpr uint32_t TX_BYTES = (A_PLANES + 4) * TILE_BYTES;
+    constexpr uint32_t B_PLANES = B_COMPLEX ? 4 : 2;
+    constexpr uint32_t TX_BYTES = (A_PLANES + B_PLANES) * TILE_BYTES;
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -133,7 +157,13 @@ __global__ void __launch_bounds__(THREADS, 1)
             for (uint32_t t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x) {
                 const Tile T = tiles[t];
                 const Problem P = probs[T.problem];
-                const int32_t m0 = T.mt * MT, n0 = T.nt * NT;
+                int32_t m0 = T.mt * MT, n0 = T.nt * NT;
+                if (STAGE == ST_T) {  // this tile's Toeplitz matrix and frequency slice
+                    const Group &Gq = groups[P.group];
+                    const uint32_t kx = T.sub % Gq.N1h;
+                    m0 += (int32_t)(T.sub * Gq.Y);
+                    n0 += (int32_t)(kx * 2 * Gq.G);
+                }
                 for (uint32_t kt = 0; kt < P.ktiles; ++kt) {
                     if (!tc::mbar_wait(&empty_bar[s], ph ^ 1u, err)) {
                         abort_flag = 1;
@@ -142,14 +172,26 @@ __global__ void __launch_bounds__(THREADS, 1)
                     uint8_t *st = smem + s * STAGE_BYTES;
                     tc::mbar_arrive_expect_tx(&full_bar[s], TX_BYTES);
                     const int32_t k0 = kt * KT;
-                    for (uint32_t p = 0; p < A_PLANES; ++p)
-                        tc::tma_load_2d(st + p * TILE_BYTES, P.ta, k0, (int32_t)(p * P.a_rows) + m0, &full_bar[s]);
-                    // B: hi block [r_hi | i_hi], lo block [r_lo | i_lo]
+                    if (STAGE == ST_RI && P.a_mn) {
+                        // MN-major A: per plane four 32(m) x 32(k) boxes, 2 KB apart
+                        const uint32_t f = P.a_mn - 1;
+                        for (uint32_t p = 0; p < A_PLANES; ++p)
+                            for (uint32_t j = 0; j < 4; ++j)
+                                tc::tma_load_2d(st + p * TILE_BYTES + j * 2048, P.ta, m0 + (int32_t)(32 * j),
+                                                (int32_t)((p * 2 + f) * P.a_rows) + k0, &full_bar[s]);
+                    } else {
+                        for (uint32_t p = 0; p < A_PLANES; ++p)
+                            tc::tma_load_2d(st + p * TILE_BYTES, P.ta, k0, (int32_t)(p * P.a_rows) + m0,
+                                            &full_bar[s]);
+                    }
+                    // B: hi block [r_hi | i_hi], lo block [r_lo | i_lo] (real B: r only)
                     uint8_t *bb = st + 4 * TILE_BYTES;
                     tc::tma_load_2d(bb + 0 * TILE_BYTES, P.tb, k0, (int32_t)(0 * P.b_rows) + n0, &full_bar[s]);
-                    tc::tma_load_2d(bb + 1 * TILE_BYTES, P.tb, k0, (int32_t)(2 * P.b_rows) + n0, &full_bar[s]);
                     tc::tma_load_2d(bb + 2 * TILE_BYTES, P.tb, k0, (int32_t)(1 * P.b_rows) + n0, &full_bar[s]);
-                    tc::tma_load_2d(bb + 3 * TILE_BYTES, P.tb, k0, (int32_t)(3 * P.b_rows) + n0, &full_bar[s]);
+                    if (B_COMPLEX) {
+                        tc::tma_load_2d(bb + 1 * TILE_BYTES, P.tb, k0, (int32_t)(2 * P.b_rows) + n0, &full_bar[s]);
+                        tc::tma_load_2d(bb + 3 * TILE_BYTES, P.tb, k0, (int32_t)(3 * P.b_rows) + n0, &full_bar[s]);
+                    }
                     if (++s == STAGES) {
                         s = 0;
                         ph ^= 1u;
@@ -160,11 +202,15 @@ __global__ void __launch_bounds__(THREADS, 1)
     } else if (warp == 1) {
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
-            constexpr uint32_t I256 = tc::idesc_bf16(128, 256), I128 = tc::idesc_bf16(128, 128);
-            constexpr uint32_t I128N = tc::idesc_bf16(128, 128, true);
+            constexpr uint32_t I256 = tc::idesc_bf16(128, 256);
             uint32_t s = 0, ph = 0, acc = 0, acc_ph = 0;
             for (uint32_t t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x) {
                 const Problem P = probs[tiles[t].problem];
+                // MN-major A only in R^-1 of Toeplitz groups; T's N is the group's column count
+                const bool amn = STAGE == ST_RI && P.a_mn != 0;
+                const uint32_t nmma = STAGE == ST_T ? groups[P.group].nT : 128u;
+                const uint32_t I128 = tc::idesc_bf16(128, nmma, false, amn);
+                const uint32_t I128N = tc::idesc_bf16(128, 128, true, amn);
                 if (!tc::mbar_wait(&acc_empty[acc], acc_ph ^ 1u, err)) {
                     abort_flag = 1;
                     break;
@@ -178,35 +224,46 @@ __global__ void __launch_bounds__(THREADS, 1)
                     }
                     tc::tc_fence_after();
                     const uint32_t st = tc::smem_u32(smem + s * STAGE_BYTES);
-                    const uint32_t arh = st, arl = st + TILE_BYTES, aih = st + 2 * TILE_BYTES,
-                                   ail = st + 3 * TILE_BYTES;
                     const uint32_t bhi = st + 4 * TILE_BYTES, blo = st + 6 * TILE_BYTES;
 #pragma unroll
                     for (int j = 0; j < KT / 16; ++j) {
-                        const uint32_t o = j * 32;  // 16 bf16 along K
+                        const uint32_t o = j * 32;  // 16 bf16 along K (K-major rows)
                         const uint32_t first = (kt == 0 && j == 0) ? 0u : 1u;
-                        if (OUT_COMPLEX) {
+                        // A planes: K-major (+32 B per K step) or MN-major (+16 rows of 64 B)
+                        auto ad = [&](uint32_t plane) {
+                            const uint32_t a = st + plane * TILE_BYTES;
+                            return amn ? tc::sdesc_mn64(a + j * 1024, 2048, 512) : tc::sdesc_k64(a + o);
+                        };
+                        const uint64_t arh = ad(0), arl = ad(1);
+                        if (STAGE == ST_T) {
+                            // D = A * B, real x real
+                            tc::mma_bf16(d, arh, tc::sdesc_k64(bhi + o), I128, first);
+                            tc::mma_bf16(d, arh, tc::sdesc_k64(blo + o), I128, 1);
+                            tc::mma_bf16(d, arl, tc::sdesc_k64(bhi + o), I128, 1);
+                        } else if (OUT_COMPLEX) {
                             // [Dr | Di] += Ar * [Br | Bi]
-                            tc::mma_bf16(d, tc::sdesc_k64(arh + o), tc::sdesc_k64(bhi + o), I256, first);
-                            tc::mma_bf16(d, tc::sdesc_k64(arh + o), tc::sdesc_k64(blo + o), I256, 1);
-                            tc::mma_bf16(d, tc::sdesc_k64(arl + o), tc::sdesc_k64(bhi + o), I256, 1);
+                            tc::mma_bf16(d, arh, tc::sdesc_k64(bhi + o), I256, first);
+                            tc::mma_bf16(d, arh, tc::sdesc_k64(blo + o), I256, 1);
+                            tc::mma_bf16(d, arl, tc::sdesc_k64(bhi + o), I256, 1);
                             if (A_COMPLEX) {
+                                const uint64_t aih = ad(2), ail = ad(3);
                                 // Dr -= Ai * Bi ; Di += Ai * Br
-                                tc::mma_bf16(d, tc::sdesc_k64(aih + o), tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
-                                tc::mma_bf16(d, tc::sdesc_k64(aih + o), tc::sdesc_k64(blo + TILE_BYTES + o), I128N, 1);
-                                tc::mma_bf16(d, tc::sdesc_k64(ail + o), tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
-                                tc::mma_bf16(d + 128, tc::sdesc_k64(aih + o), tc::sdesc_k64(bhi + o), I128, 1);
-                                tc::mma_bf16(d + 128, tc::sdesc_k64(aih + o), tc::sdesc_k64(blo + o), I128, 1);
-                                tc::mma_bf16(d + 128, tc::sdesc_k64(ail + o), tc::sdesc_k64(bhi + o), I128, 1);
+                                tc::mma_bf16(d, aih, tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
+                                tc::mma_bf16(d, aih, tc::sdesc_k64(blo + TILE_BYTES + o), I128N, 1);
+                                tc::mma_bf16(d, ail, tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
+                                tc::mma_bf16(d + 128, aih, tc::sdesc_k64(bhi + o), I128, 1);
+                                tc::mma_bf16(d + 128, aih, tc::sdesc_k64(blo + o), I128, 1);
+                                tc::mma_bf16(d + 128, ail, tc::sdesc_k64(bhi + o), I128, 1);
                             }
                         } else {
                             // Dr = Ar * Br - Ai * Bi
-                            tc::mma_bf16(d, tc::sdesc_k64(arh + o), tc::sdesc_k64(bhi + o), I128, first);
-                            tc::mma_bf16(d, tc::sdesc_k64(arh + o), tc::sdesc_k64(blo + o), I128, 1);
-                            tc::mma_bf16(d, tc::sdesc_k64(arl + o), tc::sdesc_k64(bhi + o), I128, 1);
-                            tc::mma_bf16(d, tc::sdesc_k64(aih + o), tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
-                            tc::mma_bf16(d, tc::sdesc_k64(aih + o), tc::sdesc_k64(blo + TILE_BYTES + o), I128N, 1);
-                            tc::mma_bf16(d, tc::sdesc_k64(ail + o), tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
+                            const uint64_t aih = ad(2), ail = ad(3);
+                            tc::mma_bf16(d, arh, tc::sdesc_k64(bhi + o), I128, first);
+                            tc::mma_bf16(d, arh, tc::sdesc_k64(blo + o), I128, 1);
+                            tc::mma_bf16(d, arl, tc::sdesc_k64(bhi + o), I128, 1);
+                            tc::mma_bf16(d, aih, tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
+                            tc::mma_bf16(d, aih, tc::sdesc_k64(blo + TILE_BYTES + o), I128N, 1);
+                            tc::mma_bf16(d, ail, tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
                         }
                     }
                     tc::mma_commit(&empty_bar[s]);  // frees the stage when these MMAs finish
@@ -295,14 +352,52 @@ __global__ void __launch_bounds__(THREADS, 1)
                     }
                     continue;
                 }
+                if constexpr (STAGE == ST_T) {
+                    // row m = y of the (f, kx) matrix ; col = (inst, re/im) -> R^-1's
+                    // M-major A operand aRiT[plane][f][kx][inst * Y + y]. Lanes are
+                    // consecutive y, so every store is a 64-byte run.
+                    if (mrow0 >= Gp.Y || nb >= 2 * Gp.G) continue;  // warp-uniform
+                    float v[32];
+                    tc::tmem_ld32(d + c0, v);
+                    if (!row_ok) continue;
+                    const uint32_t f = T.sub / Gp.N1h, kx = T.sub - f * Gp.N1h;
+                    const size_t pst = (size_t)2 * Gp.kpRi * Gp.MpT;  // plane stride
+                    bf16 *o = Gp.aRiT + (size_t)(f * Gp.kpRi + kx) * Gp.MpT + (size_t)(nb >> 1) * Gp.Y + m;
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        if ((nb >> 1) + i < Gp.G) {
+                            // Tx = -i tx: C_x = -i P (re = P_i, im = -P_r); Ty real: C_y = Q
+                            const float re = f ? v[2 * i] : v[2 * i + 1];
+                            const float im = f ? v[2 * i + 1] : -v[2 * i];
+                            bf16 *oi = o + (size_t)i * Gp.Y;
+                            split_store(oi, oi + pst, re);
+                            split_store(oi + 2 * pst, oi + 3 * pst, im);
+                        }
+                    }
+                    continue;
+                }
                 float vr[32], vi[32];
                 tc::tmem_ld32(d + c0, vr);
                 if (OUT_COMPLEX) tc::tmem_ld32(d + 128 + c0, vi);
                 if (mrow0 >= P.M) continue;  // warp-uniform
                 if (STAGE == ST_R) {
-                    // row m = (inst, y) ; col = kx -> B operand of C: row (inst, kx), k = y
                     if (!row_ok) continue;
                     const uint32_t il = m / Gp.Y, y = m - il * Gp.Y;
+                    if (Gp.toe) {
+                        // row m = (inst, y) ; col = kx -> B operand of T: row (kx, inst, re/im), k = y
+                        const size_t plane = (size_t)Gp.rowsT * Gp.kpC, step = (size_t)2 * Gp.G * Gp.kpC;
+                        bf16 *o = Gp.bT + (size_t)(nb * 2 * Gp.G + il * 2) * Gp.kpC + y;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            if (nb + j < Gp.N1h) {
+                                split_store(o, o + plane, vr[j]);
+                                split_store(o + Gp.kpC, o + Gp.kpC + plane, vi[j]);
+                            }
+                            o += step;
+                        }
+                        continue;
+                    }
+                    // row m = (inst, y) ; col = kx -> B operand of C: row (inst, kx), k = y
                     const size_t plane = (size_t)Gp.rowsC * Gp.kpC;
                     bf16 *o = Gp.bC + (size_t)(il * Gp.N1hp + nb) * Gp.kpC + y;
 #pragma unroll
@@ -342,10 +437,20 @@ __global__ void __launch_bounds__(THREADS, 1)
                         }
                     }
                 } else {
-                    // row m = (inst, f, y) ; col = x -> g_f[y * pitch + x], masked
+                    // row m = (inst, f, y), or (inst, y) of field a_mn - 1 ; col = x
+                    // -> g_f[y * pitch + x], masked
                     if (!row_ok) continue;
-                    const uint32_t il = m / (2 * Gp.Y), r2 = m - il * 2 * Gp.Y;
-                    const uint32_t f = r2 >= Gp.Y ? 1u : 0u, y = r2 - f * Gp.Y;
+                    uint32_t il, f, y;
+                    if (P.a_mn) {
+                        il = m / Gp.Y;
+                        y = m - il * Gp.Y;
+                        f = P.a_mn - 1;
+                    } else {
+                        il = m / (2 * Gp.Y);
+                        const uint32_t r2 = m - il * 2 * Gp.Y;
+                        f = r2 >= Gp.Y ? 1u : 0u;
+                        y = r2 - f * Gp.Y;
+                    }
                     const uint32_t inst = Gp.inst0 + il;
                     const InstIO io = (io0_active && inst == 0) ? io0 : ios[inst];
                     float *out = (f ? io.gy : io.gx) + (size_t)y * io.pitch;
@@ -481,6 +586,25 @@ __global__ void spectra_y(const double *tx, const double *ty, float *kxs, float 
     kys[(size_t)kx * N2 + ky] = (float)(-ay);
 }
 
+// Toeplitz matrices of the y stage, into 2 planes: row (f * N1h + kx) * Y + y,
+// column y' < Y holds t_f[j][kx] for j = (y - y') mod N2, where t_x = tx and
+// t_y = ty (spectra_x with the 1/N1 scale only). The -i of Tx is applied in
+// T's epilogue.
+__global__ void toeplitz_expand(const double *tx, const double *ty, bf16 *out, uint32_t Y, uint32_t N2,
+                                uint32_t N1h, uint32_t kp) {
+    const size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (size_t)2 * N1h * Y * Y) return;
+    const uint32_t yp = (uint32_t)(id % Y);
+    const size_t r = id / Y;  // (f * N1h + kx) * Y + y
+    const uint32_t y = (uint32_t)(r % Y);
+    const uint32_t sub = (uint32_t)(r / Y), f = sub / N1h, kx = sub - f * N1h;
+    const int32_t d = (int32_t)y - (int32_t)yp;
+    const uint32_t j = d >= 0 ? (uint32_t)d : (uint32_t)((int32_t)N2 + d);
+    const double v = (f ? ty : tx)[(size_t)j * N1h + kx];
+    const size_t plane = (size_t)2 * N1h * Y * kp, e = r * kp + yp;
+    split_store_d(out + e, out + plane + e, v);
+}
+
 // ---- host ---------------------------------------------------------------------
 static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
@@ -498,11 +622,13 @@ static uint32_t round_up(uint32_t v, uint32_t m) { return (v + m - 1) / m * m; }
 
 struct HostGroup {
     Group g;
-    bf16 *f1 = nullptr, *f2 = nullptr, *g2 = nullptr, *g1 = nullptr;
+    bf16 *f1 = nullptr, *f2 = nullptr, *g2 = nullptr, *g1 = nullptr, *aT = nullptr;
     uint32_t kpF1 = 0, kpF2 = 0, kpG2 = 0, kpG1 = 0;
     float *kxs = nullptr;
     double flops = 0;  // executed tensor flops of one solve of the group
 };
+
+constexpr int NSTAGES = 5;  // R, C, C^-1, R^-1, T (indexed by Stage)
 
 struct DftImpl {
     std::vector<JobShape> shapes;
@@ -514,11 +640,11 @@ struct DftImpl {
     std::vector<uint32_t> inst_group, inst_local;
     CUtensorMap *tmaps = nullptr;
     Problem *probs = nullptr;
-    Tile *tiles[4] = {};
-    uint32_t ntiles[4] = {};
+    Tile *tiles[NSTAGES] = {};
+    uint32_t ntiles[NSTAGES] = {};
     PrepRef *prep = nullptr;
     uint32_t nprep = 0;
-    uint32_t grid[4] = {};
+    uint32_t grid[NSTAGES] = {};
     double flops = 0;
     uint32_t *err = nullptr;  // device address of g_dft_err
     ~DftImpl() {
@@ -536,12 +662,15 @@ struct DftImpl {
     }
 };
 
-static int make_tmap(CUtensorMap *out, const bf16 *base, uint32_t kpitch, uint32_t rows_total) {
+// Row-major bf16 matrix of `rows_total` rows of `kpitch` elements; boxes of
+// 32 elements (64 bytes) x box_rows rows.
+static int make_tmap(CUtensorMap *out, const bf16 *base, uint32_t kpitch, uint32_t rows_total,
+                     uint32_t box_rows = MT) {
     auto fn = encode_fn();
     if (!fn) TPT_FAIL(TPT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available from the driver");
     cuuint64_t dims[2] = {kpitch, rows_total};
     cuuint64_t strides[1] = {(cuuint64_t)kpitch * 2};
-    cuuint32_t box[2] = {KT, MT};
+    cuuint32_t box[2] = {KT, box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<bf16 *>(base), dims, strides, box, estr,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -557,14 +686,39 @@ static int init_attrs() {
     TPT_CUDA(cudaFuncSetAttribute(dft_gemm<ST_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     TPT_CUDA(cudaFuncSetAttribute(dft_gemm<ST_CI>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     TPT_CUDA(cudaFuncSetAttribute(dft_gemm<ST_RI>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+    TPT_CUDA(cudaFuncSetAttribute(dft_gemm<ST_T>, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
     done = true;
     return TPT_OK;
+}
+
+// Effective rates of the cost model that picks a group's y form.
+constexpr double kTensorRate = 1.0e15;  // flop/s
+constexpr double kHbmRate = 5.0e12;     // bytes/s
+enum YMode { YMODE_AUTO = 0, YMODE_DFT = 1, YMODE_TOEPLITZ = 2 };
+
+// TPT_SPLIT_BF16_Y_STAGE = dft | toeplitz | toeplitz:<n> forces the y form
+// (toeplitz:<n>: Toeplitz for groups of at least n instances, DFT for the
+// rest), for comparisons; unset or anything else lets the cost model choose.
+static YMode y_mode_from_env(uint32_t *min_group) {
+    *min_group = 1;
+    const char *s = getenv("TPT_SPLIT_BF16_Y_STAGE");
+    if (!s) return YMODE_AUTO;
+    if (!strcmp(s, "dft")) return YMODE_DFT;
+    if (!strcmp(s, "toeplitz")) return YMODE_TOEPLITZ;
+    if (!strncmp(s, "toeplitz:", 9)) {
+        const long n = strtol(s + 9, nullptr, 10);
+        *min_group = n > 1 ? (uint32_t)n : 1u;
+        return YMODE_TOEPLITZ;
+    }
+    return YMODE_AUTO;
 }
 
 int DftSet::create(const std::vector<JobShape> &shapes) {
     destroy();
     int rc = init_attrs();
     if (rc) return rc;
+    uint32_t toe_min_group = 1;
+    const YMode ymode = y_mode_from_env(&toe_min_group);
     if (!encode_fn()) TPT_FAIL(TPT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available from the driver");
     DftImpl *I = new (std::nothrow) DftImpl();
     if (!I) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "host allocation failed");
@@ -617,46 +771,77 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
         g.rowsC = g.G * g.N1hp;
         g.rowsCi = 2 * g.G * g.N1hp;
         g.rowsRi = 2 * g.G * g.Y;
+        g.rowsT = g.N1h * 2 * g.G;
+        g.nT = std::min<uint32_t>(NT, round_up(2 * g.G, 16));
+        g.MpT = round_up(g.G * g.Y, 32);
         H.kpF1 = g.kpR;   // F1: N1h rows, K = x
         H.kpF2 = g.kpC;   // F2: N2 rows, K = y
         H.kpG2 = g.kpCi;  // G2: Y rows, K = ky
         H.kpG1 = g.kpRi;  // G1: X rows, K = kx
+        // executed tensor flops (3-term split, padded tiles) of both y forms
+        auto tiles_of = [](uint32_t v, uint32_t t) { return (double)((v + t - 1) / t) * t; };
+        const double fR = 2.0 * tiles_of(g.rowsR, MT) * tiles_of(g.N1h, NT) * 2 * g.kpR * 3;
+        const double fC = 2.0 * tiles_of(g.N2, MT) * tiles_of(g.rowsC, NT) * 4 * g.kpC * 3;
+        const double fCi = 2.0 * tiles_of(g.Y, MT) * tiles_of(g.rowsCi, NT) * 4 * g.kpCi * 3;
+        const double fRi = 2.0 * tiles_of(g.rowsRi, MT) * tiles_of(g.X, NT) * 2 * g.kpRi * 3;
+        const double nTall = 2 * g.G <= NT ? (double)g.nT : tiles_of(2 * g.G, NT);
+        const double fT = 2.0 * 2 * g.N1h * tiles_of(g.Y, MT) * nTall * g.kpC * 3;
+        const double fRiT = 2.0 * 2 * tiles_of(g.G * g.Y, MT) * tiles_of(g.X, NT) * 2 * g.kpRi * 3;
+        const double bytesT = 2.0 * 2 * g.N1h * g.Y * g.kpC * 2;  // Toeplitz planes read once
+        // Form of the y stage: the Toeplitz matrices are read from HBM once per
+        // solve, so T wins once enough instances share them.
+        const double t_dft = (fC + fCi + fRi) / kTensorRate;
+        const double t_toe = std::max((fT + fRiT) / kTensorRate, bytesT / kHbmRate);
+        g.toe = ymode == YMODE_TOEPLITZ ? (g.G >= toe_min_group ? 1u : 0u)
+                : ymode == YMODE_DFT    ? 0u
+                                        : (t_toe < t_dft ? 1u : 0u);
         if ((rc = I->alloc(&g.aR, (size_t)2 * g.rowsR * g.kpR))) return rc;
-        if ((rc = I->alloc(&g.bC, (size_t)4 * g.rowsC * g.kpC))) return rc;
-        if ((rc = I->alloc(&g.bCi, (size_t)4 * g.rowsCi * g.kpCi))) return rc;
-        if ((rc = I->alloc(&g.aRi, (size_t)4 * g.rowsRi * g.kpRi))) return rc;
         if ((rc = I->alloc(&H.f1, (size_t)4 * g.N1h * H.kpF1))) return rc;
-        if ((rc = I->alloc(&H.f2, (size_t)4 * g.N2 * H.kpF2))) return rc;
-        if ((rc = I->alloc(&H.g2, (size_t)4 * g.Y * H.kpG2))) return rc;
         if ((rc = I->alloc(&H.g1, (size_t)4 * g.X * H.kpG1))) return rc;
-        if ((rc = I->alloc(&H.kxs, (size_t)2 * g.N2 * g.N1h))) return rc;
-        g.kxs = H.kxs;
-        g.kys = H.kxs + (size_t)g.N2 * g.N1h;
+        if (g.toe) {
+            if ((rc = I->alloc(&g.bT, (size_t)2 * g.rowsT * g.kpC))) return rc;
+            if ((rc = I->alloc(&H.aT, (size_t)2 * 2 * g.N1h * g.Y * g.kpC))) return rc;
+            if ((rc = I->alloc(&g.aRiT, (size_t)4 * 2 * g.kpRi * g.MpT))) return rc;
+        } else {
+            if ((rc = I->alloc(&g.bC, (size_t)4 * g.rowsC * g.kpC))) return rc;
+            if ((rc = I->alloc(&g.bCi, (size_t)4 * g.rowsCi * g.kpCi))) return rc;
+            if ((rc = I->alloc(&g.aRi, (size_t)4 * g.rowsRi * g.kpRi))) return rc;
+            if ((rc = I->alloc(&H.f2, (size_t)4 * g.N2 * H.kpF2))) return rc;
+            if ((rc = I->alloc(&H.g2, (size_t)4 * g.Y * H.kpG2))) return rc;
+            if ((rc = I->alloc(&H.kxs, (size_t)2 * g.N2 * g.N1h))) return rc;
+            g.kxs = H.kxs;
+            g.kys = H.kxs + (size_t)g.N2 * g.N1h;
+        }
         // constants in FP64, rounded once to the hi/lo planes
         auto blocks = [](size_t cnt) { return (unsigned)((cnt + 255) / 256); };
         dft_matrix<<<blocks((size_t)g.N1h * g.X), 256>>>(H.f1, g.N1h, g.X, H.kpF1, g.N1, -1, 0);
-        dft_matrix<<<blocks((size_t)g.N2 * g.Y), 256>>>(H.f2, g.N2, g.Y, H.kpF2, g.N2, -1, 0);
-        dft_matrix<<<blocks((size_t)g.Y * g.N2), 256>>>(H.g2, g.Y, g.N2, H.kpG2, g.N2, +1, 0);
         dft_matrix<<<blocks((size_t)g.X * g.N1h), 256>>>(H.g1, g.X, g.N1h, H.kpG1, g.N1, +1, 1);
-        for (int k = 0; k < 4; ++k) count_launch();
+        count_launch();
+        count_launch();
         double *tx = nullptr;
         TPT_CUDA(cudaMalloc(&tx, (size_t)2 * g.N2 * g.N1h * sizeof(double)));
-        const double scale = -(double)6.673e-1f / ((double)g.N1 * (double)g.N2);
-        spectra_x<<<blocks((size_t)g.N2 * g.N1h), 256>>>(tx, tx + (size_t)g.N2 * g.N1h, g.N1, g.N2, g.N1h, scale);
-        spectra_y<<<blocks((size_t)g.N2 * g.N1h), 256>>>(tx, tx + (size_t)g.N2 * g.N1h, H.kxs,
-                                                         H.kxs + (size_t)g.N2 * g.N1h, g.N2, g.N1h);
+        double *ty = tx + (size_t)g.N2 * g.N1h;
+        if (g.toe) {
+            // y handled directly: only the x transform's 1/N1
+            const double scale = -(double)6.673e-1f / (double)g.N1;
+            spectra_x<<<blocks((size_t)g.N2 * g.N1h), 256>>>(tx, ty, g.N1, g.N2, g.N1h, scale);
+            toeplitz_expand<<<blocks((size_t)2 * g.N1h * g.Y * g.Y), 256>>>(tx, ty, H.aT, g.Y, g.N2, g.N1h, g.kpC);
+        } else {
+            dft_matrix<<<blocks((size_t)g.N2 * g.Y), 256>>>(H.f2, g.N2, g.Y, H.kpF2, g.N2, -1, 0);
+            dft_matrix<<<blocks((size_t)g.Y * g.N2), 256>>>(H.g2, g.Y, g.N2, H.kpG2, g.N2, +1, 0);
+            count_launch();
+            count_launch();
+            const double scale = -(double)6.673e-1f / ((double)g.N1 * (double)g.N2);
+            spectra_x<<<blocks((size_t)g.N2 * g.N1h), 256>>>(tx, ty, g.N1, g.N2, g.N1h, scale);
+            spectra_y<<<blocks((size_t)g.N2 * g.N1h), 256>>>(tx, ty, H.kxs, H.kxs + (size_t)g.N2 * g.N1h, g.N2,
+                                                             g.N1h);
+        }
         count_launch();
         count_launch();
         cudaError_t e = cudaDeviceSynchronize();
         cudaFree(tx);
         if (e != cudaSuccess) TPT_FAIL(TPT_ERR_CUDA, "split-BF16 precompute failed: %s", cudaGetErrorString(e));
-        // executed tensor flops (3-term split, padded tiles)
-        auto tiles_of = [](uint32_t v, uint32_t t) { return (double)((v + t - 1) / t) * t; };
-        double fR = 2.0 * tiles_of(g.rowsR, MT) * tiles_of(g.N1h, NT) * 2 * g.kpR * 3;
-        double fC = 2.0 * tiles_of(g.N2, MT) * tiles_of(g.rowsC, NT) * 4 * g.kpC * 3;
-        double fCi = 2.0 * tiles_of(g.Y, MT) * tiles_of(g.rowsCi, NT) * 4 * g.kpCi * 3;
-        double fRi = 2.0 * tiles_of(g.rowsRi, MT) * tiles_of(g.X, NT) * 2 * g.kpRi * 3;
-        H.flops = fR + fC + fCi + fRi;
+        H.flops = g.toe ? fR + fT + fRiT : fR + fC + fCi + fRi;
         I->flops += H.flops;
     }
     // device tables: groups, tensor maps, problems, tiles
@@ -665,46 +850,72 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
     std::vector<Group> gh(ng);
     for (size_t gi = 0; gi < ng; ++gi) gh[gi] = I->hg[gi].g;
     TPT_CUDA(cudaMemcpy(I->groups, gh.data(), ng * sizeof(Group), cudaMemcpyHostToDevice));
+    // Tensor map slots per group: 0 aR, 1 F1, 2 F2 | aT, 3 bC | bT, 4 G2,
+    // 5 bCi, 6 aRi | aRiT, 7 G1.
     std::vector<CUtensorMap> tm(8 * ng);
-    std::vector<Problem> pr(4 * ng);
+    std::vector<Problem> pr;
     if ((rc = I->alloc(&I->tmaps, tm.size()))) return rc;
-    std::vector<Tile> tl[4];
+    std::vector<Tile> tl[NSTAGES];
     std::vector<PrepRef> pref;
+    // Consecutive CTAs share the data operand's tile (L2 reuse): in C and
+    // C^-1 the data is B (M tiles fastest), in R and R^-1 it is A (N tiles
+    // fastest); the other operand is a small constant matrix.
+    auto add_tiles = [&](int st, uint32_t prob, bool m_fastest) {
+        const Problem &P = pr[prob];
+        if (m_fastest) {
+            for (uint32_t nt = 0; nt * NT < P.N; ++nt)
+                for (uint32_t mt = 0; mt * MT < P.M; ++mt) tl[st].push_back({prob, (uint16_t)mt, (uint16_t)nt, 0});
+        } else {
+            for (uint32_t mt = 0; mt * MT < P.M; ++mt)
+                for (uint32_t nt = 0; nt * NT < P.N; ++nt) tl[st].push_back({prob, (uint16_t)mt, (uint16_t)nt, 0});
+        }
+    };
     for (size_t gi = 0; gi < ng; ++gi) {
         const HostGroup &H = I->hg[gi];
         const Group &g = H.g;
         CUtensorMap *tmd = I->tmaps + 8 * gi;
-        // stage R: A = aR (2 planes), B = F1
-        if ((rc = make_tmap(&tm[8 * gi + 0], g.aR, g.kpR, 2 * g.rowsR))) return rc;
-        if ((rc = make_tmap(&tm[8 * gi + 1], H.f1, H.kpF1, 4 * g.N1h))) return rc;
-        // stage C: A = F2, B = bC
-        if ((rc = make_tmap(&tm[8 * gi + 2], H.f2, H.kpF2, 4 * g.N2))) return rc;
-        if ((rc = make_tmap(&tm[8 * gi + 3], g.bC, g.kpC, 4 * g.rowsC))) return rc;
-        // stage C^-1: A = G2, B = bCi
-        if ((rc = make_tmap(&tm[8 * gi + 4], H.g2, H.kpG2, 4 * g.Y))) return rc;
-        if ((rc = make_tmap(&tm[8 * gi + 5], g.bCi, g.kpCi, 4 * g.rowsCi))) return rc;
-        // stage R^-1: A = aRi, B = G1
-        if ((rc = make_tmap(&tm[8 * gi + 6], g.aRi, g.kpRi, 4 * g.rowsRi))) return rc;
-        if ((rc = make_tmap(&tm[8 * gi + 7], H.g1, H.kpG1, 4 * g.X))) return rc;
+        CUtensorMap *tmh = tm.data() + 8 * gi;
         const uint32_t gi32 = (uint32_t)gi;
-        pr[4 * gi + 0] = {tmd + 0, tmd + 1, gi32, g.rowsR, g.N1h, g.kpR / KT, g.rowsR, g.N1h};
-        pr[4 * gi + 1] = {tmd + 2, tmd + 3, gi32, g.N2, g.rowsC, g.kpC / KT, g.N2, g.rowsC};
-        pr[4 * gi + 2] = {tmd + 4, tmd + 5, gi32, g.Y, g.rowsCi, g.kpCi / KT, g.Y, g.rowsCi};
-        pr[4 * gi + 3] = {tmd + 6, tmd + 7, gi32, g.rowsRi, g.X, g.kpRi / KT, g.rowsRi, g.X};
-        for (int st = 0; st < 4; ++st) {
-            const Problem &P = pr[4 * gi + st];
-            // Consecutive CTAs share the data operand's tile (L2 reuse): in C and
-            // C^-1 the data is B (M tiles fastest), in R and R^-1 it is A (N
-            // tiles fastest); the other operand is a small constant matrix.
-            if (st == ST_C || st == ST_CI) {
-                for (uint32_t nt = 0; nt * NT < P.N; ++nt)
-                    for (uint32_t mt = 0; mt * MT < P.M; ++mt)
-                        tl[st].push_back({(uint32_t)(4 * gi + st), (uint16_t)mt, (uint16_t)nt});
-            } else {
-                for (uint32_t mt = 0; mt * MT < P.M; ++mt)
-                    for (uint32_t nt = 0; nt * NT < P.N; ++nt)
-                        tl[st].push_back({(uint32_t)(4 * gi + st), (uint16_t)mt, (uint16_t)nt});
+        // stage R: A = aR (2 planes), B = F1
+        if ((rc = make_tmap(&tmh[0], g.aR, g.kpR, 2 * g.rowsR))) return rc;
+        if ((rc = make_tmap(&tmh[1], H.f1, H.kpF1, 4 * g.N1h))) return rc;
+        if ((rc = make_tmap(&tmh[7], H.g1, H.kpG1, 4 * g.X))) return rc;
+        pr.push_back({tmd + 0, tmd + 1, gi32, g.rowsR, g.N1h, g.kpR / KT, g.rowsR, g.N1h, 0});
+        add_tiles(ST_R, (uint32_t)pr.size() - 1, false);
+        if (g.toe) {
+            // T: A = Toeplitz planes (rows (f, kx, y)), B = bT (rows (kx, inst, re/im))
+            if ((rc = make_tmap(&tmh[2], H.aT, g.kpC, 2 * 2 * g.N1h * g.Y))) return rc;
+            if ((rc = make_tmap(&tmh[3], g.bT, g.kpC, 2 * g.rowsT))) return rc;
+            // R^-1: A = aRiT read M-major, 32 x 32 boxes (rows (plane, f, kx))
+            if ((rc = make_tmap(&tmh[6], g.aRiT, g.MpT, 8 * g.kpRi, 32))) return rc;
+            const uint32_t pt = (uint32_t)pr.size();
+            pr.push_back({tmd + 2, tmd + 3, gi32, g.Y, 2 * g.G, g.kpC / KT, 2 * g.N1h * g.Y, g.rowsT, 0});
+            // kx slowest, so the tiles of one kx (both fields, all M tiles)
+            // share the B slice while it is in L2
+            for (uint32_t kx = 0; kx < g.N1h; ++kx)
+                for (uint32_t f = 0; f < 2; ++f)
+                    for (uint32_t mt = 0; mt * MT < g.Y; ++mt)
+                        for (uint32_t nt = 0; nt * NT < 2 * g.G; ++nt)
+                            tl[ST_T].push_back({pt, (uint16_t)mt, (uint16_t)nt, f * g.N1h + kx});
+            for (uint32_t f = 0; f < 2; ++f) {
+                pr.push_back({tmd + 6, tmd + 7, gi32, g.G * g.Y, g.X, g.kpRi / KT, g.kpRi, g.X, f + 1});
+                add_tiles(ST_RI, (uint32_t)pr.size() - 1, false);
             }
+        } else {
+            // stage C: A = F2, B = bC
+            if ((rc = make_tmap(&tmh[2], H.f2, H.kpF2, 4 * g.N2))) return rc;
+            if ((rc = make_tmap(&tmh[3], g.bC, g.kpC, 4 * g.rowsC))) return rc;
+            // stage C^-1: A = G2, B = bCi
+            if ((rc = make_tmap(&tmh[4], H.g2, H.kpG2, 4 * g.Y))) return rc;
+            if ((rc = make_tmap(&tmh[5], g.bCi, g.kpCi, 4 * g.rowsCi))) return rc;
+            // stage R^-1: A = aRi, B = G1
+            if ((rc = make_tmap(&tmh[6], g.aRi, g.kpRi, 4 * g.rowsRi))) return rc;
+            pr.push_back({tmd + 2, tmd + 3, gi32, g.N2, g.rowsC, g.kpC / KT, g.N2, g.rowsC, 0});
+            add_tiles(ST_C, (uint32_t)pr.size() - 1, true);
+            pr.push_back({tmd + 4, tmd + 5, gi32, g.Y, g.rowsCi, g.kpCi / KT, g.Y, g.rowsCi, 0});
+            add_tiles(ST_CI, (uint32_t)pr.size() - 1, true);
+            pr.push_back({tmd + 6, tmd + 7, gi32, g.rowsRi, g.X, g.kpRi / KT, g.rowsRi, g.X, 0});
+            add_tiles(ST_RI, (uint32_t)pr.size() - 1, false);
         }
         for (uint32_t r = 0; r < g.rowsR; ++r) pref.push_back({gi32, r});
     }
@@ -714,7 +925,7 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    for (int st = 0; st < 4; ++st) {
+    for (int st = 0; st < NSTAGES; ++st) {
         if ((rc = I->alloc(&I->tiles[st], tl[st].size()))) return rc;
         TPT_CUDA(cudaMemcpy(I->tiles[st], tl[st].data(), tl[st].size() * sizeof(Tile), cudaMemcpyHostToDevice));
         I->ntiles[st] = (uint32_t)tl[st].size();
@@ -753,22 +964,28 @@ int DftSet::launch(cudaStream_t st, const SolveIO *io) const {
     uint32_t *err = I->err;
     prep_mass<<<I->nprep, 128, 0, st>>>(I->groups, I->prep, I->ios, io0, act);
     TPT_LAUNCHED();
-    dft_gemm<ST_R><<<I->grid[0], THREADS, SMEM_BYTES, st>>>(I->probs, I->tiles[0], I->ntiles[0], I->groups, I->ios,
-                                                            io0, act, err);
-    TPT_LAUNCHED();
-    dft_gemm<ST_C><<<I->grid[1], THREADS, SMEM_BYTES, st>>>(I->probs, I->tiles[1], I->ntiles[1], I->groups, I->ios,
-                                                            io0, act, err);
-    TPT_LAUNCHED();
-    dft_gemm<ST_CI><<<I->grid[2], THREADS, SMEM_BYTES, st>>>(I->probs, I->tiles[2], I->ntiles[2], I->groups, I->ios,
-                                                             io0, act, err);
-    TPT_LAUNCHED();
-    dft_gemm<ST_RI><<<I->grid[3], THREADS, SMEM_BYTES, st>>>(I->probs, I->tiles[3], I->ntiles[3], I->groups, I->ios,
-                                                             io0, act, err);
-    TPT_LAUNCHED();
+#define TPT_DFT_STAGE(S)                                                                                      \
+    if (I->ntiles[S]) {                                                                                      \
+        dft_gemm<S><<<I->grid[S], THREADS, SMEM_BYTES, st>>>(I->probs, I->tiles[S], I->ntiles[S], I->groups, \
+                                                             I->ios, io0, act, err);                         \
+        TPT_LAUNCHED();                                                                                      \
+    }
+    // R, then the y stage of each group (DFT pair or Toeplitz), then R^-1
+    TPT_DFT_STAGE(ST_R)
+    TPT_DFT_STAGE(ST_C)
+    TPT_DFT_STAGE(ST_CI)
+    TPT_DFT_STAGE(ST_T)
+    TPT_DFT_STAGE(ST_RI)
+#undef TPT_DFT_STAGE
     return TPT_OK;
 }
 
-uint32_t DftSet::launches() const { return 5; }
+uint32_t DftSet::launches() const {
+    uint32_t n = 1;  // prep_mass
+    if (impl)
+        for (int s = 0; s < NSTAGES; ++s) n += impl->ntiles[s] ? 1u : 0u;
+    return n;
+}
 double DftSet::flops() const { return impl ? impl->flops : 0.0; }
 
 void DftSet::destroy() {

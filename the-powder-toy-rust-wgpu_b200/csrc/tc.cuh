@@ -1,6 +1,6 @@
 // tc.cuh -- sm_100a primitives: mbarriers with bounded waits, TMA tile loads
 // (no cluster multicast), tcgen05 TMEM allocation / MMA / loads, and the
-// shared-memory matrix descriptor of a K-major 64-byte-swizzled operand.
+// shared-memory matrix descriptors of 64-byte-swizzled operands.
 #pragma once
 
 #include <cuda.h>
@@ -137,12 +137,27 @@ __device__ __forceinline__ uint64_t sdesc_k64(uint32_t addr) {
     return d;
 }
 
-// Instruction descriptor of kind::f16: bf16 x bf16 -> f32, both K-major.
-__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t m, uint32_t n, bool neg_a = false) {
+// Shared-memory matrix descriptor, MN-major, 64-byte swizzle: each 64-byte
+// row holds 32 consecutive M (or N) elements of one k; 8-row groups along K
+// are `sbo` bytes apart and 32-element blocks along M are `lbo` bytes apart.
+__device__ __forceinline__ uint64_t sdesc_mn64(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)4u << 61;
+    return d;
+}
+
+// Instruction descriptor of kind::f16: bf16 x bf16 -> f32; B K-major, A
+// K-major unless `a_mn`.
+__host__ __device__ constexpr uint32_t idesc_bf16(uint32_t m, uint32_t n, bool neg_a = false, bool a_mn = false) {
     return (1u << 4)                 // D format f32
            | (1u << 7)               // A format bf16
            | (1u << 10)              // B format bf16
            | ((neg_a ? 1u : 0u) << 13)
+           | ((a_mn ? 1u : 0u) << 15)  // A major: 0 K, 1 MN
            | ((n >> 3) << 17)        // N / 8
            | ((m >> 4) << 24);       // M / 16
 }
