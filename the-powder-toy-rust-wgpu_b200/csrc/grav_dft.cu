@@ -57,13 +57,25 @@ using bf16 = __nv_bfloat16;
 constexpr int KT = 32;             // K elements per tile (64 bytes)
 constexpr int MT = 128;            // rows per M tile
 constexpr int NT = 128;            // complex columns per N tile
-constexpr int STAGES = 3;
-constexpr int TILE_BYTES = MT * KT * 2;  // one plane of one tile: 8 KB
-constexpr int STAGE_BYTES = 8 * TILE_BYTES;
+constexpr int TILE_BYTES = MT * KT * 2;      // one plane of one tile: 8 KB
+constexpr int RING_BYTES = 24 * TILE_BYTES;  // shared-memory ring of K-tile stages: 192 KB
+constexpr int MAX_STAGES = 6;
 constexpr int EPI_WARPS = 8;             // two per TMEM lane quarter, one column half each
 constexpr int XPOSE_BYTES = 32 * 33 * 4; // per epilogue warp: a 32x32 f32 transpose buffer
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + EPI_WARPS * XPOSE_BYTES;
+constexpr int SMEM_BYTES = RING_BYTES + 1024 + EPI_WARPS * XPOSE_BYTES;
 constexpr int THREADS = 64 + 32 * EPI_WARPS;
+
+// Toeplitz stage T. A Toeplitz matrix shifted by 32 columns is the same
+// matrix shifted by 32 rows, so the B operand of every K tile of a T tile
+// is a window of one strip of (N + K - 32) rows x 32 columns, loaded once
+// per tile: K tile kt reads rows from (K - 32 - 32 kt). T groups have
+// Y <= T_NMAX, so one N tile covers all y.
+constexpr int T_NMAX = 256;                          // y rows of a T tile (MMA N at most)
+constexpr int T_STRIP_ROWS = 512;                    // strip buffer rows (>= 2 T_NMAX - 32 + box rounding)
+constexpr int T_STRIP_PLANE = T_STRIP_ROWS * KT * 2; // 32 KB
+constexpr int T_RING_BYTES = 6 * 2 * TILE_BYTES;     // T's A stages: 6 x 16 KB
+static_assert(T_RING_BYTES + 2 * 2 * T_STRIP_PLANE + 1024 <= SMEM_BYTES, "T shared memory");
+static_assert(T_STRIP_ROWS >= 2 * T_NMAX - KT + 2 * 7, "strip buffer holds two rounded boxes");
 
 enum Stage : int { ST_R = 0, ST_C = 1, ST_CI = 2, ST_RI = 3, ST_T = 4 };
 
@@ -76,11 +88,13 @@ struct Group {
     uint32_t kpR, kpC, kpCi, kpRi;       // K pitches (elements)
     uint32_t rowsR, rowsC, rowsCi, rowsRi;  // rows per plane of the data operands
     uint32_t toe;                        // 1: y stage is the Toeplitz GEMM T
-    uint32_t rowsT;                      // T: rows per plane of B (N1h * 2G)
-    uint32_t nT;                         // T: MMA N (2G rounded up to 16, at most NT)
-    uint32_t MpT;                        // T: row length of aRiT (G*Y rounded up to 32)
+    uint32_t rowsT;                      // T: rows per plane of its A operand bT (N1h * 2G)
+    uint32_t nTy;                        // T: MMA N (Y rounded up to 16)
+    uint32_t Yp;                         // T: rows per instance in aRiT (Y rounded up to 8)
+    uint32_t MpT;                        // T: row length of aRiT (G * Yp rounded up to 32)
+    uint32_t SR, sbox, snb;              // T: strip rows per (f, kx); TMA box rows; boxes per strip
     bf16 *aR, *bC, *bCi, *aRi;           // data operands (planes stacked), DFT form
-    bf16 *bT, *aRiT;                     // T's B operand; R^-1's A operand [plane][f][kx][inst*Y + y]
+    bf16 *bT, *aRiT;                     // T's A operand [plane][kx][inst][re/im][y]; R^-1's A [plane][f][kx][inst*Yp + y]
     const float *kxs, *kys;              // imaginary parts of the kernel spectra, [kx][ky]
 };
 
@@ -112,34 +126,63 @@ __device__ __forceinline__ void split_store(bf16 *hi, bf16 *lo, float v) {
     *lo = __float2bfloat16_rn(v - __bfloat162float(h));
 }
 
+// Splits 32 floats (times sgn) into packed bf16 hi and lo words.
+__device__ __forceinline__ void split_pack32(const float (&v)[32], float sgn, uint32_t (&hw)[16], uint32_t (&lw)[16]) {
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        const float v0 = sgn * v[2 * i], v1 = sgn * v[2 * i + 1];
+        const bf16 h0 = __float2bfloat16_rn(v0), h1 = __float2bfloat16_rn(v1);
+        const bf16 l0 = __float2bfloat16_rn(v0 - __bfloat162float(h0));
+        const bf16 l1 = __float2bfloat16_rn(v1 - __bfloat162float(h1));
+        hw[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+        lw[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+    }
+}
+
 // ---- the GEMM kernel ---------------------------------------------------------
 template <int STAGE>
 __global__ void __launch_bounds__(THREADS, 1)
     dft_gemm(const Problem *__restrict__ probs, const Tile *__restrict__ tiles, uint32_t ntiles,
              const Group *__restrict__ groups, const InstIO *__restrict__ ios, InstIO io0, int io0_active,
              uint32_t *err) {
-    constexpr bool A_COMPLEX = STAGE != ST_R && STAGE != ST_T;
-    constexpr bool B_COMPLEX = STAGE != ST_T;
-    constexpr bool OUT_COMPLEX = STAGE != ST_RI && STAGE != ST_T;
+    // R^-1 keeps only the real part, so it runs as one real GEMM over K' =
+    // [kx of Re C | kx of Im C] against [G1r ; -G1i]: each K tile loads one
+    // hi/lo plane pair of A and of B, and its N tiles are 256 wide. T's B
+    // (the Toeplitz strip) lives outside the ring.
+    constexpr bool A_COMPLEX = STAGE == ST_C || STAGE == ST_CI;
+    constexpr bool B_COMPLEX = STAGE == ST_R || STAGE == ST_C || STAGE == ST_CI;
+    constexpr bool OUT_COMPLEX = B_COMPLEX;
+    constexpr bool WIDE = STAGE == ST_RI || STAGE == ST_T;         // real N tiles of 256
+    constexpr uint32_t NTS = WIDE ? 2 * NT : NT;                     // N tile (complex columns if complex)
     constexpr uint32_t A_PLANES = A_COMPLEX ? 4 : 2;
-    constexpr uint32_t B_PLANES = B_COMPLEX ? 4 : 2;
-    constexpr uint32_t TX_BYTES = (A_PLANES + B_PLANES) * TILE_BYTES;
+    constexpr uint32_t B_PLANES = STAGE == ST_T ? 0 : (B_COMPLEX ? 4 : 2);
+    constexpr uint32_t BPB = STAGE == ST_RI ? 2 * TILE_BYTES : TILE_BYTES;  // bytes of one B plane
+    constexpr uint32_t SBYTES = A_PLANES * TILE_BYTES + B_PLANES * BPB;   // one stage
+    constexpr uint32_t RING = STAGE == ST_T ? T_RING_BYTES : RING_BYTES;
+    constexpr uint32_t NSTG = RING / SBYTES < MAX_STAGES ? RING / SBYTES : MAX_STAGES;  // 3 (C, C^-1), 4, 6 (T)
+    constexpr uint32_t B_OFF = A_PLANES * TILE_BYTES;
+    constexpr uint32_t BLO = (B_COMPLEX ? 2 : 1) * BPB;  // B lo block from B hi block
+    static_assert(NSTG >= 3, "stage ring");
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    __shared__ uint64_t full_bar[STAGES], empty_bar[STAGES], acc_full[2], acc_empty[2];
+    uint8_t *strip = smem + T_RING_BYTES;  // T: two strip buffers, [hi plane | lo plane] each
+    __shared__ uint64_t full_bar[MAX_STAGES], empty_bar[MAX_STAGES], acc_full[2], acc_empty[2];
+    __shared__ uint64_t strip_full[2], strip_empty[2];
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; ++s) {
+        for (uint32_t s = 0; s < NSTG; ++s) {
             tc::mbar_init(&full_bar[s], 1);
             tc::mbar_init(&empty_bar[s], 1);
         }
         for (int a = 0; a < 2; ++a) {
             tc::mbar_init(&acc_full[a], 1);
             tc::mbar_init(&acc_empty[a], EPI_WARPS);
+            tc::mbar_init(&strip_full[a], 1);
+            tc::mbar_init(&strip_empty[a], 1);
         }
         abort_flag = 0;
         tc::fence_mbar_init();
@@ -153,46 +196,71 @@ __global__ void __launch_bounds__(THREADS, 1)
     if (warp == 0) {
         // ---------------- TMA producer ----------------
         if (lane == 0) {
-            uint32_t s = 0, ph = 0;
-            for (uint32_t t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x) {
+            uint32_t s = 0, ph = 0, tl = 0;
+            for (uint32_t t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++tl) {
                 const Tile T = tiles[t];
                 const Problem P = probs[T.problem];
-                int32_t m0 = T.mt * MT, n0 = T.nt * NT;
-                if (STAGE == ST_T) {  // this tile's Toeplitz matrix and frequency slice
+                int32_t m0 = T.mt * MT;
+                const int32_t n0 = T.nt * NTS;
+                if (STAGE == ST_T) {
+                    // A = this tile's frequency slice of bT; B = the (f, kx) strip
                     const Group &Gq = groups[P.group];
-                    const uint32_t kx = T.sub % Gq.N1h;
-                    m0 += (int32_t)(T.sub * Gq.Y);
-                    n0 += (int32_t)(kx * 2 * Gq.G);
+                    m0 += (int32_t)((T.sub % Gq.N1h) * 2 * Gq.G);
+                    const uint32_t sb = tl & 1u;
+                    if (!tc::mbar_wait(&strip_empty[sb], ((tl >> 1) & 1u) ^ 1u, err)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    uint8_t *sdst = strip + sb * 2 * T_STRIP_PLANE;
+                    tc::mbar_arrive_expect_tx(&strip_full[sb], 2 * Gq.snb * Gq.sbox * KT * 2);
+                    for (uint32_t p = 0; p < 2; ++p)
+                        for (uint32_t b = 0; b < Gq.snb; ++b)
+                            tc::tma_load_2d(sdst + p * T_STRIP_PLANE + b * Gq.sbox * KT * 2, P.tb, 0,
+                                            (int32_t)((p * 2 * Gq.N1h + T.sub) * Gq.SR + b * Gq.sbox),
+                                            &strip_full[sb]);
                 }
                 for (uint32_t kt = 0; kt < P.ktiles; ++kt) {
                     if (!tc::mbar_wait(&empty_bar[s], ph ^ 1u, err)) {
                         abort_flag = 1;
                         break;
                     }
-                    uint8_t *st = smem + s * STAGE_BYTES;
-                    tc::mbar_arrive_expect_tx(&full_bar[s], TX_BYTES);
-                    const int32_t k0 = kt * KT;
-                    if (STAGE == ST_RI && P.a_mn) {
-                        // MN-major A: per plane four 32(m) x 32(k) boxes, 2 KB apart
-                        const uint32_t f = P.a_mn - 1;
-                        for (uint32_t p = 0; p < A_PLANES; ++p)
-                            for (uint32_t j = 0; j < 4; ++j)
-                                tc::tma_load_2d(st + p * TILE_BYTES + j * 2048, P.ta, m0 + (int32_t)(32 * j),
-                                                (int32_t)((p * 2 + f) * P.a_rows) + k0, &full_bar[s]);
+                    uint8_t *st = smem + s * SBYTES;
+                    tc::mbar_arrive_expect_tx(&full_bar[s], SBYTES);
+                    if (STAGE == ST_RI) {
+                        // K' tile kt: real parts (planes 0, 1), then imaginary parts (2, 3)
+                        const uint32_t kh = P.ktiles / 2, part = kt >= kh ? 1u : 0u;
+                        const int32_t k0 = (int32_t)((kt - part * kh) * KT);
+                        for (uint32_t p = 0; p < 2; ++p) {
+                            const uint32_t pl = 2 * part + p;
+                            if (P.a_mn) {
+                                // MN-major A: four 32(m) x 32(k) boxes, 2 KB apart
+                                const uint32_t f = P.a_mn - 1;
+                                for (uint32_t j = 0; j < 4; ++j)
+                                    tc::tma_load_2d(st + p * TILE_BYTES + j * 2048, P.ta, m0 + (int32_t)(32 * j),
+                                                    (int32_t)((pl * 2 + f) * P.a_rows) + k0, &full_bar[s]);
+                            } else {
+                                tc::tma_load_2d(st + p * TILE_BYTES, P.ta, k0, (int32_t)(pl * P.a_rows) + m0,
+                                                &full_bar[s]);
+                            }
+                            tc::tma_load_2d(st + B_OFF + p * BPB, P.tb, k0, (int32_t)(pl * P.b_rows) + n0,
+                                            &full_bar[s]);
+                        }
                     } else {
+                        const int32_t k0 = kt * KT;
                         for (uint32_t p = 0; p < A_PLANES; ++p)
                             tc::tma_load_2d(st + p * TILE_BYTES, P.ta, k0, (int32_t)(p * P.a_rows) + m0,
                                             &full_bar[s]);
+                        if (B_COMPLEX) {
+                            // B: hi block [r_hi | i_hi], lo block [r_lo | i_lo]
+                            uint8_t *bb = st + B_OFF;
+                            tc::tma_load_2d(bb, P.tb, k0, (int32_t)(0 * P.b_rows) + n0, &full_bar[s]);
+                            tc::tma_load_2d(bb + BLO, P.tb, k0, (int32_t)(1 * P.b_rows) + n0, &full_bar[s]);
+                            tc::tma_load_2d(bb + TILE_BYTES, P.tb, k0, (int32_t)(2 * P.b_rows) + n0, &full_bar[s]);
+                            tc::tma_load_2d(bb + BLO + TILE_BYTES, P.tb, k0, (int32_t)(3 * P.b_rows) + n0,
+                                            &full_bar[s]);
+                        }
                     }
-                    // B: hi block [r_hi | i_hi], lo block [r_lo | i_lo] (real B: r only)
-                    uint8_t *bb = st + 4 * TILE_BYTES;
-                    tc::tma_load_2d(bb + 0 * TILE_BYTES, P.tb, k0, (int32_t)(0 * P.b_rows) + n0, &full_bar[s]);
-                    tc::tma_load_2d(bb + 2 * TILE_BYTES, P.tb, k0, (int32_t)(1 * P.b_rows) + n0, &full_bar[s]);
-                    if (B_COMPLEX) {
-                        tc::tma_load_2d(bb + 1 * TILE_BYTES, P.tb, k0, (int32_t)(2 * P.b_rows) + n0, &full_bar[s]);
-                        tc::tma_load_2d(bb + 3 * TILE_BYTES, P.tb, k0, (int32_t)(3 * P.b_rows) + n0, &full_bar[s]);
-                    }
-                    if (++s == STAGES) {
+                    if (++s == NSTG) {
                         s = 0;
                         ph ^= 1u;
                     }
@@ -203,14 +271,21 @@ __global__ void __launch_bounds__(THREADS, 1)
         // ---------------- MMA issuer ----------------
         if (lane == 0) {
             constexpr uint32_t I256 = tc::idesc_bf16(128, 256);
-            uint32_t s = 0, ph = 0, acc = 0, acc_ph = 0;
-            for (uint32_t t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x) {
+            uint32_t s = 0, ph = 0, acc = 0, acc_ph = 0, tl = 0;
+            for (uint32_t t = blockIdx.x; t < ntiles && !abort_flag; t += gridDim.x, ++tl) {
                 const Problem P = probs[tiles[t].problem];
-                // MN-major A only in R^-1 of Toeplitz groups; T's N is the group's column count
+                // MN-major A only in R^-1 of Toeplitz groups; T's N is the group's y count
                 const bool amn = STAGE == ST_RI && P.a_mn != 0;
-                const uint32_t nmma = STAGE == ST_T ? groups[P.group].nT : 128u;
+                const uint32_t nmma = STAGE == ST_T ? groups[P.group].nTy : 128u;
+                const uint32_t kpT = STAGE == ST_T ? groups[P.group].kpC : 0u;
                 const uint32_t I128 = tc::idesc_bf16(128, nmma, false, amn);
                 const uint32_t I128N = tc::idesc_bf16(128, 128, true, amn);
+                const uint32_t IRI = tc::idesc_bf16(128, 256, false, amn), IRIN = tc::idesc_bf16(128, 256, true, amn);
+                const uint32_t sb = tl & 1u;
+                if (STAGE == ST_T && !tc::mbar_wait(&strip_full[sb], (tl >> 1) & 1u, err)) {
+                    abort_flag = 1;
+                    break;
+                }
                 if (!tc::mbar_wait(&acc_empty[acc], acc_ph ^ 1u, err)) {
                     abort_flag = 1;
                     break;
@@ -223,8 +298,13 @@ __global__ void __launch_bounds__(THREADS, 1)
                         break;
                     }
                     tc::tc_fence_after();
-                    const uint32_t st = tc::smem_u32(smem + s * STAGE_BYTES);
-                    const uint32_t bhi = st + 4 * TILE_BYTES, blo = st + 6 * TILE_BYTES;
+                    const uint32_t st = tc::smem_u32(smem + s * SBYTES);
+                    uint32_t bhi = st + B_OFF, blo = bhi + BLO;
+                    if (STAGE == ST_T) {
+                        // rows (K - 32 - 32 kt) .. of the strip
+                        bhi = tc::smem_u32(strip + sb * 2 * T_STRIP_PLANE) + (kpT - KT - kt * KT) * KT * 2;
+                        blo = bhi + T_STRIP_PLANE;
+                    }
 #pragma unroll
                     for (int j = 0; j < KT / 16; ++j) {
                         const uint32_t o = j * 32;  // 16 bf16 along K (K-major rows)
@@ -240,7 +320,13 @@ __global__ void __launch_bounds__(THREADS, 1)
                             tc::mma_bf16(d, arh, tc::sdesc_k64(bhi + o), I128, first);
                             tc::mma_bf16(d, arh, tc::sdesc_k64(blo + o), I128, 1);
                             tc::mma_bf16(d, arl, tc::sdesc_k64(bhi + o), I128, 1);
-                        } else if (OUT_COMPLEX) {
+                        } else if (STAGE == ST_RI) {
+                            // D += Ar * Br over the first half of K', D -= Ai * Bi over the second
+                            const uint32_t id = kt < P.ktiles / 2 ? IRI : IRIN;
+                            tc::mma_bf16(d, arh, tc::sdesc_k64(bhi + o), id, first);
+                            tc::mma_bf16(d, arh, tc::sdesc_k64(blo + o), id, 1);
+                            tc::mma_bf16(d, arl, tc::sdesc_k64(bhi + o), id, 1);
+                        } else {
                             // [Dr | Di] += Ar * [Br | Bi]
                             tc::mma_bf16(d, arh, tc::sdesc_k64(bhi + o), I256, first);
                             tc::mma_bf16(d, arh, tc::sdesc_k64(blo + o), I256, 1);
@@ -255,23 +341,15 @@ __global__ void __launch_bounds__(THREADS, 1)
                                 tc::mma_bf16(d + 128, aih, tc::sdesc_k64(blo + o), I128, 1);
                                 tc::mma_bf16(d + 128, ail, tc::sdesc_k64(bhi + o), I128, 1);
                             }
-                        } else {
-                            // Dr = Ar * Br - Ai * Bi
-                            const uint64_t aih = ad(2), ail = ad(3);
-                            tc::mma_bf16(d, arh, tc::sdesc_k64(bhi + o), I128, first);
-                            tc::mma_bf16(d, arh, tc::sdesc_k64(blo + o), I128, 1);
-                            tc::mma_bf16(d, arl, tc::sdesc_k64(bhi + o), I128, 1);
-                            tc::mma_bf16(d, aih, tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
-                            tc::mma_bf16(d, aih, tc::sdesc_k64(blo + TILE_BYTES + o), I128N, 1);
-                            tc::mma_bf16(d, ail, tc::sdesc_k64(bhi + TILE_BYTES + o), I128N, 1);
                         }
                     }
                     tc::mma_commit(&empty_bar[s]);  // frees the stage when these MMAs finish
-                    if (++s == STAGES) {
+                    if (++s == NSTG) {
                         s = 0;
                         ph ^= 1u;
                     }
                 }
+                if (STAGE == ST_T) tc::mma_commit(&strip_empty[sb]);  // the strip is free once they finish
                 tc::mma_commit(&acc_full[acc]);
                 if (++acc == 2) {
                     acc = 0;
@@ -286,7 +364,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         // chunks; C and C^-1 columns are padded per instance to N1hp, so a
         // chunk never straddles an instance or field.
         const uint32_t ew = warp - 2, q = warp & 3, half = ew >> 2;
-        float *xbuf = reinterpret_cast<float *>(smem + STAGES * STAGE_BYTES) + ew * (32 * 33);
+        float *xbuf = reinterpret_cast<float *>(smem + RING_BYTES) + ew * (32 * 33);
         uint32_t acc = 0, acc_ph = 0;
         for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
             const Tile T = tiles[t];
@@ -300,8 +378,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint32_t mrow0 = T.mt * MT + q * 32;  // first row of this warp
             const uint32_t m = mrow0 + lane;            // this thread's row
             const uint32_t d = tmem + acc * 256 + ((q * 32u) << 16);
-            for (uint32_t c0 = half * (NT / 2); c0 < (half + 1) * (NT / 2); c0 += 32) {
-                const uint32_t nb = T.nt * NT + c0;
+            for (uint32_t c0 = half * (NTS / 2); c0 < (half + 1) * (NTS / 2); c0 += 32) {
+                const uint32_t nb = T.nt * NTS + c0;
                 const bool row_ok = m < P.M;
                 if constexpr (STAGE == ST_C) {
                     // row m = ky ; col = (inst, kx) -> B operand of C^-1: row (inst, f, kx), k = ky.
@@ -353,25 +431,29 @@ __global__ void __launch_bounds__(THREADS, 1)
                     continue;
                 }
                 if constexpr (STAGE == ST_T) {
-                    // row m = y of the (f, kx) matrix ; col = (inst, re/im) -> R^-1's
-                    // M-major A operand aRiT[plane][f][kx][inst * Y + y]. Lanes are
-                    // consecutive y, so every store is a 64-byte run.
-                    if (mrow0 >= Gp.Y || nb >= 2 * Gp.G) continue;  // warp-uniform
+                    // row m = (inst, re/im) ; col = y -> R^-1's M-major A operand
+                    // aRiT[plane][f][kx][inst * Yp + y]: each lane writes 32
+                    // consecutive y of one part of C as 16-byte stores.
+                    if (mrow0 >= 2 * Gp.G || nb >= Gp.Yp) continue;  // warp-uniform
                     float v[32];
                     tc::tmem_ld32(d + c0, v);
-                    if (!row_ok) continue;
+                    if (m >= 2 * Gp.G) continue;
                     const uint32_t f = T.sub / Gp.N1h, kx = T.sub - f * Gp.N1h;
+                    const uint32_t inst = m >> 1, ri = m & 1u;
+                    // Tx = -i tx: C_x = -i P (Re = P_i, Im = -P_r); Ty is real: C_y = Q
+                    const uint32_t part = f ? ri : (ri ^ 1u);  // 0: Re C, 1: Im C
+                    const float sgn = (f == 0 && ri == 0) ? -1.0f : 1.0f;
                     const size_t pst = (size_t)2 * Gp.kpRi * Gp.MpT;  // plane stride
-                    bf16 *o = Gp.aRiT + (size_t)(f * Gp.kpRi + kx) * Gp.MpT + (size_t)(nb >> 1) * Gp.Y + m;
+                    bf16 *o = Gp.aRiT + (size_t)((4 * part + f) * Gp.kpRi + kx) * Gp.MpT + (size_t)inst * Gp.Yp + nb;
+                    uint32_t hw[16], lw[16];
+                    split_pack32(v, sgn, hw, lw);
+                    // Yp is a multiple of 8: an 8-element piece is wholly inside or past the instance
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        if ((nb >> 1) + i < Gp.G) {
-                            // Tx = -i tx: C_x = -i P (re = P_i, im = -P_r); Ty real: C_y = Q
-                            const float re = f ? v[2 * i] : v[2 * i + 1];
-                            const float im = f ? v[2 * i + 1] : -v[2 * i];
-                            bf16 *oi = o + (size_t)i * Gp.Y;
-                            split_store(oi, oi + pst, re);
-                            split_store(oi + 2 * pst, oi + 3 * pst, im);
+                    for (int k = 0; k < 4; ++k) {
+                        if (nb + 8 * k < Gp.Yp) {
+                            reinterpret_cast<uint4 *>(o)[k] = make_uint4(hw[4 * k], hw[4 * k + 1], hw[4 * k + 2], hw[4 * k + 3]);
+                            reinterpret_cast<uint4 *>(o + pst)[k] =
+                                make_uint4(lw[4 * k], lw[4 * k + 1], lw[4 * k + 2], lw[4 * k + 3]);
                         }
                     }
                     continue;
@@ -384,7 +466,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                     if (!row_ok) continue;
                     const uint32_t il = m / Gp.Y, y = m - il * Gp.Y;
                     if (Gp.toe) {
-                        // row m = (inst, y) ; col = kx -> B operand of T: row (kx, inst, re/im), k = y
+                        // row m = (inst, y) ; col = kx -> A operand of T: row (kx, inst, re/im), k = y
                         const size_t plane = (size_t)Gp.rowsT * Gp.kpC, step = (size_t)2 * Gp.G * Gp.kpC;
                         bf16 *o = Gp.bT + (size_t)(nb * 2 * Gp.G + il * 2) * Gp.kpC + y;
 #pragma unroll
@@ -418,16 +500,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                     bf16 *o = Gp.aRi + (size_t)((il * 2 + f) * Gp.Y + m) * Gp.kpRi + kx0;
 #pragma unroll
                     for (int part = 0; part < 2; ++part) {
-                        const float *v = part ? vi : vr;
                         uint32_t hw[16], lw[16];
-#pragma unroll
-                        for (int i = 0; i < 16; ++i) {
-                            const bf16 h0 = __float2bfloat16_rn(v[2 * i]), h1 = __float2bfloat16_rn(v[2 * i + 1]);
-                            const bf16 l0 = __float2bfloat16_rn(v[2 * i] - __bfloat162float(h0));
-                            const bf16 l1 = __float2bfloat16_rn(v[2 * i + 1] - __bfloat162float(h1));
-                            hw[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
-                            lw[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
-                        }
+                        split_pack32(part ? vi : vr, 1.0f, hw, lw);
                         uint4 *oh = reinterpret_cast<uint4 *>(o + (size_t)(2 * part) * plane);
                         uint4 *ol = reinterpret_cast<uint4 *>(o + (size_t)(2 * part + 1) * plane);
 #pragma unroll
@@ -442,9 +516,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                     if (!row_ok) continue;
                     uint32_t il, f, y;
                     if (P.a_mn) {
-                        il = m / Gp.Y;
-                        y = m - il * Gp.Y;
+                        il = m / Gp.Yp;  // aRiT rows are inst * Yp + y
+                        y = m - il * Gp.Yp;
                         f = P.a_mn - 1;
+                        if (y >= Gp.Y) continue;
                     } else {
                         il = m / (2 * Gp.Y);
                         const uint32_t r2 = m - il * 2 * Gp.Y;
@@ -504,11 +579,53 @@ __global__ void prep_mass(const Group *__restrict__ groups, const PrepRef *__res
     const InstIO io = (io0_active && inst == 0) ? io0 : ios[inst];
     const size_t plane = (size_t)Gp.rowsR * Gp.kpR;
     bf16 *o = Gp.aR + (size_t)r.row * Gp.kpR;
-    for (uint32_t x = threadIdx.x; x < Gp.X; x += blockDim.x) {
-        size_t c = (size_t)y * io.pitch + x;
-        float v = 0.0f;
-        if (__ldg(io.mask + c) != 0u) v = io.mass_f ? __ldg(io.mass_f + c) : (float)__ldg(io.mass_i + c) * io.inv;
-        split_store(o + x, o + plane + x, v);
+    const size_t c0 = (size_t)y * io.pitch;
+    const void *src = io.mass_f ? (const void *)(io.mass_f + c0) : (const void *)(io.mass_i + c0);
+    // 8 cells per thread with 16-byte accesses when the rows allow it (pitch a
+    // multiple of 8, so the chunk that holds x = X-1 ends inside the row);
+    // the aR row is 64-byte aligned and padded to a multiple of 32.
+    const bool vec = (io.pitch & 7u) == 0u &&
+                     ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(io.mask + c0)) & 15u) == 0u;
+    for (uint32_t x0 = threadIdx.x * 8; x0 < Gp.X; x0 += blockDim.x * 8) {
+        float v[8];
+        if (vec) {
+            const uint4 *mk = reinterpret_cast<const uint4 *>(io.mask + c0 + x0);
+            const uint4 m0 = __ldg(mk), m1 = __ldg(mk + 1);
+            const uint32_t mm[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+            float a[8];
+            if (io.mass_f) {
+                const float4 *p = reinterpret_cast<const float4 *>(io.mass_f + c0 + x0);
+                const float4 q0 = __ldg(p), q1 = __ldg(p + 1);
+                a[0] = q0.x, a[1] = q0.y, a[2] = q0.z, a[3] = q0.w, a[4] = q1.x, a[5] = q1.y, a[6] = q1.z, a[7] = q1.w;
+            } else {
+                const int4 *p = reinterpret_cast<const int4 *>(io.mass_i + c0 + x0);
+                const int4 q0 = __ldg(p), q1 = __ldg(p + 1);
+                const int32_t qi[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+#pragma unroll
+                for (int j = 0; j < 8; ++j) a[j] = (float)qi[j] * io.inv;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = (x0 + j < Gp.X && mm[j] != 0u) ? a[j] : 0.0f;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const size_t c = c0 + x0 + j;
+                v[j] = 0.0f;
+                if (x0 + j < Gp.X && __ldg(io.mask + c) != 0u)
+                    v[j] = io.mass_f ? __ldg(io.mass_f + c) : (float)__ldg(io.mass_i + c) * io.inv;
+            }
+        }
+        uint32_t hw[4], lw[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const bf16 h0 = __float2bfloat16_rn(v[2 * i]), h1 = __float2bfloat16_rn(v[2 * i + 1]);
+            const bf16 l0 = __float2bfloat16_rn(v[2 * i] - __bfloat162float(h0));
+            const bf16 l1 = __float2bfloat16_rn(v[2 * i + 1] - __bfloat162float(h1));
+            hw[i] = (uint32_t)__bfloat16_as_ushort(h0) | ((uint32_t)__bfloat16_as_ushort(h1) << 16);
+            lw[i] = (uint32_t)__bfloat16_as_ushort(l0) | ((uint32_t)__bfloat16_as_ushort(l1) << 16);
+        }
+        *reinterpret_cast<uint4 *>(o + x0) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        *reinterpret_cast<uint4 *>(o + plane + x0) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
     }
 }
 
@@ -586,23 +703,23 @@ __global__ void spectra_y(const double *tx, const double *ty, float *kxs, float 
     kys[(size_t)kx * N2 + ky] = (float)(-ay);
 }
 
-// Toeplitz matrices of the y stage, into 2 planes: row (f * N1h + kx) * Y + y,
-// column y' < Y holds t_f[j][kx] for j = (y - y') mod N2, where t_x = tx and
-// t_y = ty (spectra_x with the 1/N1 scale only). The -i of Tx is applied in
-// T's epilogue.
-__global__ void toeplitz_expand(const double *tx, const double *ty, bf16 *out, uint32_t Y, uint32_t N2,
-                                uint32_t N1h, uint32_t kp) {
+// Toeplitz strips of the y stage, into 2 planes: row (f * N1h + kx) * SR + r,
+// column c < 32 holds t_f[(r - (kp - 32) - c) mod N2][kx], with t_x = tx and
+// t_y = ty from spectra_x with the 1/N1 scale only. Rows r .. r + N of a
+// strip are the Toeplitz matrix T[y][y'] = t_f[(y - y') mod N2] for
+// y' in [kp - 32 - r, kp - r); the -i of Tx is applied in T's epilogue.
+__global__ void toeplitz_strip(const double *tx, const double *ty, bf16 *out, uint32_t SR, uint32_t N2,
+                               uint32_t N1h, uint32_t kp) {
     const size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (id >= (size_t)2 * N1h * Y * Y) return;
-    const uint32_t yp = (uint32_t)(id % Y);
-    const size_t r = id / Y;  // (f * N1h + kx) * Y + y
-    const uint32_t y = (uint32_t)(r % Y);
-    const uint32_t sub = (uint32_t)(r / Y), f = sub / N1h, kx = sub - f * N1h;
-    const int32_t d = (int32_t)y - (int32_t)yp;
-    const uint32_t j = d >= 0 ? (uint32_t)d : (uint32_t)((int32_t)N2 + d);
+    if (id >= (size_t)2 * N1h * SR * KT) return;
+    const uint32_t c = (uint32_t)(id % KT);
+    const size_t row = id / KT;  // (f * N1h + kx) * SR + r
+    const uint32_t r = (uint32_t)(row % SR), sub = (uint32_t)(row / SR), f = sub / N1h, kx = sub - f * N1h;
+    const int64_t d = (int64_t)r - (int64_t)(kp - KT) - (int64_t)c;
+    const uint32_t j = (uint32_t)(((d % (int64_t)N2) + (int64_t)N2) % (int64_t)N2);
     const double v = (f ? ty : tx)[(size_t)j * N1h + kx];
-    const size_t plane = (size_t)2 * N1h * Y * kp, e = r * kp + yp;
-    split_store_d(out + e, out + plane + e, v);
+    const size_t plane = (size_t)2 * N1h * SR * KT;
+    split_store_d(out + id, out + plane + id, v);
 }
 
 // ---- host ---------------------------------------------------------------------
@@ -622,7 +739,7 @@ static uint32_t round_up(uint32_t v, uint32_t m) { return (v + m - 1) / m * m; }
 
 struct HostGroup {
     Group g;
-    bf16 *f1 = nullptr, *f2 = nullptr, *g2 = nullptr, *g1 = nullptr, *aT = nullptr;
+    bf16 *f1 = nullptr, *f2 = nullptr, *g2 = nullptr, *g1 = nullptr, *ts = nullptr;
     uint32_t kpF1 = 0, kpF2 = 0, kpG2 = 0, kpG1 = 0;
     float *kxs = nullptr;
     double flops = 0;  // executed tensor flops of one solve of the group
@@ -691,9 +808,8 @@ static int init_attrs() {
     return TPT_OK;
 }
 
-// Effective rates of the cost model that picks a group's y form.
-constexpr double kTensorRate = 1.0e15;  // flop/s
-constexpr double kHbmRate = 5.0e12;     // bytes/s
+// Smallest group that takes the Toeplitz y stage by default.
+constexpr uint32_t kToeMinGroup = 8;
 enum YMode { YMODE_AUTO = 0, YMODE_DFT = 1, YMODE_TOEPLITZ = 2 };
 
 // TPT_SPLIT_BF16_Y_STAGE = dft | toeplitz | toeplitz:<n> forces the y form
@@ -772,8 +888,12 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
         g.rowsCi = 2 * g.G * g.N1hp;
         g.rowsRi = 2 * g.G * g.Y;
         g.rowsT = g.N1h * 2 * g.G;
-        g.nT = std::min<uint32_t>(NT, round_up(2 * g.G, 16));
-        g.MpT = round_up(g.G * g.Y, 32);
+        g.nTy = std::min<uint32_t>(T_NMAX, round_up(g.Y, 16));
+        g.Yp = round_up(g.Y, 8);
+        g.MpT = round_up(g.G * g.Yp, 32);
+        g.SR = g.nTy + g.kpC - KT;                               // strip rows
+        g.snb = (g.SR + T_NMAX - 1) / T_NMAX;                    // TMA boxes per strip (box rows <= 256)
+        g.sbox = round_up((g.SR + g.snb - 1) / g.snb, 8);        // box rows, 512-byte multiples
         H.kpF1 = g.kpR;   // F1: N1h rows, K = x
         H.kpF2 = g.kpC;   // F2: N2 rows, K = y
         H.kpG2 = g.kpCi;  // G2: Y rows, K = ky
@@ -783,24 +903,26 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
         const double fR = 2.0 * tiles_of(g.rowsR, MT) * tiles_of(g.N1h, NT) * 2 * g.kpR * 3;
         const double fC = 2.0 * tiles_of(g.N2, MT) * tiles_of(g.rowsC, NT) * 4 * g.kpC * 3;
         const double fCi = 2.0 * tiles_of(g.Y, MT) * tiles_of(g.rowsCi, NT) * 4 * g.kpCi * 3;
-        const double fRi = 2.0 * tiles_of(g.rowsRi, MT) * tiles_of(g.X, NT) * 2 * g.kpRi * 3;
-        const double nTall = 2 * g.G <= NT ? (double)g.nT : tiles_of(2 * g.G, NT);
-        const double fT = 2.0 * 2 * g.N1h * tiles_of(g.Y, MT) * nTall * g.kpC * 3;
-        const double fRiT = 2.0 * 2 * tiles_of(g.G * g.Y, MT) * tiles_of(g.X, NT) * 2 * g.kpRi * 3;
-        const double bytesT = 2.0 * 2 * g.N1h * g.Y * g.kpC * 2;  // Toeplitz planes read once
-        // Form of the y stage: the Toeplitz matrices are read from HBM once per
-        // solve, so T wins once enough instances share them.
-        const double t_dft = (fC + fCi + fRi) / kTensorRate;
-        const double t_toe = std::max((fT + fRiT) / kTensorRate, bytesT / kHbmRate);
-        g.toe = ymode == YMODE_TOEPLITZ ? (g.G >= toe_min_group ? 1u : 0u)
-                : ymode == YMODE_DFT    ? 0u
-                                        : (t_toe < t_dft ? 1u : 0u);
+        const double fRi = 2.0 * tiles_of(g.rowsRi, MT) * tiles_of(g.X, 2 * NT) * 2 * g.kpRi * 3;
+        const double fT = 2.0 * 2 * g.N1h * tiles_of(2 * g.G, MT) * g.nTy * g.kpC * 3;
+        const double fRiT = 2.0 * 2 * tiles_of(g.G * g.Yp, MT) * tiles_of(g.X, 2 * NT) * 2 * g.kpRi * 3;
+        // Form of the y stage: Toeplitz when the group has at least
+        // kToeMinGroup instances (below that, T's M tile of 2G instance rows
+        // is mostly padding, and a lone instance's y DFT pair is cheaper:
+        // measured on B200 with single-instance groups of 32..512 cells), Y
+        // fits one T tile, and T executes fewer tensor flops than the y DFT pair.
+        const bool toe_ok = g.Y <= (uint32_t)T_NMAX;
+        const bool toe_cheaper = g.G >= kToeMinGroup && fT + fRiT < fC + fCi + fRi;
+        g.toe = !toe_ok                   ? 0u
+                : ymode == YMODE_TOEPLITZ ? (g.G >= toe_min_group ? 1u : 0u)
+                : ymode == YMODE_DFT      ? 0u
+                                          : (toe_cheaper ? 1u : 0u);
         if ((rc = I->alloc(&g.aR, (size_t)2 * g.rowsR * g.kpR))) return rc;
         if ((rc = I->alloc(&H.f1, (size_t)4 * g.N1h * H.kpF1))) return rc;
         if ((rc = I->alloc(&H.g1, (size_t)4 * g.X * H.kpG1))) return rc;
         if (g.toe) {
             if ((rc = I->alloc(&g.bT, (size_t)2 * g.rowsT * g.kpC))) return rc;
-            if ((rc = I->alloc(&H.aT, (size_t)2 * 2 * g.N1h * g.Y * g.kpC))) return rc;
+            if ((rc = I->alloc(&H.ts, (size_t)2 * 2 * g.N1h * g.SR * KT))) return rc;
             if ((rc = I->alloc(&g.aRiT, (size_t)4 * 2 * g.kpRi * g.MpT))) return rc;
         } else {
             if ((rc = I->alloc(&g.bC, (size_t)4 * g.rowsC * g.kpC))) return rc;
@@ -825,7 +947,7 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
             // y handled directly: only the x transform's 1/N1
             const double scale = -(double)6.673e-1f / (double)g.N1;
             spectra_x<<<blocks((size_t)g.N2 * g.N1h), 256>>>(tx, ty, g.N1, g.N2, g.N1h, scale);
-            toeplitz_expand<<<blocks((size_t)2 * g.N1h * g.Y * g.Y), 256>>>(tx, ty, H.aT, g.Y, g.N2, g.N1h, g.kpC);
+            toeplitz_strip<<<blocks((size_t)2 * g.N1h * g.SR * KT), 256>>>(tx, ty, H.ts, g.SR, g.N2, g.N1h, g.kpC);
         } else {
             dft_matrix<<<blocks((size_t)g.N2 * g.Y), 256>>>(H.f2, g.N2, g.Y, H.kpF2, g.N2, -1, 0);
             dft_matrix<<<blocks((size_t)g.Y * g.N2), 256>>>(H.g2, g.Y, g.N2, H.kpG2, g.N2, +1, 0);
@@ -850,7 +972,7 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
     std::vector<Group> gh(ng);
     for (size_t gi = 0; gi < ng; ++gi) gh[gi] = I->hg[gi].g;
     TPT_CUDA(cudaMemcpy(I->groups, gh.data(), ng * sizeof(Group), cudaMemcpyHostToDevice));
-    // Tensor map slots per group: 0 aR, 1 F1, 2 F2 | aT, 3 bC | bT, 4 G2,
+    // Tensor map slots per group: 0 aR, 1 F1, 2 F2 | strips, 3 bC | bT, 4 G2,
     // 5 bCi, 6 aRi | aRiT, 7 G1.
     std::vector<CUtensorMap> tm(8 * ng);
     std::vector<Problem> pr;
@@ -862,12 +984,13 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
     // fastest); the other operand is a small constant matrix.
     auto add_tiles = [&](int st, uint32_t prob, bool m_fastest) {
         const Problem &P = pr[prob];
+        const uint32_t nts = st == ST_RI ? 2 * NT : NT;  // R^-1 tiles are 256 columns wide
         if (m_fastest) {
-            for (uint32_t nt = 0; nt * NT < P.N; ++nt)
+            for (uint32_t nt = 0; nt * nts < P.N; ++nt)
                 for (uint32_t mt = 0; mt * MT < P.M; ++mt) tl[st].push_back({prob, (uint16_t)mt, (uint16_t)nt, 0});
         } else {
             for (uint32_t mt = 0; mt * MT < P.M; ++mt)
-                for (uint32_t nt = 0; nt * NT < P.N; ++nt) tl[st].push_back({prob, (uint16_t)mt, (uint16_t)nt, 0});
+                for (uint32_t nt = 0; nt * nts < P.N; ++nt) tl[st].push_back({prob, (uint16_t)mt, (uint16_t)nt, 0});
         }
     };
     for (size_t gi = 0; gi < ng; ++gi) {
@@ -879,26 +1002,25 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
         // stage R: A = aR (2 planes), B = F1
         if ((rc = make_tmap(&tmh[0], g.aR, g.kpR, 2 * g.rowsR))) return rc;
         if ((rc = make_tmap(&tmh[1], H.f1, H.kpF1, 4 * g.N1h))) return rc;
-        if ((rc = make_tmap(&tmh[7], H.g1, H.kpG1, 4 * g.X))) return rc;
+        if ((rc = make_tmap(&tmh[7], H.g1, H.kpG1, 4 * g.X, 2 * NT))) return rc;
         pr.push_back({tmd + 0, tmd + 1, gi32, g.rowsR, g.N1h, g.kpR / KT, g.rowsR, g.N1h, 0});
         add_tiles(ST_R, (uint32_t)pr.size() - 1, false);
         if (g.toe) {
-            // T: A = Toeplitz planes (rows (f, kx, y)), B = bT (rows (kx, inst, re/im))
-            if ((rc = make_tmap(&tmh[2], H.aT, g.kpC, 2 * 2 * g.N1h * g.Y))) return rc;
+            // T: A = bT (rows (kx, inst, re/im)), B = the (f, kx) strips (sbox-row boxes)
+            if ((rc = make_tmap(&tmh[2], H.ts, KT, 2 * 2 * g.N1h * g.SR, g.sbox))) return rc;
             if ((rc = make_tmap(&tmh[3], g.bT, g.kpC, 2 * g.rowsT))) return rc;
             // R^-1: A = aRiT read M-major, 32 x 32 boxes (rows (plane, f, kx))
             if ((rc = make_tmap(&tmh[6], g.aRiT, g.MpT, 8 * g.kpRi, 32))) return rc;
             const uint32_t pt = (uint32_t)pr.size();
-            pr.push_back({tmd + 2, tmd + 3, gi32, g.Y, 2 * g.G, g.kpC / KT, 2 * g.N1h * g.Y, g.rowsT, 0});
+            pr.push_back({tmd + 3, tmd + 2, gi32, 2 * g.G, g.Y, g.kpC / KT, g.rowsT, 0, 0});
             // kx slowest, so the tiles of one kx (both fields, all M tiles)
-            // share the B slice while it is in L2
+            // share the A slice while it is in L2
             for (uint32_t kx = 0; kx < g.N1h; ++kx)
                 for (uint32_t f = 0; f < 2; ++f)
-                    for (uint32_t mt = 0; mt * MT < g.Y; ++mt)
-                        for (uint32_t nt = 0; nt * NT < 2 * g.G; ++nt)
-                            tl[ST_T].push_back({pt, (uint16_t)mt, (uint16_t)nt, f * g.N1h + kx});
+                    for (uint32_t mt = 0; mt * MT < 2 * g.G; ++mt)
+                        tl[ST_T].push_back({pt, (uint16_t)mt, 0, f * g.N1h + kx});
             for (uint32_t f = 0; f < 2; ++f) {
-                pr.push_back({tmd + 6, tmd + 7, gi32, g.G * g.Y, g.X, g.kpRi / KT, g.kpRi, g.X, f + 1});
+                pr.push_back({tmd + 6, tmd + 7, gi32, g.G * g.Yp, g.X, 2 * g.kpRi / KT, g.kpRi, g.X, f + 1});
                 add_tiles(ST_RI, (uint32_t)pr.size() - 1, false);
             }
         } else {
@@ -914,7 +1036,7 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
             add_tiles(ST_C, (uint32_t)pr.size() - 1, true);
             pr.push_back({tmd + 4, tmd + 5, gi32, g.Y, g.rowsCi, g.kpCi / KT, g.Y, g.rowsCi, 0});
             add_tiles(ST_CI, (uint32_t)pr.size() - 1, true);
-            pr.push_back({tmd + 6, tmd + 7, gi32, g.rowsRi, g.X, g.kpRi / KT, g.rowsRi, g.X, 0});
+            pr.push_back({tmd + 6, tmd + 7, gi32, g.rowsRi, g.X, 2 * g.kpRi / KT, g.rowsRi, g.X, 0});
             add_tiles(ST_RI, (uint32_t)pr.size() - 1, false);
         }
         for (uint32_t r = 0; r < g.rowsR; ++r) pref.push_back({gi32, r});
@@ -962,7 +1084,7 @@ int DftSet::launch(cudaStream_t st, const SolveIO *io) const {
         act = 1;
     }
     uint32_t *err = I->err;
-    prep_mass<<<I->nprep, 128, 0, st>>>(I->groups, I->prep, I->ios, io0, act);
+    prep_mass<<<I->nprep, 64, 0, st>>>(I->groups, I->prep, I->ios, io0, act);
     TPT_LAUNCHED();
 #define TPT_DFT_STAGE(S)                                                                                      \
     if (I->ntiles[S]) {                                                                                      \
