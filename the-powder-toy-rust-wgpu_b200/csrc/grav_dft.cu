@@ -25,18 +25,24 @@
 //   T    C_f[y,kx] = sum_y' Tf_kx[y - y'] A[y',kx]     Tf_kx(dy) = sum_dx K_f(dx,dy) e^{-2 pi i kx dx/N1} / N1
 //
 // Tx is purely imaginary (Kx is odd in dx) and Ty real (Ky is even in dx),
-// so T is a real GEMM per (f, kx): M = Y, K = Y, N = the group's instances'
-// real and imaginary parts. Its epilogue writes R^-1's A operand M-major
-// ([kx][inst*Y + y]), which R^-1 reads as an MN-major tcgen05 operand. A
-// cost model picks the form per group (many instances amortise the Y x Y
-// matrices; a lone instance is cheaper through the y DFT).
+// so T is a real GEMM per (f, kx): M = the group's instances' real and
+// imaginary parts (2G rows), K = y', N = y. Its B operand, the Y x Y
+// Toeplitz matrix, is a window of a strip precomputed once per (f, kx)
+// (one TMA load per tile). Its epilogue writes R^-1's A operand M-major,
+// rows m' = ((y / 8) * G + inst) * 8 + y % 8 per (f, kx), which R^-1 reads
+// as an MN-major tcgen05 operand. Groups of at least 8 instances with
+// Y <= 256 take T; smaller groups are cheaper through the y DFT.
+//
+// R^-1 keeps only the real part, so it runs as one real GEMM over the
+// concatenated K' = [kx of Re C | kx of Im C] against [G1r ; -G1i] (the
+// second half with the A-negate bit), with 256-wide N tiles.
 //
 // GEMM kernel: 320 threads. Warp 0 issues TMA tile loads (64-byte swizzle,
-// 32-wide K tiles, no multicast) into a 3-stage shared-memory ring; warp 1
-// issues tcgen05.mma (M=128, N<=256, K=16) into a double-buffered TMEM
-// accumulator; warps 2-9 read the accumulator with tcgen05.ld and run the
-// stage's epilogue, which writes the next stage's operand planes. Every
-// mbarrier wait is bounded (see tc.cuh).
+// 32-wide K tiles, no multicast) into a shared-memory ring of 3 to 6
+// stages; warp 1 issues tcgen05.mma (M=128, N<=256, K=16) into a
+// double-buffered TMEM accumulator; warps 2-9 read the accumulator with
+// tcgen05.ld and run the stage's epilogue, which writes the next stage's
+// operand planes. Every mbarrier wait is bounded (see tc.cuh).
 #include <cudaTypedefs.h>
 #include <math.h>
 #include <stdlib.h>
@@ -94,7 +100,7 @@ struct Group {
     uint32_t MpT;                        // T: row length of aRiT (G * Yp rounded up to 32)
     uint32_t SR, sbox, snb;              // T: strip rows per (f, kx); TMA box rows; boxes per strip
     bf16 *aR, *bC, *bCi, *aRi;           // data operands (planes stacked), DFT form
-    bf16 *bT, *aRiT;                     // T's A operand [plane][kx][inst][re/im][y]; R^-1's A [plane][f][kx][inst*Yp + y]
+    bf16 *bT, *aRiT;                     // T's A operand [plane][kx][inst][re/im][y]; R^-1's A [plane][f][kx][m']
     const float *kxs, *kys;              // imaginary parts of the kernel spectra, [kx][ky]
 };
 
@@ -432,8 +438,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                 }
                 if constexpr (STAGE == ST_T) {
                     // row m = (inst, re/im) ; col = y -> R^-1's M-major A operand
-                    // aRiT[plane][f][kx][inst * Yp + y]: each lane writes 32
-                    // consecutive y of one part of C as 16-byte stores.
+                    // aRiT[plane][f][kx][m'], m' = ((y / 8) * G + inst) * 8 + y % 8:
+                    // a lane's 8-y piece sits next to the next instance's, so the
+                    // 16 lanes of one part write 256 contiguous bytes per store.
                     if (mrow0 >= 2 * Gp.G || nb >= Gp.Yp) continue;  // warp-uniform
                     float v[32];
                     tc::tmem_ld32(d + c0, v);
@@ -444,15 +451,17 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const uint32_t part = f ? ri : (ri ^ 1u);  // 0: Re C, 1: Im C
                     const float sgn = (f == 0 && ri == 0) ? -1.0f : 1.0f;
                     const size_t pst = (size_t)2 * Gp.kpRi * Gp.MpT;  // plane stride
-                    bf16 *o = Gp.aRiT + (size_t)((4 * part + f) * Gp.kpRi + kx) * Gp.MpT + (size_t)inst * Gp.Yp + nb;
+                    bf16 *o = Gp.aRiT + (size_t)((4 * part + f) * Gp.kpRi + kx) * Gp.MpT;
                     uint32_t hw[16], lw[16];
                     split_pack32(v, sgn, hw, lw);
                     // Yp is a multiple of 8: an 8-element piece is wholly inside or past the instance
 #pragma unroll
                     for (int k = 0; k < 4; ++k) {
-                        if (nb + 8 * k < Gp.Yp) {
-                            reinterpret_cast<uint4 *>(o)[k] = make_uint4(hw[4 * k], hw[4 * k + 1], hw[4 * k + 2], hw[4 * k + 3]);
-                            reinterpret_cast<uint4 *>(o + pst)[k] =
+                        const uint32_t yb = (nb >> 3) + k;
+                        if (8 * yb < Gp.Yp) {
+                            const size_t e = ((size_t)yb * Gp.G + inst) * 8;
+                            *reinterpret_cast<uint4 *>(o + e) = make_uint4(hw[4 * k], hw[4 * k + 1], hw[4 * k + 2], hw[4 * k + 3]);
+                            *reinterpret_cast<uint4 *>(o + pst + e) =
                                 make_uint4(lw[4 * k], lw[4 * k + 1], lw[4 * k + 2], lw[4 * k + 3]);
                         }
                     }
@@ -516,8 +525,10 @@ __global__ void __launch_bounds__(THREADS, 1)
                     if (!row_ok) continue;
                     uint32_t il, f, y;
                     if (P.a_mn) {
-                        il = m / Gp.Yp;  // aRiT rows are inst * Yp + y
-                        y = m - il * Gp.Yp;
+                        // aRiT rows are m = ((y / 8) * G + inst) * 8 + y % 8
+                        const uint32_t t8 = m >> 3, yb = t8 / Gp.G;
+                        il = t8 - yb * Gp.G;
+                        y = yb * 8 + (m & 7u);
                         f = P.a_mn - 1;
                         if (y >= Gp.Y) continue;
                     } else {
