@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(NT) kb_pressure_velocity(const AirInst *__rest
         tc::fence_mbar_init();
     }
     __syncthreads();
-    uint32_t uses[2] = {0, 0};
+    uint32_t uses = 0;  // bit k: phase parity of full[k] (a register, not an indexed array)
     auto issue = [&](uint32_t t, int k) {
         uint32_t i;
         int x0, y0;
@@ -76,8 +76,8 @@ __global__ void __launch_bounds__(NT) kb_pressure_velocity(const AirInst *__rest
             issue(tn, k ^ 1);
         }
         if (!a_loads(I)) continue;
-        bool ok = tc::mbar_wait(&full[k], uses[k] & 1u, &g_air_err);
-        ++uses[k];
+        bool ok = tc::mbar_wait(&full[k], (uses >> k) & 1u, &g_air_err);
+        uses ^= 1u << k;
         if (!__syncthreads_and(ok)) return;
         LayoutA2 S{&buf[k], opv};
         pass_a(I, x0, y0, S);
@@ -112,8 +112,12 @@ __device__ __forceinline__ void issue_b(const AirInst &I, const CUtensorMap *m, 
 
 // Also rebuilds the masks of its tile into the other half of the mask
 // ping-pong (read by the next tick) and writes the new heat into the other
-// half of the heat ping-pong, so a tick is two launches.
-__global__ void __launch_bounds__(NT) kb_advect_heat(const AirInst *__restrict__ insts,
+// half of the heat ping-pong, so a tick is two launches. The pass is bound
+// by issue latency (barriers, shared loads, the IEEE division sequences), so
+// registers are capped at 40 to keep six CTAs (48 warps) resident; shared
+// memory allows no more. Measured on B200: 6 CTAs 0.47 ms, 4 CTAs 0.52 ms,
+// 3 CTAs (69 registers) 0.55 ms per tick of the 6.1 M-cell batch.
+__global__ void __launch_bounds__(NT, 6) kb_advect_heat(const AirInst *__restrict__ insts,
                                                      const CUtensorMap *__restrict__ tmaps,
                                                      const TileRef *__restrict__ tiles, uint32_t ntiles,
                                                      uint32_t parity) {
@@ -126,7 +130,7 @@ __global__ void __launch_bounds__(NT) kb_advect_heat(const AirInst *__restrict__
         tc::fence_mbar_init();
     }
     __syncthreads();
-    uint32_t uses[2] = {0, 0};
+    uint32_t uses = 0;  // bit k: phase parity of full[k] (a register, not an indexed array)
     auto issue = [&](uint32_t t, int k) {
         uint32_t i;
         int x0, y0;
@@ -147,8 +151,8 @@ __global__ void __launch_bounds__(NT) kb_advect_heat(const AirInst *__restrict__
             issue(tn, k ^ 1);
         }
         if (b_loads(I)) {
-            bool ok = tc::mbar_wait(&full[k], uses[k] & 1u, &g_air_err);
-            ++uses[k];
+            bool ok = tc::mbar_wait(&full[k], (uses >> k) & 1u, &g_air_err);
+            uses ^= 1u << k;
             if (!__syncthreads_and(ok)) return;
             LayoutB2 S{&buf[k], &work};
             if (I.air_mode == 4u) {  // stored velocity of the +1 ring for the heat pass
