@@ -99,6 +99,7 @@ struct Group {
     uint32_t Yp;                         // T: rows per instance in aRiT (Y rounded up to 8)
     uint32_t MpT;                        // T: row length of aRiT (G * Yp rounded up to 32)
     uint32_t SR, sbox, snb;              // T: strip rows per (f, kx); TMA box rows; boxes per strip
+    uint32_t wR, wRI;                    // N tile widths of R (complex columns) and R^-1 (multiples of 16)
     bf16 *aR, *bC, *bCi, *aRi;           // data operands (planes stacked), DFT form
     bf16 *bT, *aRiT;                     // T's A operand [plane][kx][inst][re/im][y]; R^-1's A [plane][f][kx][m']
     const float *kxs, *kys;              // imaginary parts of the kernel spectra, [kx][ky]
@@ -207,7 +208,12 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const Tile T = tiles[t];
                 const Problem P = probs[T.problem];
                 int32_t m0 = T.mt * MT;
-                const int32_t n0 = T.nt * NTS;
+                // R and R^-1 tiles are the group's N width (little padding of N1h or X)
+                const uint32_t wN = STAGE == ST_R ? groups[P.group].wR : STAGE == ST_RI ? groups[P.group].wRI : NTS;
+                const int32_t n0 = T.nt * wN;
+                const uint32_t tx = STAGE == ST_R    ? 2 * TILE_BYTES + 4 * wN * KT * 2
+                                    : STAGE == ST_RI ? 2 * TILE_BYTES + 2 * wN * KT * 2
+                                                     : SBYTES;
                 if (STAGE == ST_T) {
                     // A = this tile's frequency slice of bT; B = the (f, kx) strip
                     const Group &Gq = groups[P.group];
@@ -231,7 +237,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                         break;
                     }
                     uint8_t *st = smem + s * SBYTES;
-                    tc::mbar_arrive_expect_tx(&full_bar[s], SBYTES);
+                    tc::mbar_arrive_expect_tx(&full_bar[s], tx);
                     if (STAGE == ST_RI) {
                         // K' tile kt: real parts (planes 0, 1), then imaginary parts (2, 3)
                         const uint32_t kh = P.ktiles / 2, part = kt >= kh ? 1u : 0u;
@@ -286,7 +292,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const uint32_t kpT = STAGE == ST_T ? groups[P.group].kpC : 0u;
                 const uint32_t I128 = tc::idesc_bf16(128, nmma, false, amn);
                 const uint32_t I128N = tc::idesc_bf16(128, 128, true, amn);
-                const uint32_t IRI = tc::idesc_bf16(128, 256, false, amn), IRIN = tc::idesc_bf16(128, 256, true, amn);
+                const uint32_t wRI = STAGE == ST_RI ? groups[P.group].wRI : 256u;
+                const uint32_t IRI = tc::idesc_bf16(128, wRI, false, amn), IRIN = tc::idesc_bf16(128, wRI, true, amn);
+                const uint32_t IR = tc::idesc_bf16(128, STAGE == ST_R ? groups[P.group].wR : 128u);
                 const uint32_t sb = tl & 1u;
                 if (STAGE == ST_T && !tc::mbar_wait(&strip_full[sb], (tl >> 1) & 1u, err)) {
                     abort_flag = 1;
@@ -332,6 +340,14 @@ __global__ void __launch_bounds__(THREADS, 1)
                             tc::mma_bf16(d, arh, tc::sdesc_k64(bhi + o), id, first);
                             tc::mma_bf16(d, arh, tc::sdesc_k64(blo + o), id, 1);
                             tc::mma_bf16(d, arl, tc::sdesc_k64(bhi + o), id, 1);
+                        } else if (STAGE == ST_R) {
+                            // Dr += Ar * Br, Di += Ar * Bi, each wR columns wide
+                            tc::mma_bf16(d, arh, tc::sdesc_k64(bhi + o), IR, first);
+                            tc::mma_bf16(d, arh, tc::sdesc_k64(blo + o), IR, 1);
+                            tc::mma_bf16(d, arl, tc::sdesc_k64(bhi + o), IR, 1);
+                            tc::mma_bf16(d + 128, arh, tc::sdesc_k64(bhi + TILE_BYTES + o), IR, first);
+                            tc::mma_bf16(d + 128, arh, tc::sdesc_k64(blo + TILE_BYTES + o), IR, 1);
+                            tc::mma_bf16(d + 128, arl, tc::sdesc_k64(bhi + TILE_BYTES + o), IR, 1);
                         } else {
                             // [Dr | Di] += Ar * [Br | Bi]
                             tc::mma_bf16(d, arh, tc::sdesc_k64(bhi + o), I256, first);
@@ -384,8 +400,10 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint32_t mrow0 = T.mt * MT + q * 32;  // first row of this warp
             const uint32_t m = mrow0 + lane;            // this thread's row
             const uint32_t d = tmem + acc * 256 + ((q * 32u) << 16);
+            const uint32_t wN = STAGE == ST_R ? Gp.wR : STAGE == ST_RI ? Gp.wRI : NTS;
             for (uint32_t c0 = half * (NTS / 2); c0 < (half + 1) * (NTS / 2); c0 += 32) {
-                const uint32_t nb = T.nt * NTS + c0;
+                if (c0 >= wN) continue;  // warp-uniform: past this tile's N width
+                const uint32_t nb = T.nt * wN + c0, jmax = wN - c0;  // columns j < jmax belong to the tile
                 const bool row_ok = m < P.M;
                 if constexpr (STAGE == ST_C) {
                     // row m = ky ; col = (inst, kx) -> B operand of C^-1: row (inst, f, kx), k = ky.
@@ -480,7 +498,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                         bf16 *o = Gp.bT + (size_t)(nb * 2 * Gp.G + il * 2) * Gp.kpC + y;
 #pragma unroll
                         for (int j = 0; j < 32; ++j) {
-                            if (nb + j < Gp.N1h) {
+                            if (nb + j < Gp.N1h && (uint32_t)j < jmax) {
                                 split_store(o, o + plane, vr[j]);
                                 split_store(o + Gp.kpC, o + Gp.kpC + plane, vi[j]);
                             }
@@ -493,7 +511,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                     bf16 *o = Gp.bC + (size_t)(il * Gp.N1hp + nb) * Gp.kpC + y;
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
-                        if (nb + j < Gp.N1h) {
+                        if (nb + j < Gp.N1h && (uint32_t)j < jmax) {
                             split_store(o, o + plane, vr[j]);
                             split_store(o + 2 * plane, o + 3 * plane, vi[j]);
                         }
@@ -541,7 +559,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                     const InstIO io = (io0_active && inst == 0) ? io0 : ios[inst];
                     float *out = (f ? io.gy : io.gx) + (size_t)y * io.pitch;
                     const uint32_t *mask = io.mask + (size_t)y * io.pitch;
-                    if (nb + 32 <= Gp.X && ((reinterpret_cast<uintptr_t>(out + nb) | reinterpret_cast<uintptr_t>(mask + nb)) & 15u) == 0u) {
+                    if (nb + 32 <= Gp.X && jmax >= 32u &&
+                        ((reinterpret_cast<uintptr_t>(out + nb) | reinterpret_cast<uintptr_t>(mask + nb)) & 15u) == 0u) {
                         // whole chunk, 16-byte aligned
                         const uint4 *mk = reinterpret_cast<const uint4 *>(mask + nb);
                         float4 *o4 = reinterpret_cast<float4 *>(out + nb);
@@ -555,7 +574,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                         for (int j = 0; j < 32; ++j) {
                             const uint32_t x = nb + j;
-                            if (x < Gp.X) out[x] = __ldg(mask + x) != 0u ? vr[j] : 0.0f;
+                            if (x < Gp.X && (uint32_t)j < jmax) out[x] = __ldg(mask + x) != 0u ? vr[j] : 0.0f;
                         }
                     }
                 }
@@ -903,6 +922,11 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
         g.Yp = round_up(g.Y, 8);
         g.MpT = round_up(g.G * g.Yp, 32);
         g.SR = g.nTy + g.kpC - KT;                               // strip rows
+        // R / R^-1 N tiles: the fewest tiles of at most 128 complex / 256 real
+        // columns, each a multiple of 16 wide (X = 400: 2 x 208 rather than 2 x 256)
+        const uint32_t ntR = (g.N1h + NT - 1) / NT, ntRI = (g.X + 2 * NT - 1) / (2 * NT);
+        g.wR = round_up((g.N1h + ntR - 1) / ntR, 16);
+        g.wRI = round_up((g.X + ntRI - 1) / ntRI, 16);
         g.snb = (g.SR + T_NMAX - 1) / T_NMAX;                    // TMA boxes per strip (box rows <= 256)
         g.sbox = round_up((g.SR + g.snb - 1) / g.snb, 8);        // box rows, 512-byte multiples
         H.kpF1 = g.kpR;   // F1: N1h rows, K = x
@@ -911,12 +935,12 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
         H.kpG1 = g.kpRi;  // G1: X rows, K = kx
         // executed tensor flops (3-term split, padded tiles) of both y forms
         auto tiles_of = [](uint32_t v, uint32_t t) { return (double)((v + t - 1) / t) * t; };
-        const double fR = 2.0 * tiles_of(g.rowsR, MT) * tiles_of(g.N1h, NT) * 2 * g.kpR * 3;
+        const double fR = 2.0 * tiles_of(g.rowsR, MT) * tiles_of(g.N1h, g.wR) * 2 * g.kpR * 3;
         const double fC = 2.0 * tiles_of(g.N2, MT) * tiles_of(g.rowsC, NT) * 4 * g.kpC * 3;
         const double fCi = 2.0 * tiles_of(g.Y, MT) * tiles_of(g.rowsCi, NT) * 4 * g.kpCi * 3;
-        const double fRi = 2.0 * tiles_of(g.rowsRi, MT) * tiles_of(g.X, 2 * NT) * 2 * g.kpRi * 3;
+        const double fRi = 2.0 * tiles_of(g.rowsRi, MT) * tiles_of(g.X, g.wRI) * 2 * g.kpRi * 3;
         const double fT = 2.0 * 2 * g.N1h * tiles_of(2 * g.G, MT) * g.nTy * g.kpC * 3;
-        const double fRiT = 2.0 * 2 * tiles_of(g.G * g.Yp, MT) * tiles_of(g.X, 2 * NT) * 2 * g.kpRi * 3;
+        const double fRiT = 2.0 * 2 * tiles_of(g.G * g.Yp, MT) * tiles_of(g.X, g.wRI) * 2 * g.kpRi * 3;
         // Form of the y stage: Toeplitz when the group has at least
         // kToeMinGroup instances (below that, T's M tile of 2G instance rows
         // is mostly padding, and a lone instance's y DFT pair is cheaper:
@@ -995,7 +1019,8 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
     // fastest); the other operand is a small constant matrix.
     auto add_tiles = [&](int st, uint32_t prob, bool m_fastest) {
         const Problem &P = pr[prob];
-        const uint32_t nts = st == ST_RI ? 2 * NT : NT;  // R^-1 tiles are 256 columns wide
+        const Group &gq = I->hg[P.group].g;
+        const uint32_t nts = st == ST_R ? gq.wR : st == ST_RI ? gq.wRI : NT;
         if (m_fastest) {
             for (uint32_t nt = 0; nt * nts < P.N; ++nt)
                 for (uint32_t mt = 0; mt * MT < P.M; ++mt) tl[st].push_back({prob, (uint16_t)mt, (uint16_t)nt, 0});
@@ -1012,8 +1037,8 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
         const uint32_t gi32 = (uint32_t)gi;
         // stage R: A = aR (2 planes), B = F1
         if ((rc = make_tmap(&tmh[0], g.aR, g.kpR, 2 * g.rowsR))) return rc;
-        if ((rc = make_tmap(&tmh[1], H.f1, H.kpF1, 4 * g.N1h))) return rc;
-        if ((rc = make_tmap(&tmh[7], H.g1, H.kpG1, 4 * g.X, 2 * NT))) return rc;
+        if ((rc = make_tmap(&tmh[1], H.f1, H.kpF1, 4 * g.N1h, g.wR))) return rc;
+        if ((rc = make_tmap(&tmh[7], H.g1, H.kpG1, 4 * g.X, g.wRI))) return rc;
         pr.push_back({tmd + 0, tmd + 1, gi32, g.rowsR, g.N1h, g.kpR / KT, g.rowsR, g.N1h, 0});
         add_tiles(ST_R, (uint32_t)pr.size() - 1, false);
         if (g.toe) {
@@ -1059,6 +1084,10 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     for (int st = 0; st < NSTAGES; ++st) {
+        // Longest K loops first: CTA b takes tiles b, b + grid, ..., so a
+        // long tile placed late would start late and stretch the launch.
+        std::stable_sort(tl[st].begin(), tl[st].end(),
+                         [&](const Tile &a, const Tile &b) { return pr[a.problem].ktiles > pr[b.problem].ktiles; });
         if ((rc = I->alloc(&I->tiles[st], tl[st].size()))) return rc;
         TPT_CUDA(cudaMemcpy(I->tiles[st], tl[st].data(), tl[st].size() * sizeof(Tile), cudaMemcpyHostToDevice));
         I->ntiles[st] = (uint32_t)tl[st].size();
