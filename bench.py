@@ -41,6 +41,11 @@ sys.path.insert(0, os.path.join(ROOT, "the-powder-toy-rust-wgpu_b200"))
 import numpy as np  # noqa: E402
 
 B_AIR = 52  # algorithmic bytes per cell-tick of the air step (reference layout)
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one air tick
+# (both launches) and of one gravity solve of the whole batch (the five GEMM
+# launches), from one ncu capture of each kernel on that workload at the tuned
+# setting; workloads without a capture report null.
+MEASURED_DRAM_BYTES = {5: {"air_tick": 532.8e6, "grav_solve": 418.4e6}}
 WORKLOAD_NAMES = {
     1: "C1 plain FP32 air+gravity, 153x96 cells (612x384 canvas)",
     2: "C2 plain FP32 air+gravity, 400x225 cells (1600x900 canvas)",
@@ -316,14 +321,17 @@ def run_ours(args, rank, world, local):
     roof_air = {"kernel": "air tick (pressure+velocity, advection+heat+masks)", "bound": "hbm",
                 "achieved": round(air_gbs, 1), "peak": hbm, "unit": "GB/s", "frac": round(air_gbs / hbm, 4),
                 "peak_source": peak_src, "algorithmic_bytes_per_cell_tick": B_AIR,
-                "traffic": None, "ms_per_tick": round(prof.air_ms / prof.ticks, 5),
+                "traffic": MEASURED_DRAM_BYTES.get(cid, {}).get("air_tick"),
+                "traffic_unit": "DRAM bytes per tick, both launches (ncu)",
+                "ms_per_tick": round(prof.air_ms / prof.ticks, 5),
                 "avg_launch_ms": round(air_launch_ms, 5)}
     phases = {"air_ms_per_tick": prof.air_ms / prof.ticks, "grav_ms_per_tick": prof.grav_ms / prof.ticks}
     if precision == tf.PRECISION_SPLIT_BF16 and prof.grav_ms > 0:
         tfl = prof.grav_flops_per_tick * prof.ticks / (prof.grav_ms / 1e3) / 1e12
         roof_grav = {"kernel": "split-BF16 DFT-GEMM gravity", "bound": "tensor", "achieved": round(tfl, 2),
                      "peak": bf16, "unit": "TFLOP/s", "frac": round(tfl / bf16, 4), "peak_source": peak_src,
-                     "traffic": None}
+                     "traffic": MEASURED_DRAM_BYTES.get(cid, {}).get("grav_solve"),
+                     "traffic_unit": "DRAM bytes per solve of the batch, GEMM launches (ncu)"}
     else:
         roof_grav = None
     dominant = roof_grav if (roof_grav and prof.grav_ms > prof.air_ms) else roof_air

@@ -84,3 +84,28 @@ def test_air_100_ticks_vs_fp64(cuda, tf, oracle, case):
         rec[f"{k}_relmax"] = float(np.abs(got[k] - want64[k]).max() / max(np.abs(want64[k]).max(), 1e-30))
     REPORT[f"air/100 ticks/{case} ({inst.xcells}x{inst.ycells}) vs fp64"] = rec
     _dump()
+
+
+def test_gravity_error_c5_batch_both_y_forms(cuda, tf, oracle):
+    """The C5 batch as benchmarked: its 64-instance 400x225 group takes the
+    Toeplitz y stage and the heavy-tail singletons the y DFT pair; both are
+    held to the 1e-4 bar against FP64."""
+    import workloads as W
+
+    insts = W.config_instances(5)
+    b = tf.Batch(insts, tf.PRECISION_SPLIT_BF16)
+    b.step(2)  # mass is fixed, so the fields of any tick are the solve of that mass
+    cuda.cuda.synchronize()
+    assert tf.lib().tpt_check_device_errors() == 0
+    worst = 0.0
+    for i, label in ((0, "Toeplitz y stage"), (63, "Toeplitz y stage"), (70, "y DFT pair"), (100, "y DFT pair")):
+        inst = insts[i]
+        st = b.state(i)
+        dx, dy = oracle.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx, dtype=np.float64)
+        ex, ey = _err(st["gx"], dx), _err(st["gy"], dy)
+        REPORT[f"gravity/split_bf16/C5 batch, instance {i}, {label} ({inst.xcells}x{inst.ycells})"] = {
+            "gx_relmax": ex[0], "gx_relL2": ex[1], "gy_relmax": ey[0], "gy_relL2": ey[1]}
+        worst = max(worst, *ex, *ey)
+    _dump()
+    b.close()
+    assert worst <= 1e-4
