@@ -222,6 +222,57 @@ int tpt_grav_mask_rebuild(const uint32_t *wall_bmap_host, uint32_t *mask_host,
  * round half away from zero of m * 65536 in f32 arithmetic. */
 int32_t tpt_mass_to_fixed(float m);
 
+/* ---- gravity tick with particles -------------------------------------- */
+
+/* Particle slots, struct of arrays (`SimBuffers::part_*`,
+ * crates/tpt-sim/src/buffers/mod.rs:186-230), device pointers. */
+typedef struct tpt_particles {
+    uint32_t num_slots;       /* slots scanned (`used_slot_bound`)               */
+    const uint32_t *ty;       /* element id; 0 = PT_NONE                         */
+    const float *x, *y;       /* position in pixels                              */
+    float *vx, *vy;           /* velocity, updated in place                      */
+    const int32_t *life, *tmp;
+    const float *temp;        /* kelvin                                          */
+    const uint32_t *flags;    /* 0x08 FLAG_MOVABLE, 0x10 rigid-body pixel         */
+    const uint32_t *move_lut; /* 12 words per element id (`build_move_lut`):
+                                 [0] properties, [7] loss as f32 bits           */
+    uint32_t n_types;         /* element ids below this have a record (PT_NUM)   */
+} tpt_particles;
+
+/* One sandbox's gravity grids (`SimBuffers`), device pointers, each
+ * (xres / 4) * (yres / 4) cells; the plan's size must be that cell grid. */
+typedef struct tpt_grav_state {
+    uint32_t xres, yres;              /* canvas in pixels                        */
+    const uint32_t *wall_bmap, *wall_emap, *grav_mask;
+    int32_t *mass;                    /* this tick's accumulator (gpu_grav_mass)  */
+    int32_t *mass_prev;               /* snapshot the solve reads                 */
+    float *tool_mass;                 /* painted PGRV/NGRV wells, consumed; NULL = none */
+    const int32_t *override_mass;     /* one-tick CEXP/GSNS mass writes; NULL = none   */
+    const uint32_t *override_set;
+    float *gx, *gy;                   /* the solved field                         */
+    float newton_grav;                /* NEWTON_GRAVITY_SCALE (1.0)               */
+} tpt_grav_state;
+
+/*
+ * One Newtonian-gravity tick around the solve, replacing the body of
+ * `step_gravity_gpu` (crates/tpt-sim/src/gravity_kernel.rs:826-1010) after
+ * the mask rebuild (call tpt_grav_mask_rebuild on a wall change, as the
+ * reference does):
+ *   0. painted wells are folded into mass_prev (`seed_gravity_tool_mass_kernel`,
+ *      :241-262) and the accumulator is cleared (`seed_gravity_mass_kernel`,
+ *      :217-229);
+ *   1. gx/gy = the plan's solve of mass_prev (`GravityFft::solve`);
+ *   2. every particle gets its element's Loss, then newton_grav * g of its
+ *      cell (`apply_gravity_kernel`, :434-516), and adds its element's mass to
+ *      the accumulator in fixed point (`build_gravity_mass_kernel`, :275-376),
+ *      in one pass over the slots;
+ *   3. the override writes replace their cells (`apply_grav_mass_override_kernel`,
+ *      :379-391) and mass_prev = mass (`copy_gravity_mass_kernel`, :518-527).
+ * With Newtonian gravity off the reference skips the pass; so does the caller.
+ */
+int tpt_grav_step(tpt_grav_plan *plan, const tpt_grav_state *state,
+                  const tpt_particles *parts, tpt_stream_t stream);
+
 /* ---- batched instances ------------------------------------------------- */
 
 typedef struct tpt_batch tpt_batch;

@@ -66,6 +66,9 @@ def lib():
         _lib.ora_align_dim.argtypes = [u32]
         _lib.ora_align_dim.restype = u32
         _lib.ora_set_threads.argtypes = [i32]
+        _lib.ora_grav_seed.argtypes = [P, u32]
+        _lib.ora_grav_particles.argtypes = [P, P, u32, u32]
+        _lib.ora_grav_finish.argtypes = [P, u32]
         _lib.ora_num_threads.restype = i32
     return _lib
 
@@ -181,3 +184,49 @@ def gravity_tool_cell(x, y, xres, yres, xcells, ycells):
 
 def align_dim(v: int) -> int:
     return int(lib().ora_align_dim(v))
+
+
+# ---- gravity tick around the solve (gravity_kernel.rs:217-527) ------------
+class _Particles(ctypes.Structure):  # tpt_particles with host pointers
+    _fields_ = [("num_slots", ctypes.c_uint32)] + [(n, ctypes.c_void_p) for n in (
+        "ty", "x", "y", "vx", "vy", "life", "tmp", "temp", "flags", "move_lut")] + [("n_types", ctypes.c_uint32)]
+
+
+class _GravState(ctypes.Structure):  # tpt_grav_state with host pointers
+    _fields_ = [("xres", ctypes.c_uint32), ("yres", ctypes.c_uint32)] + [(n, ctypes.c_void_p) for n in (
+        "wall_bmap", "wall_emap", "grav_mask", "mass", "mass_prev", "tool_mass", "override_mass", "override_set",
+        "gx", "gy")] + [("newton_grav", ctypes.c_float)]
+
+
+_STATE_TYPES = {"wall_bmap": np.uint32, "wall_emap": np.uint32, "grav_mask": np.uint32, "mass": np.int32,
+                "mass_prev": np.int32, "tool_mass": np.float32, "override_mass": np.int32,
+                "override_set": np.uint32, "gx": np.float32, "gy": np.float32}
+_PART_TYPES = {"ty": np.uint32, "x": np.float32, "y": np.float32, "vx": np.float32, "vy": np.float32,
+               "life": np.int32, "tmp": np.int32, "temp": np.float32, "flags": np.uint32}
+
+
+def _state(state: dict, xres: int, yres: int, newton: float):
+    arrs = {k: (None if state.get(k) is None else np.ascontiguousarray(state[k], t).copy())
+            for k, t in _STATE_TYPES.items()}
+    st = _GravState(xres=xres, yres=yres, newton_grav=float(newton), **{k: _p(a) for k, a in arrs.items()})
+    return st, arrs
+
+
+def grav_seed(state: dict, xres: int, yres: int) -> dict:
+    """Wells folded into mass_prev, accumulator cleared (before the solve)."""
+    st, arrs = _state(state, xres, yres, 1.0)
+    lib().ora_grav_seed(ctypes.byref(st), (xres // 4) * (yres // 4))
+    return arrs
+
+
+def grav_particles_and_finish(state: dict, parts: dict, move_lut, n_types: int, xres: int, yres: int,
+                              newton: float = 1.0):
+    """Force on the particles (with the gx/gy given in `state`), mass build,
+    overrides, snapshot copy. Returns (state', parts')."""
+    st, arrs = _state(state, xres, yres, newton)
+    pa = {k: np.ascontiguousarray(parts[k], t).copy() for k, t in _PART_TYPES.items()}
+    lut = np.ascontiguousarray(move_lut, np.uint32)
+    q = _Particles(num_slots=len(pa["ty"]), n_types=n_types, move_lut=_p(lut), **{k: _p(a) for k, a in pa.items()})
+    lib().ora_grav_particles(ctypes.byref(st), ctypes.byref(q), xres // 4, yres // 4)
+    lib().ora_grav_finish(ctypes.byref(st), (xres // 4) * (yres // 4))
+    return arrs, pa

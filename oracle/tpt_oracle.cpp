@@ -9,6 +9,8 @@
 //   air      crates/tpt-sim/src/air_kernel/{mod,pressure,advect,heat,settle}.rs
 //   gravity  crates/tpt-sim/src/gravity_gpu/{mod,fft}.rs
 //   masks    crates/tpt-sim/src/gravity_kernel.rs:658-712 (flood fill)
+//   particles crates/tpt-sim/src/gravity_kernel.rs:217-527 (wells, force,
+//            mass build, overrides, snapshot copy)
 //
 // Two forms, one template:
 //   R = float   the FP32 mirror: the reference's operation order, every
@@ -851,6 +853,120 @@ int32_t ora_mass_to_fixed(float m) {
     if (scaled >= 0.0f) scaled += 0.5f;
     else scaled -= 0.5f;
     return (int32_t)scaled;
+}
+
+// ---- gravity tick around the solve (host pointers in the ABI structs) ------
+// f32 -> i32 truncation as the GPU converts: NaN -> 0, out of range saturates.
+static int32_t trunc_i32(float v) {
+    if (!(v == v)) return 0;
+    if (v >= 2147483648.0f) return INT32_MAX;
+    if (v < -2147483648.0f) return INT32_MIN;
+    return (int32_t)v;
+}
+static int32_t to_fixed(float m) {  // gravity_kernel.rs:346-353
+    float scaled = m * 65536.0f;
+    if (scaled >= 0.0f) scaled += 0.5f;
+    else scaled -= 0.5f;
+    return trunc_i32(scaled);
+}
+
+// seed_gravity_tool_mass_kernel (gravity_kernel.rs:241-262), then
+// seed_gravity_mass_kernel (:217-229) once the wells are consumed.
+void ora_grav_seed(const tpt_grav_state *s, uint32_t cells) {
+    for (uint32_t c = 0; c < cells; ++c) {
+        if (s->tool_mass && s->tool_mass[c] != 0.0f) {
+            s->mass_prev[c] = to_fixed(s->tool_mass[c]);
+            s->tool_mass[c] = 0.0f;
+        }
+    }
+    for (uint32_t c = 0; c < cells; ++c) {
+        float tool = s->tool_mass ? s->tool_mass[c] : 0.0f;
+        s->mass[c] = to_fixed(tool);
+        if (s->tool_mass) s->tool_mass[c] = 0.0f;
+    }
+}
+
+// apply_gravity_kernel (gravity_kernel.rs:434-516), all slots, then
+// build_gravity_mass_kernel (:275-376), all slots; the accumulator wraps like
+// the device's 32-bit atomic add.
+void ora_grav_particles(const tpt_grav_state *s, const tpt_particles *q, uint32_t xcells, uint32_t ycells) {
+    const int32_t xres = (int32_t)s->xres, yres = (int32_t)s->yres;
+    for (uint32_t i = 0; i < q->num_slots; ++i) {
+        const uint32_t ty = q->ty[i];
+        if (ty == 0u || ty >= q->n_types) continue;
+        const uint32_t flags = q->flags[i];
+        bool eligible = (flags & 0x10u) == 0u;
+        const int32_t xi = trunc_i32(q->x[i] + 0.5f), yi = trunc_i32(q->y[i] + 0.5f);
+        if (xi < 0 || yi < 0 || xi >= xres || yi >= yres) eligible = false;
+        if (xi < 4 || yi < 4 || xi >= xres - 4 || yi >= yres - 4) eligible = false;
+        if (!eligible) continue;
+        const size_t cell = (size_t)((uint32_t)yi / 4u) * xcells + (uint32_t)xi / 4u;
+        if (s->wall_bmap[cell] == 18u && (s->wall_emap[cell] & 0xFFu) < 8u) continue;
+        const uint32_t props = q->move_lut[(size_t)ty * 12];
+        float loss;
+        std::memcpy(&loss, &q->move_lut[(size_t)ty * 12 + 7], 4);
+        if (!(ty == 78u && (flags & 0x08u) != 0u)) {
+            q->vx[i] *= loss;
+            q->vy[i] *= loss;
+        }
+        if ((props & 0x4u) == 0u) {
+            q->vx[i] += s->newton_grav * s->gx[cell];
+            q->vy[i] += s->newton_grav * s->gy[cell];
+        }
+    }
+    for (uint32_t i = 0; i < q->num_slots; ++i) {
+        const uint32_t ty = q->ty[i];
+        if (ty == 0u) continue;
+        float mass = 0.0f;
+        bool contributes = false;
+        if (ty == 39u) {  // GRVT
+            int32_t tmp = q->tmp[i];
+            if (tmp < -100) tmp = -100;
+            if (tmp > 100) tmp = 100;
+            mass = 0.2f * (float)tmp;
+            contributes = true;
+        } else if (ty == 40u || ty == 41u) {  // NBHL, NWHL
+            float hole = 0.1f;
+            if (q->tmp[i] != 0) {
+                hole = 0.001f * (float)q->tmp[i];
+                if (hole < 0.1f) hole = 0.1f;
+                if (hole > 51.2f) hole = 51.2f;
+            }
+            if (ty == 41u) hole = -hole;
+            mass = hole;
+            contributes = true;
+        } else if (ty == 42u) {  // GBMB
+            if (q->life[i] > 20) {
+                mass = 20.0f;
+                contributes = true;
+            } else if (q->life[i] >= 1) {
+                mass = -80.0f;
+                contributes = true;
+            }
+        } else if (ty == 43u) {  // GPMP
+            if (q->life[i] == 10) {
+                mass = 0.2f * (q->temp[i] - 273.15f);
+                contributes = true;
+            }
+        }
+        if (!contributes) continue;
+        const int32_t xi = trunc_i32(q->x[i] + 0.5f), yi = trunc_i32(q->y[i] + 0.5f);
+        if (xi < 0 || yi < 0 || xi >= xres || yi >= yres) continue;
+        const uint32_t cx = (uint32_t)xi / 4u, cy = (uint32_t)yi / 4u;
+        if (cx >= xcells || cy >= ycells) continue;
+        const size_t cell = (size_t)cy * xcells + cx;
+        if (s->grav_mask[cell] == 0u) continue;
+        const int32_t qv = to_fixed(mass);
+        if (qv != 0) s->mass[cell] = (int32_t)((uint32_t)s->mass[cell] + (uint32_t)qv);
+    }
+}
+
+// apply_grav_mass_override_kernel (gravity_kernel.rs:379-391), then
+// copy_gravity_mass_kernel (:518-527).
+void ora_grav_finish(const tpt_grav_state *s, uint32_t cells) {
+    for (uint32_t c = 0; c < cells; ++c)
+        if (s->override_set && s->override_set[c] != 0u) s->mass[c] = s->override_mass[c];
+    for (uint32_t c = 0; c < cells; ++c) s->mass_prev[c] = s->mass[c];
 }
 
 }  // extern "C"

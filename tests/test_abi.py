@@ -52,6 +52,7 @@ def test_arguments_are_validated_before_any_device_work(tf):
     d[0].air.xcells, d[0].air.ycells = 2, 10
     assert lib.tpt_batch_create(1, d, 0, ctypes.byref(h)) == -1
     assert lib.tpt_grav_solve(None, None, 1.0, None, None, None, None) == -2
+    assert lib.tpt_grav_step(None, None, None, None) == -2
     assert lib.tpt_batch_step(None, 1, None) == -2
     assert lib.tpt_grav_plan_destroy(None) == 0 and lib.tpt_batch_destroy(None) == 0
 

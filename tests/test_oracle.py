@@ -172,3 +172,118 @@ def test_gravity_mask_flood_fill(oracle):
         m = oracle.grav_mask(inst.wall, X, Y)
         assert np.array_equal(m, W.grav_mask(inst.wall, X, Y))
         assert (m == 0).any() and (m == 0xFFFFFFFF).any()
+
+
+def _tick_case(oracle, parts, state_over=None, lut_loss=0.5, solid=(), newton=1.0):
+    """One particle-side tick on a 64x64-px (16x16-cell) sandbox with g = (1.5,
+    -2.0) everywhere; returns (state', parts')."""
+    import workloads as W
+
+    xres = yres = 64
+    cells = 16 * 16
+    st = {"wall_bmap": np.zeros(cells, np.uint32), "wall_emap": np.zeros(cells, np.uint32),
+          "grav_mask": np.full(cells, 0xFFFFFFFF, np.uint32), "mass": np.full(cells, 77, np.int32),
+          "mass_prev": np.zeros(cells, np.int32), "gx": np.full(cells, 1.5, np.float32),
+          "gy": np.full(cells, -2.0, np.float32)}
+    st.update(state_over or {})
+    n = len(parts["ty"])
+    full = {"ty": np.zeros(n, np.uint32), "x": np.full(n, 20.0, np.float32), "y": np.full(n, 20.0, np.float32),
+            "vx": np.full(n, 2.0, np.float32), "vy": np.full(n, -4.0, np.float32), "life": np.zeros(n, np.int32),
+            "tmp": np.zeros(n, np.int32), "temp": np.full(n, 295.15, np.float32), "flags": np.zeros(n, np.uint32)}
+    full.update({k: np.asarray(v, full[k].dtype) for k, v in parts.items()})
+    lut = np.zeros((192, 12), np.uint32)
+    lut[:, 7] = np.float32(lut_loss).view(np.uint32)
+    for t in solid:
+        lut[t, 0] = W.TYPE_SOLID
+    seeded = oracle.grav_seed(st, xres, yres)
+    return oracle.grav_particles_and_finish(seeded, full, lut.reshape(-1), 192, xres, yres, newton)
+
+
+def test_gravity_tick_element_masses(oracle):
+    # gravity_kernel.rs:297-334: the mass each gravity element adds, in fixed point
+    import workloads as W
+
+    cell = 5 * 16 + 5  # pixel (20, 20)
+    cases = [  # (ty, life, tmp, temp) -> mass
+        ((W.PT_NBHL, 0, 0, 0.0), 0.1),          # NBHL default hole
+        ((W.PT_NBHL, 0, 5000, 0.0), 5.0),       # 0.001 * tmp
+        ((W.PT_NBHL, 0, 90000, 0.0), 51.2),     # clamped high
+        ((W.PT_NWHL, 0, 20, 0.0), -0.1),        # clamped low, negated
+        ((W.PT_GRVT, 0, 300, 0.0), 20.0),       # tmp clamped to 100, * 0.2
+        ((W.PT_GRVT, 0, -7, 0.0), -1.4),
+        ((W.PT_GBMB, 25, 0, 0.0), 20.0),        # armed
+        ((W.PT_GBMB, 3, 0, 0.0), -80.0),        # counting down
+        ((W.PT_GBMB, 0, 0, 0.0), None),         # inert
+        ((W.PT_GPMP, 10, 0, 373.15), 20.0),     # on: 0.2 * (temp - 273.15)
+        ((W.PT_GPMP, 9, 0, 373.15), None),      # off
+        ((W.PT_SPNG, 0, 0, 0.0), None),         # not a gravity element
+    ]
+    for (ty, life, tmp, temp), m in cases:
+        st, _ = _tick_case(oracle, {"ty": [ty], "life": [life], "tmp": [tmp], "temp": [temp]})
+        want = 0 if m is None else oracle.mass_to_fixed(np.float32(m) if ty != W.PT_GRVT else
+                                                        np.float32(0.2) * np.float32(min(max(tmp, -100), 100)))
+        assert st["mass"][cell] == want and st["mass_prev"][cell] == want, (ty, life, tmp, st["mass"][cell], want)
+        assert np.count_nonzero(st["mass"]) == (0 if m is None else 1)  # the stale accumulator is cleared
+
+
+def test_gravity_tick_accumulates_masks_and_overrides(oracle):
+    import workloads as W
+
+    cell = 5 * 16 + 5
+    # two holes in one cell add; a masked cell drops its contribution
+    st, _ = _tick_case(oracle, {"ty": [W.PT_NBHL, W.PT_NBHL, W.PT_NBHL], "x": [20.0, 21.0, 44.0],
+                                "y": [20.0, 22.0, 44.0]},
+                       {"grav_mask": np.where(np.arange(256) == 11 * 16 + 11, 0, 0xFFFFFFFF).astype(np.uint32)})
+    assert st["mass"][cell] == 2 * oracle.mass_to_fixed(0.1) and st["mass"][11 * 16 + 11] == 0
+    # an override replaces the cell's accumulated mass; the snapshot copies it
+    ovr = np.zeros(256, np.int32)
+    ovr[cell] = -123
+    st, _ = _tick_case(oracle, {"ty": [W.PT_NBHL]}, {"override_mass": ovr,
+                                                    "override_set": (ovr != 0).astype(np.uint32)})
+    assert st["mass"][cell] == -123 and st["mass_prev"][cell] == -123
+    # a painted well is folded into the snapshot the solve reads, then consumed
+    tool = np.zeros(256, np.float32)
+    tool[7] = 2.5
+    seeded = oracle.grav_seed({"mass": np.ones(256, np.int32), "mass_prev": np.zeros(256, np.int32),
+                               "tool_mass": tool, "wall_bmap": None, "wall_emap": None, "grav_mask": None,
+                               "gx": None, "gy": None}, 64, 64)
+    assert seeded["mass_prev"][7] == oracle.mass_to_fixed(2.5) and not seeded["tool_mass"].any()
+    assert not seeded["mass"].any()
+
+
+def test_gravity_tick_force_on_particles(oracle):
+    # apply_gravity_kernel (gravity_kernel.rs:434-516): Loss then newton * g
+    import workloads as W
+
+    f32 = np.float32
+    loss = f32(0.5)
+    _, p = _tick_case(oracle, {"ty": [1, 27, W.PT_SPNG, W.PT_SPNG, 1, 1, 1, 1, 250],
+                               "flags": [0, 0, 0x08, 0, 0x10, 0, 0, 0, 0],
+                               "x": [20, 20, 20, 20, 20, 2.0, 61.0, -3.0, 20], "y": [20] * 9},
+                      solid=(27,))
+    vx, vy = f32(2.0), f32(-4.0)
+    assert p["vx"][0] == vx * loss + f32(1.5) and p["vy"][0] == vy * loss + f32(-2.0)   # plain element
+    assert p["vx"][1] == vx * loss and p["vy"][1] == vy * loss                           # solid: Loss only
+    assert p["vx"][2] == vx + f32(1.5)                                                   # movable sponge: no Loss
+    assert p["vx"][3] == vx * loss + f32(1.5)                                            # sponge
+    for i in (4, 5, 6, 7, 8):  # rigid pixel, margin, margin, off canvas, id past the table
+        assert p["vx"][i] == vx and p["vy"][i] == vy, i
+    # unpowered stasis freezes, powered does not
+    w = np.zeros(256, np.uint32)
+    w[5 * 16 + 5] = W.WL_STASIS
+    for emap, frozen in ((3, True), (8, False)):
+        e = np.zeros(256, np.uint32)
+        e[5 * 16 + 5] = emap
+        _, p = _tick_case(oracle, {"ty": [1]}, {"wall_bmap": w, "wall_emap": e})
+        assert (p["vx"][0] == vx) == frozen
+
+
+def test_gravity_tick_fixed_point_literals(oracle):
+    # hand-computed: 0.1f * 65536 = 6553.6 -> 6554; 20 * 65536; -80 * 65536; -0.1 -> -6554
+    import workloads as W
+
+    cell = 5 * 16 + 5
+    for ty, life, tmp, want in ((W.PT_NBHL, 0, 0, 6554), (W.PT_GBMB, 21, 0, 1310720), (W.PT_GBMB, 1, 0, -5242880),
+                                (W.PT_NWHL, 0, 0, -6554)):
+        st, _ = _tick_case(oracle, {"ty": [ty], "life": [life], "tmp": [tmp]})
+        assert st["mass_prev"][cell] == want, (ty, st["mass_prev"][cell])

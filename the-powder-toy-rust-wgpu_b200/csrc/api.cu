@@ -10,6 +10,7 @@
 
 #include "air_launch.hpp"
 #include "grav_dft.hpp"
+#include "grav_particles.hpp"
 #include "grav_plan.hpp"
 #include "tmap.hpp"
 
@@ -307,6 +308,30 @@ int tpt_grav_solve_f32(tpt_grav_plan *p, const float *mass, const uint32_t *mask
                        tpt_stream_t stream) {
     if (!mass) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_grav_solve_f32: mass is NULL");
     return grav_solve_any(p, nullptr, mass, 1.0f, mask, gx, gy, stream);
+}
+
+int tpt_grav_step(tpt_grav_plan *p, const tpt_grav_state *s, const tpt_particles *q, tpt_stream_t stream) {
+    if (!p || !s || !q) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_grav_step: NULL plan, state or particles");
+    if (!s->wall_bmap || !s->wall_emap || !s->grav_mask || !s->mass || !s->mass_prev || !s->gx || !s->gy)
+        TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_grav_step: NULL grid pointer");
+    if (!s->override_mass != !s->override_set)
+        TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_grav_step: override_mass and override_set must both be set or both NULL");
+    if (s->xres / 4u != p->X || s->yres / 4u != p->Y)
+        TPT_FAIL(TPT_ERR_INVALID_DIMS, "tpt_grav_step: canvas %ux%u px is not the plan's %ux%u cells", s->xres,
+                 s->yres, p->X, p->Y);
+    if (q->num_slots && (!q->ty || !q->x || !q->y || !q->vx || !q->vy || !q->life || !q->tmp || !q->temp ||
+                         !q->flags || !q->move_lut))
+        TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_grav_step: NULL particle array");
+    gp::GravGrids G{s->xres, s->yres, p->X, p->Y, s->wall_bmap, s->wall_emap, s->grav_mask, s->mass, s->mass_prev,
+                    s->tool_mass, s->override_mass, s->override_set, s->gx, s->gy, s->newton_grav};
+    gp::Parts P{q->num_slots, q->n_types, q->ty, q->x, q->y, q->vx, q->vy, q->life, q->tmp, q->temp, q->flags,
+                q->move_lut};
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = gp::launch_seed(G, st);
+    if (rc) return rc;
+    rc = grav_solve_any(p, s->mass_prev, nullptr, 1.0f / 65536.0f, s->grav_mask, s->gx, s->gy, stream);
+    if (rc) return rc;
+    return gp::launch_particles_and_finish(G, P, st);
 }
 
 }  // extern "C"

@@ -45,7 +45,7 @@ PRECISION_SPLIT_BF16 = 1
 EXPORTS = [
     "tpt_air_params_default", "tpt_air_step", "tpt_air_step_static_scratch", "tpt_wall_masks_host", "tpt_grav_plan_create",
     "tpt_grav_plan_destroy", "tpt_grav_plan_dims", "tpt_grav_solve", "tpt_grav_solve_f32",
-    "tpt_grav_mask_rebuild", "tpt_mass_to_fixed", "tpt_batch_create", "tpt_batch_destroy", "tpt_batch_fields",
+    "tpt_grav_mask_rebuild", "tpt_mass_to_fixed", "tpt_grav_step", "tpt_batch_create", "tpt_batch_destroy", "tpt_batch_fields",
     "tpt_batch_write", "tpt_batch_read", "tpt_batch_step", "tpt_batch_tune", "tpt_batch_get_tuning",
     "tpt_batch_set_tuning", "tpt_batch_profile_phases", "tpt_check_device_errors", "tpt_last_error_string",
     "tpt_kernel_launch_count", "tpt_version",
@@ -74,6 +74,24 @@ class AirBufs(ctypes.Structure):
         "pv", "vx", "vy", "hv", "opv", "ovx", "ovy", "ohv", "block_air", "block_airh", "wall_bmap", "wall_emap",
         "elem_block_air", "elem_block_airh", "fan_vx", "fan_vy", "pmap", "elem_props")] + [
         ("xres", ctypes.c_uint32), ("yres", ctypes.c_uint32), ("n_elements", ctypes.c_uint32)]
+
+
+class Particles(ctypes.Structure):
+    """tpt_particles: particle slots, struct of arrays (device pointers)."""
+    _fields_ = [("num_slots", ctypes.c_uint32)] + [(n, ctypes.c_void_p) for n in (
+        "ty", "x", "y", "vx", "vy", "life", "tmp", "temp", "flags", "move_lut")] + [("n_types", ctypes.c_uint32)]
+
+
+class GravState(ctypes.Structure):
+    """tpt_grav_state: one sandbox's gravity grids (device pointers)."""
+    _fields_ = [("xres", ctypes.c_uint32), ("yres", ctypes.c_uint32)] + [(n, ctypes.c_void_p) for n in (
+        "wall_bmap", "wall_emap", "grav_mask", "mass", "mass_prev", "tool_mass", "override_mass", "override_set",
+        "gx", "gy")] + [("newton_grav", ctypes.c_float)]
+
+
+PARTICLE_FIELDS = ("ty", "x", "y", "vx", "vy", "life", "tmp", "temp", "flags")
+GRAV_STATE_FIELDS = ("wall_bmap", "wall_emap", "grav_mask", "mass", "mass_prev", "tool_mass", "override_mass",
+                     "override_set", "gx", "gy")
 
 
 class InstanceDesc(ctypes.Structure):
@@ -126,6 +144,7 @@ def lib() -> ctypes.CDLL:
         L.tpt_grav_mask_rebuild.argtypes = [P, P, u32, u32]
         L.tpt_mass_to_fixed.argtypes = [f32]
         L.tpt_mass_to_fixed.restype = ctypes.c_int32
+        L.tpt_grav_step.argtypes = [P, ctypes.POINTER(GravState), ctypes.POINTER(Particles), P]
         L.tpt_batch_create.argtypes = [u32, ctypes.POINTER(InstanceDesc), i32, ctypes.POINTER(P)]
         L.tpt_batch_destroy.argtypes = [P]
         L.tpt_batch_fields.argtypes = [P, u32, ctypes.POINTER(InstanceFields)]
@@ -342,6 +361,23 @@ class GravityFft:
         else:
             check(lib().tpt_grav_solve(self._plan, _ptr(mass), float(mass_scale_inv), _ptr(bufs.grav_mask),
                                        _ptr(bufs.grav_fx), _ptr(bufs.grav_fy), _stream(stream)))
+
+    def step(self, state: dict, parts: dict, move_lut, n_types: int, xres: int, yres: int,
+             newton_grav: float = 1.0, stream=None) -> None:
+        """One gravity tick with particles (`step_gravity_gpu`,
+        crates/tpt-sim/src/gravity_kernel.rs:826-1010, after the mask
+        rebuild): wells into `mass_prev`, the solve into `gx`/`gy`, Loss and
+        the force on the particles' `vx`/`vy`, the mass grid rebuilt from the
+        particles and copied into `mass_prev`. `state` maps GRAV_STATE_FIELDS
+        to device tensors (tool_mass and the override pair may be missing or
+        None); `parts` maps PARTICLE_FIELDS to device tensors of one length."""
+        self._ensure(xres // 4, yres // 4)
+        st = GravState(xres=xres, yres=yres, newton_grav=float(newton_grav),
+                       **{k: (_ptr(state[k]) if state.get(k) is not None else None) for k in GRAV_STATE_FIELDS})
+        n = int(parts["ty"].numel()) if parts else 0
+        pa = Particles(num_slots=n, n_types=int(n_types), move_lut=_ptr(move_lut),
+                       **{k: _ptr(parts[k]) for k in PARTICLE_FIELDS})
+        check(lib().tpt_grav_step(self._plan, ctypes.byref(st), ctypes.byref(pa), _stream(stream)))
 
     def close(self):
         if self._plan is not None:

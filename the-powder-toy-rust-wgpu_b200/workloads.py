@@ -340,3 +340,82 @@ def config_instances(config_id: int, limit: int | None = None) -> list[Instance]
 
 
 CONFIG_TICKS = {1: 1000, 2: 10000, 3: 1, 4: 1000, 5: 1000}
+
+
+# ------------------------------------------------ gravity tick particles --
+
+# Element ids the gravity tick branches on (crates/tpt-core/src/constants.rs).
+PT_GRVT, PT_NBHL, PT_NWHL, PT_GBMB, PT_GPMP, PT_SPNG = 39, 40, 41, 42, 43, 78
+TYPE_SOLID = 0x4
+WL_STASIS = 18
+
+
+def move_lut(n_types: int, seed: int) -> np.ndarray:
+    """A movement table of `n_types` 12-word records (the layout of the
+    reference's `build_move_lut`): word 0 the element properties (TYPE_SOLID
+    on about a third of the ids), word 7 the f32 bits of Loss in [0.5, 1]."""
+    st = Stream(seed)
+    lut = np.zeros((n_types, 12), np.uint32)
+    props = (st.u64(n_types) % np.uint64(3) == np.uint64(0)).astype(np.uint32) * np.uint32(TYPE_SOLID)
+    loss = st.uniform(0.5, 1.0, n_types).astype(np.float32)
+    lut[:, 0] = props
+    lut[:, 7] = loss.view(np.uint32)
+    return lut.reshape(-1)
+
+
+def gravity_particles(xres: int, yres: int, n: int, seed: int, n_types: int = 192) -> dict:
+    """Seeded particle slots for the gravity tick: every gravity element with
+    its mass cases (GRVT tmp beyond the clamp, NBHL/NWHL tmp 0 and beyond the
+    range, GBMB armed / counting / inert, GPMP on and off), SPNG with and
+    without FLAG_MOVABLE, rigid pixels, empty slots, ids past the table,
+    positions off the canvas and in the 4-px margin, several particles per
+    cell. Struct of arrays, numpy."""
+    st = Stream(seed)
+    kinds = np.array([0, PT_GRVT, PT_NBHL, PT_NWHL, PT_GBMB, PT_GPMP, PT_SPNG, 1, 5, 27, n_types + 3],
+                     np.uint32)
+    ty = kinds[(st.u64(n) % np.uint64(len(kinds))).astype(np.int64)]
+    x = st.uniform(-6.0, xres + 6.0, n).astype(np.float32)
+    y = st.uniform(-6.0, yres + 6.0, n).astype(np.float32)
+    # a cluster of particles in a few cells, so several add to one cell
+    k = n // 8
+    x[:k] = (40.0 + (st.u64(k) % np.uint64(3)).astype(np.float64) * 4.0).astype(np.float32)
+    y[:k] = np.float32(48.0)
+    vx = st.uniform(-20.0, 20.0, n).astype(np.float32)
+    vy = st.uniform(-20.0, 20.0, n).astype(np.float32)
+    life = (st.u64(n) % np.uint64(40)).astype(np.int32)
+    life[(st.u64(n) % np.uint64(4)) == 0] = 10
+    tmp = (st.u64(n) % np.uint64(120001)).astype(np.int64) - 60000
+    tmp[(st.u64(n) % np.uint64(5)) == 0] = 0
+    temp = st.uniform(0.0, 9999.0, n).astype(np.float32)
+    flags = np.zeros(n, np.uint32)
+    r = st.u64(n) % np.uint64(8)
+    flags[r == 0] |= np.uint32(0x08)
+    flags[r == 1] |= np.uint32(0x10)
+    return {"ty": ty, "x": x, "y": y, "vx": vx, "vy": vy, "life": life, "tmp": tmp.astype(np.int32),
+            "temp": temp, "flags": flags}
+
+
+def gravity_state(xres: int, yres: int, seed: int) -> dict:
+    """Seeded gravity grids of one sandbox for the tick: walls with WL_GRAV
+    pockets (masked cells) and WL_STASIS with powered and unpowered emap,
+    painted wells, overrides on a few cells, a stale accumulator."""
+    X, Y = xres // 4, yres // 4
+    st = Stream(seed)
+    cells = X * Y
+    wall = np.zeros(cells, np.uint32)
+    r = st.u64(cells) % np.uint64(40)
+    wall[r == 0] = WL_STASIS
+    g = np.zeros((Y, X), bool)
+    g[Y // 3:Y // 3 + 3, X // 4:X // 4 + 6] = True  # a ring of GRAV walls
+    g[Y // 3 + 1, X // 4 + 1:X // 4 + 5] = False
+    wall[g.reshape(-1)] = WL_GRAV
+    emap = (st.u64(cells) % np.uint64(16)).astype(np.uint32)
+    tool = np.zeros(cells, np.float32)
+    tool[(st.u64(cells) % np.uint64(97)) == 0] = st.uniform(-5.0, 5.0, 1)[0]
+    ovr_set = ((st.u64(cells) % np.uint64(61)) == 0).astype(np.uint32)
+    ovr = (st.u64(cells) % np.uint64(200001)).astype(np.int64) - 100000
+    return {"wall_bmap": wall, "wall_emap": emap, "grav_mask": grav_mask(wall, X, Y),
+            "mass": (st.u64(cells) % np.uint64(1000)).astype(np.int32),  # stale: the tick clears it
+            "mass_prev": (st.u64(cells) % np.uint64(70000)).astype(np.int32),
+            "tool_mass": tool, "override_mass": ovr.astype(np.int32), "override_set": ovr_set,
+            "gx": np.zeros(cells, np.float32), "gy": np.zeros(cells, np.float32)}
