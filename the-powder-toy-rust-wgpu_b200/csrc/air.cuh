@@ -29,6 +29,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "exact_div.cuh"
 
 namespace tpt {
 namespace air {
@@ -360,7 +361,7 @@ __device__ __forceinline__ void smooth_advect_cell(const AirInst &I, L &S, int x
                                                    float &out_vy, float &out_pv) {
     const uint32_t X = I.X, Y = I.Y;
     const float cvx = S.OVX(x, y, x0, y0), cvy = S.OVY(x, y, x0, y0), cpv = S.OPV(x, y, x0, y0);
-    float sx = 0.0f, sy = 0.0f, sp = 0.0f, ws = 0.0f;
+    float sx = 0.0f, sy = 0.0f, sp = 0.0f;
     if ((uint32_t)x >= 2u && (uint32_t)x + 3u <= X && (uint32_t)y >= 2u && (uint32_t)y + 3u <= Y) {
         // every tap is an interior cell: fixed offsets, no saturation
 #pragma unroll
@@ -376,7 +377,6 @@ __device__ __forceinline__ void smooth_advect_cell(const AirInst &I, L &S, int x
                 sx += tx * w;
                 sy += ty * w;
                 sp += tp * w;
-                ws += w;
             }
         }
     } else {
@@ -399,11 +399,12 @@ __device__ __forceinline__ void smooth_advect_cell(const AirInst &I, L &S, int x
                 sx += tx * w;
                 sy += ty * w;
                 sp += tp * w;
-                ws += w;
             }
         }
     }
-    float nvx = sx / ws, nvy = sy / ws, npv = sp / ws;
+    // / wsum: every tap adds its weight, so the sum is the constant kSmoothWsum
+    float nvx = div_by_const(sx, kSmoothWsum, kSmoothWsumRcp), nvy = div_by_const(sy, kSmoothWsum, kSmoothWsumRcp),
+          npv = div_by_const(sp, kSmoothWsum, kSmoothWsumRcp);
 
     float tx0, ty0;
     far_advect_target(
@@ -458,7 +459,7 @@ __device__ __forceinline__ void smooth_advect_cell(const AirInst &I, L &S, int x
         float dwx = (wxp - wxm) * 0.5f;
         float dwy = (wyp - wym) * 0.5f;
         float norm = sqrtf(dwx * dwx + dwy * dwy);
-        float k = I.vcoef / 5.0f;
+        float k = I.vk;
         nvx += k * dwy / (norm + 0.001f) * w;
         nvy += k * (0.0f - dwx) / (norm + 0.001f) * w;
     }
@@ -486,7 +487,7 @@ __device__ __forceinline__ float heat_cell(const AirInst &I, L &S, int x, int y,
                                            float &vy_io) {
     const uint32_t X = I.X, Y = I.Y;
     const float ch = S.HV(x, y, x0, y0), cvx = S.NVX(x, y, x0, y0), cvy = S.NVY(x, y, x0, y0);
-    float sh = 0.0f, sx = 0.0f, sy = 0.0f, ws = 0.0f;
+    float sh = 0.0f, sx = 0.0f, sy = 0.0f;
     if ((uint32_t)x >= 2u && (uint32_t)x + 3u <= X && (uint32_t)y >= 2u && (uint32_t)y + 3u <= Y) {
         // every tap is an interior cell: fixed offsets, no saturation
 #pragma unroll
@@ -502,7 +503,6 @@ __device__ __forceinline__ float heat_cell(const AirInst &I, L &S, int x, int y,
                 sh += th * w;
                 sx += tx * w;
                 sy += ty * w;
-                ws += w;
             }
         }
     } else {
@@ -525,12 +525,11 @@ __device__ __forceinline__ float heat_cell(const AirInst &I, L &S, int x, int y,
                 sh += th * w;
                 sx += tx * w;
                 sy += ty * w;
-                ws += w;
             }
         }
     }
-    float dh = sh / ws;
-    float svx = sx / ws, svy = sy / ws;
+    float dh = div_by_const(sh, kSmoothWsum, kSmoothWsumRcp);
+    float svx = div_by_const(sx, kSmoothWsum, kSmoothWsumRcp), svy = div_by_const(sy, kSmoothWsum, kSmoothWsumRcp);
     float tx, ty;
     far_advect_target(
         x, y, svx, svy,
@@ -587,7 +586,8 @@ __device__ __forceinline__ float heat_cell(const AirInst &I, L &S, int x, int y,
         float convx = 0.0f - gxv, convy = 0.0f - gyv;
         float nx = cvx, ny = cvy;
         if (I.conv == 1u) {
-            float weight = ((ch - S.HV(x - 1, y, x0, y0)) * convx + (ch - S.HV(x, y - 1, x0, y0)) * convy) / 5000.0f;
+            float weight = div_by_const((ch - S.HV(x - 1, y, x0, y0)) * convx + (ch - S.HV(x, y - 1, x0, y0)) * convy,
+                                        kConvLegacy, kConvLegacyRcp);
             if (weight > 0.0f && !S.hblk(x, y - 1, x0, y0)) {
                 nx += weight * convx;
                 ny += weight * convy;
@@ -598,7 +598,7 @@ __device__ __forceinline__ float heat_cell(const AirInst &I, L &S, int x, int y,
                 convx /= 0.1f * gm;
                 convy /= 0.1f * gm;
             }
-            float weight = (ch - I.amb) / 10000.0f;
+            float weight = div_by_const(ch - I.amb, kConvBouss, kConvBoussRcp);
             if (weight > 0.01f) weight = 0.01f;
             nx += weight * convx;
             ny += weight * convy;

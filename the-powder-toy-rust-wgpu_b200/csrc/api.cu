@@ -97,6 +97,7 @@ AirInst make_air_inst(const tpt_air_params &p) {
     I.evy = p.edge_vy;
     I.amb = p.ambient_air_temp;
     I.vcoef = p.vorticity_coeff;
+    I.vk = p.vorticity_coeff / 5.0f;
     I.cgx = p.custom_gx;
     I.cgy = p.custom_gy;
     return I;

@@ -53,6 +53,7 @@ struct AirInst {
     uint32_t pitch;  // row stride (elements) of every grid of the instance
     uint32_t air_mode, aheat, conv, gmode;
     float ep, evx, evy, amb, vcoef, cgx, cgy;
+    float vk;  // vcoef / 5 (advect.rs:317), divided once on the host in f32
     float *pv, *vx, *vy, *hv;
     float *opv, *ovx, *ovy, *ohv;
     uint32_t *bair, *bairh;
