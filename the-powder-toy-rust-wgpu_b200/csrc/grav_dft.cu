@@ -414,20 +414,22 @@ __global__ void __launch_bounds__(THREADS, 1)
                     if (mrow0 >= P.M || il >= Gp.G) continue;  // warp-uniform
                     const size_t plane = (size_t)Gp.rowsCi * Gp.kpCi;
                     const uint32_t kx = kx0 + lane;  // after the transpose
+                    // Each field's 32 spectrum values are loaded once (one round
+                    // trip) and serve both parts.
 #pragma unroll 1
-                    for (int part = 0; part < 2; ++part) {
-                        float v[32];
-                        tc::tmem_ld32(d + (part ? 0u : 128u) + c0, v);  // part 0 needs Bi, part 1 Br
+                    for (int f = 0; f < 2; ++f) {
+                        const float *ks = f ? Gp.kys : Gp.kxs;
+                        float kv[32];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            kv[j] = (row_ok && kx0 + j < Gp.N1h) ? __ldg(ks + (size_t)(kx0 + j) * Gp.N2 + m) : 0.0f;
 #pragma unroll 1
-                        for (int f = 0; f < 2; ++f) {
-                            const float *ks = f ? Gp.kys : Gp.kxs;
+                        for (int part = 0; part < 2; ++part) {
+                            float v[32];
+                            tc::tmem_ld32(d + (part ? 0u : 128u) + c0, v);  // part 0 needs Bi, part 1 Br
                             const float sgn = part ? 1.0f : -1.0f;
 #pragma unroll
-                            for (int j = 0; j < 32; ++j) {
-                                const float kv =
-                                    (row_ok && kx0 + j < Gp.N1h) ? __ldg(ks + (size_t)(kx0 + j) * Gp.N2 + m) : 0.0f;
-                                xbuf[lane * 33 + j] = sgn * v[j] * kv;
-                            }
+                            for (int j = 0; j < 32; ++j) xbuf[lane * 33 + j] = sgn * v[j] * kv[j];
                             __syncwarp();
                             if (kx < Gp.N1h) {
                                 bf16 *o = Gp.bCi + (size_t)((il * 2 + f) * Gp.N1hp + kx) * Gp.kpCi + mrow0 +
