@@ -370,6 +370,109 @@ typedef struct tpt_batch_profile {
 int tpt_batch_profile_phases(tpt_batch *batch, uint32_t ticks,
                              tpt_stream_t stream, tpt_batch_profile *out);
 
+/* ---- 3-D sandbox field step (crates/tpt-sim/src/voxel3d) ---------------
+ *
+ * The 3-D sandbox's coarse grid: 64^3 cells of 4^3 voxels, one f32 (or i32)
+ * per cell, index (y << 12) | (z << 6) | x (air_kernel.rs:5-8). Voxels are
+ * 256^3 u32 words, index (y << 16) | (z << 8) | x, packed as
+ * ty | temp_q << 8 | life << 24 with temp = temp_q * 0.125 K
+ * (step/mod.rs:125-133). Bricks are 8^3 voxels, brick id
+ * (by << 10) | (bz << 5) | bx (air_kernel.rs:227-230).
+ *
+ * The reference's tick (engine.rs:195-208) calls, in order,
+ * AirState::gather, AirState::solve, gravity::solve, gravity::clear_mass and,
+ * after the element passes, gravity::gather. Each has an entry point below;
+ * tpt_vox_field_step runs the first four for a list of worlds.
+ */
+enum {
+    TPT_VOX_AXIS = 64,          /* cells per axis (AIR_AXIS)               */
+    TPT_VOX_CELLS = 262144,     /* AIR_COUNT                               */
+    TPT_VOX_VOXELS = 16777216,  /* VOXEL_COUNT                             */
+    TPT_VOX_BRICKS = 32768,     /* BRICK_COUNT                             */
+    TPT_VOX_AIR_ITERATIONS = 12,  /* AIR_JACOBI_ITERATIONS, the default    */
+    TPT_VOX_GRAV_ITERATIONS = 24  /* GRAVITY_ITERATIONS (fixed)            */
+};
+
+/* How a plan runs the Jacobi solves. */
+enum {
+    TPT_VOX_AUTO = 0,      /* the cluster form when the device can schedule it */
+    TPT_VOX_CLUSTER = 1,   /* one 16-CTA cluster per field, the whole grid in
+                              distributed shared memory, one launch per step */
+    TPT_VOX_PER_SWEEP = 2  /* one launch per pass and per sweep, the
+                              reference's launch structure                  */
+};
+
+/*
+ * One world's device buffers. Every field is TPT_VOX_CELLS elements except
+ * `voxel` and `aux_tmp` (TPT_VOX_VOXELS) and `sim_list` (TPT_VOX_BRICKS).
+ * `sim_count` is the device word triple [n, 1, 1] the brick compaction
+ * writes (step/active.rs:38-46); the gathers read n on the device.
+ */
+typedef struct tpt_vox_world {
+    const uint32_t *voxel;     /* voxel_a                                  */
+    const int32_t *aux_tmp;    /* per-voxel tmp, read by the gravity gather */
+    const uint32_t *sim_list;  /* active brick ids                         */
+    const uint32_t *sim_count; /* [n, 1, 1]                                */
+    /* AirState (air.rs:52-80) */
+    float *vx, *vy, *vz;
+    float *p, *p_tmp;          /* Jacobi pressure pair                     */
+    float *temp, *solid;
+    int32_t *pv;               /* TPT pressure, 1/1024 fixed point         */
+    /* gravity (buffers.rs:108-118) */
+    int32_t *grav_mass;        /* 1/1024 fixed-point mass accumulator      */
+    float *grav_potential, *grav_potential_tmp;
+    float *grav_force_x, *grav_force_y, *grav_force_z;
+} tpt_vox_world;
+
+typedef struct tpt_vox_plan tpt_vox_plan;
+
+/*
+ * Creates a plan running the solves in `form` (TPT_VOX_*). AUTO picks the
+ * cluster form when the device can hold a 16-CTA cluster of the kernel and
+ * the per-sweep form otherwise; CLUSTER fails with TPT_ERR_UNSUPPORTED
+ * then. The plan owns the per-sweep form's scratch (the reference's
+ * velocity snapshot, air.rs:78-79); no entry point below allocates.
+ */
+int tpt_vox_plan_create(int form, tpt_vox_plan **out);
+int tpt_vox_plan_destroy(tpt_vox_plan *plan);
+/* The form the plan runs (TPT_VOX_CLUSTER or TPT_VOX_PER_SWEEP). */
+int tpt_vox_plan_form(const tpt_vox_plan *plan);
+
+/* air_clear_kernel (air_kernel.rs:182-204): zero velocity, pressure, solid
+ * and pv; ambient temperature 293.15 K. Replaces AirState::new's clear. */
+int tpt_vox_air_clear(const tpt_vox_world *world, tpt_stream_t stream);
+/* AirState::gather (air.rs:126-148, air_kernel.rs:218-278): solid fraction
+ * and mean non-empty temperature of the cells of every listed brick. */
+int tpt_vox_air_gather(tpt_vox_plan *plan, const tpt_vox_world *world,
+                       tpt_stream_t stream);
+/* AirState::solve (air.rs:162-222): pv update, `iterations` Jacobi sweeps of
+ * p / p_tmp (the reference's alternation: odd sweeps write p_tmp, even ones
+ * p), then the advection of vx/vy/vz. iterations <= 65536. */
+int tpt_vox_air_solve(tpt_vox_plan *plan, const tpt_vox_world *world,
+                      uint32_t iterations, tpt_stream_t stream);
+/* gravity::solve (gravity.rs:228-260): 24 Jacobi sweeps of the potential
+ * from grav_mass, then the force field. On return grav_potential holds the
+ * last sweep and grav_potential_tmp the one before, as the reference's
+ * handle swap leaves them. */
+int tpt_vox_grav_solve(tpt_vox_plan *plan, const tpt_vox_world *world,
+                       tpt_stream_t stream);
+/* gravity::clear_mass (gravity.rs:264-273). */
+int tpt_vox_grav_clear_mass(tpt_vox_plan *plan, const tpt_vox_world *world,
+                            tpt_stream_t stream);
+/* gravity::gather (gravity.rs:276-289, 125-166): adds the fixed-point mass
+ * of every listed brick's gravity elements to grav_mass. */
+int tpt_vox_grav_gather(tpt_vox_plan *plan, const tpt_vox_world *world,
+                        tpt_stream_t stream);
+/*
+ * For each of the `n` worlds: air gather, air solve (`air_iterations`),
+ * gravity solve, clear mass -- the same result as calling the four entry
+ * points above in that order per world. In the cluster form the solves of
+ * all worlds are one launch, air and gravity clusters running side by side.
+ */
+int tpt_vox_field_step(tpt_vox_plan *plan, const tpt_vox_world *worlds,
+                       uint32_t n, uint32_t air_iterations,
+                       tpt_stream_t stream);
+
 /* ---- diagnostics ------------------------------------------------------- */
 
 /*

@@ -31,6 +31,14 @@ class AirParams(ctypes.Structure):
     ]
 
 
+class VoxWorld(ctypes.Structure):
+    """Same layout as `tpt_vox_world` in include/tpt_field.h (host pointers here)."""
+
+    _fields_ = [(n, ctypes.c_void_p) for n in (
+        "voxel", "aux_tmp", "sim_list", "sim_count", "vx", "vy", "vz", "p", "p_tmp", "temp", "solid", "pv",
+        "grav_mass", "grav_potential", "grav_potential_tmp", "grav_force_x", "grav_force_y", "grav_force_z")]
+
+
 def build() -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
 
@@ -70,6 +78,13 @@ def lib():
         _lib.ora_grav_particles.argtypes = [P, P, u32, u32]
         _lib.ora_grav_finish.argtypes = [P, u32]
         _lib.ora_num_threads.restype = i32
+        W = ctypes.POINTER(VoxWorld)
+        _lib.ora_vox_air_clear.argtypes = [W]
+        _lib.ora_vox_air_gather.argtypes = [W, u32]
+        _lib.ora_vox_air_solve.argtypes = [W, u32]
+        _lib.ora_vox_grav_solve.argtypes = [W, u32]
+        _lib.ora_vox_grav_clear_mass.argtypes = [W]
+        _lib.ora_vox_grav_gather.argtypes = [W, u32]
     return _lib
 
 
@@ -230,3 +245,50 @@ def grav_particles_and_finish(state: dict, parts: dict, move_lut, n_types: int, 
     lib().ora_grav_particles(ctypes.byref(st), ctypes.byref(q), xres // 4, yres // 4)
     lib().ora_grav_finish(ctypes.byref(st), (xres // 4) * (yres // 4))
     return arrs, pa
+
+
+# ------------------------------------------------------------ 3-D ------
+# The 3-D sandbox's field step (crates/tpt-sim/src/voxel3d), in place on a
+# dict of numpy arrays with the keys of workloads.voxel_world.
+
+def _vox(d: dict) -> VoxWorld:
+    w = VoxWorld()
+    for name, _ in VoxWorld._fields_:
+        if name in d:
+            a = d[name]
+            assert a.flags["C_CONTIGUOUS"]
+            setattr(w, name, a.ctypes.data)
+    return w
+
+
+def vox_air_clear(d: dict) -> None:
+    lib().ora_vox_air_clear(ctypes.byref(_vox(d)))
+
+
+def vox_air_gather(d: dict) -> None:
+    lib().ora_vox_air_gather(ctypes.byref(_vox(d)), int(d["sim_count"][0]))
+
+
+def vox_air_solve(d: dict, iterations: int = 12) -> None:
+    lib().ora_vox_air_solve(ctypes.byref(_vox(d)), int(iterations))
+
+
+def vox_grav_solve(d: dict, iterations: int = 24) -> None:
+    lib().ora_vox_grav_solve(ctypes.byref(_vox(d)), int(iterations))
+
+
+def vox_grav_clear_mass(d: dict) -> None:
+    lib().ora_vox_grav_clear_mass(ctypes.byref(_vox(d)))
+
+
+def vox_grav_gather(d: dict) -> None:
+    lib().ora_vox_grav_gather(ctypes.byref(_vox(d)), int(d["sim_count"][0]))
+
+
+def vox_field_step(d: dict, iterations: int = 12) -> None:
+    """The reference tick's field part (engine.rs:195-208): air gather, air
+    solve, gravity solve, clear mass."""
+    vox_air_gather(d)
+    vox_air_solve(d, iterations)
+    vox_grav_solve(d)
+    vox_grav_clear_mass(d)

@@ -970,3 +970,274 @@ void ora_grav_finish(const tpt_grav_state *s, uint32_t cells) {
 }
 
 }  // extern "C"
+
+// ======================================================= 3-D field step ====
+// The 3-D sandbox's coarse grid (crates/tpt-sim/src/voxel3d): 64^3 cells,
+// index (y << 12) | (z << 6) | x; voxels 256^3, index (y << 16) | (z << 8) | x.
+// Each function is the reference kernel run over every cell in index order,
+// f32 throughout (no contraction), with the reference's buffer alternation.
+namespace vox {
+
+constexpr uint32_t N = 64, SZ = 64, SY = 4096, CELLS = 262144;
+
+static inline float clampf(float v, float lo, float hi) {  // step/mod.rs:425-435
+    float out = v;
+    if (out < lo) out = lo;
+    if (out > hi) out = hi;
+    return out;
+}
+static inline float seed_f32(float anchor, float v) { return anchor * 0.0f + v; }  // step/mod.rs:371-373
+
+// air_kernel.rs:80-91
+static inline float clamp_speed(float v) {
+    float out = v;
+    if (out > 8.0f) out = 8.0f;
+    if (out < -8.0f) out = -8.0f;
+    return out;
+}
+
+// air_kernel.rs:99-135
+static float neighbour_average(const float *s, uint32_t i, uint32_t x, uint32_t y, uint32_t z) {
+    float sum = s[i];
+    float count = 1.0f;
+    if (x > 0) { sum += s[i - 1]; count += 1.0f; }
+    if (x + 1 < N) { sum += s[i + 1]; count += 1.0f; }
+    if (z > 0) { sum += s[i - SZ]; count += 1.0f; }
+    if (z + 1 < N) { sum += s[i + SZ]; count += 1.0f; }
+    if (y > 0) { sum += s[i - SY]; count += 1.0f; }
+    if (y + 1 < N) { sum += s[i + SY]; count += 1.0f; }
+    return sum / count;
+}
+
+// air_kernel.rs:142-176
+static float upwind_sample(const float *s, uint32_t i, float cur, int axis, uint32_t x, uint32_t y, uint32_t z) {
+    float sample = cur;
+    if (cur > 0.0f) {
+        if (axis == 0 && x > 0) sample = s[i - 1];
+        if (axis == 1 && y > 0) sample = s[i - SY];
+        if (axis == 2 && z > 0) sample = s[i - SZ];
+    } else if (cur < 0.0f) {
+        if (axis == 0 && x + 1 < N) sample = s[i + 1];
+        if (axis == 1 && y + 1 < N) sample = s[i + SY];
+        if (axis == 2 && z + 1 < N) sample = s[i + SZ];
+    }
+    return sample;
+}
+
+// gravity.rs:74-109 (voxel_mass), MASS_SCALE = 1024
+static int32_t voxel_mass(uint32_t ty, uint32_t life, int32_t tmp, float temp_k) {
+    int32_t out = 0;  // seed_i32(tmp, 0)
+    if (ty == 39u) {  // GRVT
+        const int32_t t = trunc_i32(clampf((float)tmp, -100.0f, 100.0f));
+        out = trunc_i32(0.2f * (float)t * 1024.0f);
+    } else if (ty == 40u || ty == 41u) {  // NBHL, NWHL
+        float add = seed_f32(temp_k, 0.1f);
+        if (tmp != 0) add = clampf(0.001f * (float)tmp, 0.1f, 51.2f);
+        out = ty == 40u ? trunc_i32(add * 1024.0f) : trunc_i32(-add * 1024.0f);
+    } else if (ty == 42u) {  // GBMB
+        if (life > 20u) out = trunc_i32(20.0f * 1024.0f);
+        else if (life >= 1u) out = trunc_i32(-80.0f * 1024.0f);
+    } else if (ty == 43u) {  // GPMP
+        if (life == 10u) out = trunc_i32(0.2f * (temp_k - 273.15f) * 1024.0f);
+    }
+    return out;
+}
+
+static inline uint32_t brick_cell(uint32_t brick, uint32_t slot, uint32_t *bx, uint32_t *by, uint32_t *bz) {
+    const uint32_t cx = (brick & 31u) * 2u + (slot & 1u);
+    const uint32_t cz = ((brick >> 5) & 31u) * 2u + ((slot >> 1) & 1u);
+    const uint32_t cy = ((brick >> 10) & 31u) * 2u + ((slot >> 2) & 1u);
+    *bx = cx * 4u;
+    *by = cy * 4u;
+    *bz = cz * 4u;
+    return (cy << 12) | (cz << 6) | cx;
+}
+
+}  // namespace vox
+
+extern "C" {
+
+// air_clear_kernel (air_kernel.rs:182-204)
+void ora_vox_air_clear(const tpt_vox_world *w) {
+    for (uint32_t i = 0; i < vox::CELLS; ++i) {
+        w->vx[i] = 0.0f;
+        w->vy[i] = 0.0f;
+        w->vz[i] = 0.0f;
+        w->p[i] = 0.0f;
+        w->p_tmp[i] = 0.0f;
+        w->temp[i] = 293.15f;
+        w->solid[i] = 0.0f;
+        w->pv[i] = 0;
+    }
+}
+
+// air_gather_kernel (air_kernel.rs:218-278) over the first n listed bricks.
+void ora_vox_air_gather(const tpt_vox_world *w, uint32_t n) {
+    for (uint32_t b = 0; b < n; ++b) {
+        for (uint32_t slot = 0; slot < 8u; ++slot) {
+            uint32_t bx, by, bz;
+            const uint32_t air = vox::brick_cell(w->sim_list[b], slot, &bx, &by, &bz);
+            uint32_t occupied = 0;
+            float temp_sum = 0.0f;
+            for (uint32_t ly = 0; ly < 4u; ++ly)
+                for (uint32_t lz = 0; lz < 4u; ++lz)
+                    for (uint32_t lx = 0; lx < 4u; ++lx) {
+                        const uint32_t v = w->voxel[((by + ly) << 16) | ((bz + lz) << 8) | (bx + lx)];
+                        if ((v & 0xFFu) != 0u) {
+                            occupied += 1u;
+                            temp_sum += (float)((v >> 8) & 0xFFFFu) * 0.125f;
+                        }
+                    }
+            w->solid[air] = (float)occupied * (1.0f / 64.0f);
+            w->temp[air] = occupied > 0u ? temp_sum / (float)occupied : 293.15f;
+        }
+    }
+}
+
+// AirState::solve (air.rs:162-222): air_pressure_volume_kernel
+// (air_kernel.rs:294-326), air_velocity_snapshot_kernel (:338-351),
+// `iterations` x air_pressure_jacobi_kernel (:361-398) alternating p / p_tmp,
+// then air_advect_kernel (:414-536).
+void ora_vox_air_solve(const tpt_vox_world *w, uint32_t iterations) {
+    using namespace vox;
+    for (uint32_t i = 0; i < CELLS; ++i) {
+        const uint32_t x = i & 63u, z = (i >> 6) & 63u, y = i >> 12;
+        int32_t value = w->pv[i];
+        if (x < 2u || x >= 62u || y < 2u || y >= 62u || z < 2u || z >= 62u) {
+            value = trunc_i32((float)value * 0.2f);
+        } else {
+            const float dp = (w->vx[i - 1] - w->vx[i + 1]) + (w->vy[i - SY] - w->vy[i + SY]) +
+                             (w->vz[i - SZ] - w->vz[i + SZ]);
+            const float mixed = (float)value * 0.9999f;
+            const float next = mixed + dp * 0.3f * 0.5f * 1024.0f;
+            if (next > 262144.0f) value = 262144;
+            else if (next < -262144.0f) value = -262144;
+            else value = trunc_i32(next);
+        }
+        w->pv[i] = value;
+    }
+    std::vector<float> snap(3 * (size_t)CELLS);
+    for (uint32_t i = 0; i < CELLS; ++i) {
+        snap[i] = w->vx[i];
+        snap[CELLS + i] = w->vy[i];
+        snap[2 * CELLS + i] = w->vz[i];
+    }
+    float *pin = w->p, *pout = w->p_tmp;
+    for (uint32_t it = 0; it < iterations; ++it) {
+        for (uint32_t i = 0; i < CELLS; ++i) {
+            const uint32_t x = i & 63u, z = (i >> 6) & 63u, y = i >> 12;
+            const bool boundary = x == 0u || y == 0u || z == 0u || x == 63u || y == 63u || z == 63u;
+            if (boundary || w->solid[i] > 0.5f) {
+                pout[i] = 0.0f;
+            } else {
+                const float divergence = 0.5f * ((w->vx[i + 1] - w->vx[i - 1]) + (w->vy[i + SY] - w->vy[i - SY]) +
+                                                 (w->vz[i + SZ] - w->vz[i - SZ]));
+                const float nb = pin[i - 1] + pin[i + 1] + pin[i - SZ] + pin[i + SZ] + pin[i - SY] + pin[i + SY];
+                pout[i] = (nb - divergence) / 6.0f;
+            }
+        }
+        std::swap(pin, pout);
+    }
+    const float *pr = pin, *sx = snap.data(), *sy = snap.data() + CELLS, *sz = snap.data() + 2 * (size_t)CELLS;
+    for (uint32_t i = 0; i < CELLS; ++i) {
+        if (w->solid[i] > 0.5f) {
+            w->vx[i] = 0.0f;
+            w->vy[i] = 0.0f;
+            w->vz[i] = 0.0f;
+            continue;
+        }
+        const uint32_t x = i & 63u, z = (i >> 6) & 63u, y = i >> 12;
+        const float local_temp = neighbour_average(w->temp, i, x, y, z);
+        const uint32_t lx = x > 0 ? i - 1 : i, ux = x + 1 < N ? i + 1 : i;
+        const uint32_t lz = z > 0 ? i - SZ : i, uz = z + 1 < N ? i + SZ : i;
+        const uint32_t ly = y > 0 ? i - SY : i, uy = y + 1 < N ? i + SY : i;
+        const float gx = (pr[ux] - pr[lx]) * 0.5f, gy = (pr[uy] - pr[ly]) * 0.5f, gz = (pr[uz] - pr[lz]) * 0.5f;
+        const float ox = sx[i], oy = sy[i], oz = sz[i];
+        const float buoyancy = (local_temp - 293.15f) * 0.02f;
+        float nx = (ox - gx) * 0.99f, ny = (oy + buoyancy - gy) * 0.99f, nz = (oz - gz) * 0.99f;
+        const float keep_n = 1.0f - 0.1f, keep_u = 1.0f - 0.25f;
+        nx = nx * keep_n + neighbour_average(sx, i, x, y, z) * 0.1f;
+        ny = ny * keep_n + neighbour_average(sy, i, x, y, z) * 0.1f;
+        nz = nz * keep_n + neighbour_average(sz, i, x, y, z) * 0.1f;
+        nx = nx * keep_u + upwind_sample(sx, i, ox, 0, x, y, z) * 0.25f;
+        ny = ny * keep_u + upwind_sample(sy, i, oy, 1, x, y, z) * 0.25f;
+        nz = nz * keep_u + upwind_sample(sz, i, oz, 2, x, y, z) * 0.25f;
+        w->vx[i] = clamp_speed(nx);
+        w->vy[i] = clamp_speed(ny);
+        w->vz[i] = clamp_speed(nz);
+    }
+}
+
+// gravity::solve (gravity.rs:228-260): `iterations` (24 in the reference)
+// gravity_jacobi_kernel sweeps (:170-196) with the potential handles swapped
+// after each, then gravity_force_kernel (:199-224). On return grav_potential
+// names the last sweep, as the swapped handles do.
+void ora_vox_grav_solve(const tpt_vox_world *w, uint32_t iterations) {
+    using namespace vox;
+    float *uin = w->grav_potential, *uout = w->grav_potential_tmp;
+    for (uint32_t it = 0; it < iterations; ++it) {
+        for (uint32_t i = 0; i < CELLS; ++i) {
+            const uint32_t x = i & 63u, z = (i >> 6) & 63u, y = (i >> 12) & 63u;
+            const bool boundary = x == 0u || x == 63u || y == 0u || y == 63u || z == 0u || z == 63u;
+            float out = seed_f32(uin[i], 0.0f);
+            if (!boundary) {
+                const float sum = uin[i - 1] + uin[i + 1] + uin[i - SZ] + uin[i + SZ] + uin[i - SY] + uin[i + SY];
+                const float rho = (float)w->grav_mass[i] * (1.0f / 1024.0f);
+                out = (sum - 8.385539f * rho) * (1.0f / 6.0f);
+            }
+            uout[i] = out;
+        }
+        std::swap(uin, uout);
+    }
+    if (uin != w->grav_potential) {  // odd sweep count: give the names their swapped contents
+        std::vector<float> t(uin, uin + CELLS);
+        std::memcpy(w->grav_potential_tmp, w->grav_potential, CELLS * sizeof(float));
+        std::memcpy(w->grav_potential, t.data(), CELLS * sizeof(float));
+    }
+    const float *u = w->grav_potential;
+    for (uint32_t i = 0; i < CELLS; ++i) {
+        const uint32_t x = i & 63u, z = (i >> 6) & 63u, y = (i >> 12) & 63u;
+        const bool boundary = x == 0u || x == 63u || y == 0u || y == 63u || z == 0u || z == 63u;
+        float fx = seed_f32(u[i], 0.0f), fy = seed_f32(u[i], 0.0f), fz = seed_f32(u[i], 0.0f);
+        if (!boundary) {
+            fx = (u[i - 1] - u[i + 1]) * 0.5f;
+            fz = (u[i - SZ] - u[i + SZ]) * 0.5f;
+            fy = (u[i - SY] - u[i + SY]) * 0.5f;
+        }
+        w->grav_force_x[i] = fx;
+        w->grav_force_y[i] = fy;
+        w->grav_force_z[i] = fz;
+    }
+}
+
+// gravity_clear_kernel (gravity.rs:112-118)
+void ora_vox_grav_clear_mass(const tpt_vox_world *w) {
+    std::memset(w->grav_mass, 0, vox::CELLS * sizeof(int32_t));
+}
+
+// gravity_gather_kernel (gravity.rs:125-166) over the first n listed bricks;
+// the i32 accumulator and the atomic add wrap.
+void ora_vox_grav_gather(const tpt_vox_world *w, uint32_t n) {
+    for (uint32_t b = 0; b < n; ++b) {
+        for (uint32_t slot = 0; slot < 8u; ++slot) {
+            uint32_t bx, by, bz;
+            const uint32_t cell = vox::brick_cell(w->sim_list[b], slot, &bx, &by, &bz);
+            uint32_t acc = 0;
+            for (uint32_t ly = 0; ly < 4u; ++ly)
+                for (uint32_t lz = 0; lz < 4u; ++lz)
+                    for (uint32_t lx = 0; lx < 4u; ++lx) {
+                        const uint32_t index = ((by + ly) << 16) | ((bz + lz) << 8) | (bx + lx);
+                        const uint32_t word = w->voxel[index];
+                        const uint32_t ty = word & 0xFFu;
+                        if (ty != 0u) {
+                            const uint32_t life = (word >> 24) & 0xFFu;
+                            const float temp_k = (float)((word >> 8) & 0xFFFFu) * 0.125f;
+                            acc += (uint32_t)vox::voxel_mass(ty, life, w->aux_tmp[index], temp_k);
+                        }
+                    }
+            w->grav_mass[cell] = (int32_t)((uint32_t)w->grav_mass[cell] + acc);
+        }
+    }
+}
+
+}  // extern "C"

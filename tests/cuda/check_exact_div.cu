@@ -26,9 +26,15 @@ __global__ void check(float c, float rc, unsigned long long *bad, uint32_t *firs
 }
 
 int main() {
-    const float cs[3][2] = {{tpt::kSmoothWsum, tpt::kSmoothWsumRcp},
+    // The 2-D air divisors, then the 3-D field step's: the six-neighbour
+    // counts 4..7 of its averages and the 6 of its pressure sweep.
+    const float cs[7][2] = {{tpt::kSmoothWsum, tpt::kSmoothWsumRcp},
                             {tpt::kConvLegacy, tpt::kConvLegacyRcp},
-                            {tpt::kConvBouss, tpt::kConvBoussRcp}};
+                            {tpt::kConvBouss, tpt::kConvBoussRcp},
+                            {4.0f, 1.0f / 4.0f},
+                            {5.0f, 1.0f / 5.0f},
+                            {6.0f, 1.0f / 6.0f},
+                            {7.0f, 1.0f / 7.0f}};
     unsigned long long *bad;
     uint32_t *first, *maxmag;
     if (cudaMalloc(&bad, sizeof(*bad)) != cudaSuccess || cudaMalloc(&first, sizeof(*first)) != cudaSuccess ||

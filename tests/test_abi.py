@@ -55,6 +55,19 @@ def test_arguments_are_validated_before_any_device_work(tf):
     assert lib.tpt_grav_step(None, None, None, None) == -2
     assert lib.tpt_batch_step(None, 1, None) == -2
     assert lib.tpt_grav_plan_destroy(None) == 0 and lib.tpt_batch_destroy(None) == 0
+    # 3-D field step
+    assert lib.tpt_vox_plan_create(0, None) == -2
+    assert lib.tpt_vox_plan_create(9, ctypes.byref(h)) == -5
+    w = tf.VoxWorld()
+    assert lib.tpt_vox_air_clear(None, None) == -2
+    assert lib.tpt_vox_air_clear(ctypes.byref(w), None) == -2
+    assert lib.tpt_vox_air_gather(None, ctypes.byref(w), None) == -2
+    assert lib.tpt_vox_air_solve(None, ctypes.byref(w), 12, None) == -2
+    assert lib.tpt_vox_grav_solve(None, ctypes.byref(w), None) == -2
+    assert lib.tpt_vox_grav_clear_mass(None, ctypes.byref(w), None) == -2
+    assert lib.tpt_vox_grav_gather(None, ctypes.byref(w), None) == -2
+    assert lib.tpt_vox_field_step(None, ctypes.byref(w), 1, 12, None) == -2
+    assert lib.tpt_vox_plan_form(None) == -2 and lib.tpt_vox_plan_destroy(None) == 0
 
 
 def test_default_params_match_reference(tf):

@@ -1,5 +1,6 @@
 """The library divides by its constants (the smoothing weights' sum, the two
-convection scales) with a multiply and two fused multiply-adds instead of a
+convection scales, and in the 3-D field step the neighbour counts 4..7 and
+the pressure sweep's 6) with a multiply and two fused multiply-adds instead of a
 division (csrc/exact_div.cuh). This checks, for each of those divisors and
 every one of the 2^32 f32 inputs, that the result is bit-identical to IEEE
 division on the device (tests/cuda/check_exact_div.cu, built here with nvcc
@@ -22,6 +23,6 @@ def test_division_by_constants_is_exact_for_every_input(cuda, tmp_path):
                     os.path.join(HERE, "cuda", "check_exact_div.cu"), "-o", exe], check=True)
     out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split("\n")
     rows = [line.split() for line in out if line.strip()]
-    assert len(rows) == 3
+    assert len(rows) == 7
     for divisor, mismatches, first, largest in rows:
         assert int(mismatches) == 0, (divisor, mismatches, first, largest)

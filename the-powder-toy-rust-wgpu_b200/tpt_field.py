@@ -47,9 +47,12 @@ EXPORTS = [
     "tpt_grav_plan_destroy", "tpt_grav_plan_dims", "tpt_grav_solve", "tpt_grav_solve_f32",
     "tpt_grav_mask_rebuild", "tpt_mass_to_fixed", "tpt_grav_step", "tpt_batch_create", "tpt_batch_destroy", "tpt_batch_fields",
     "tpt_batch_write", "tpt_batch_read", "tpt_batch_step", "tpt_batch_tune", "tpt_batch_get_tuning",
-    "tpt_batch_set_tuning", "tpt_batch_profile_phases", "tpt_check_device_errors", "tpt_last_error_string",
-    "tpt_kernel_launch_count", "tpt_version",
+    "tpt_batch_set_tuning", "tpt_batch_profile_phases", "tpt_vox_plan_create", "tpt_vox_plan_destroy",
+    "tpt_vox_plan_form", "tpt_vox_air_clear", "tpt_vox_air_gather", "tpt_vox_air_solve", "tpt_vox_grav_solve",
+    "tpt_vox_grav_clear_mass", "tpt_vox_grav_gather", "tpt_vox_field_step", "tpt_check_device_errors",
+    "tpt_last_error_string", "tpt_kernel_launch_count", "tpt_version",
 ]
+VOX_AUTO, VOX_CLUSTER, VOX_PER_SWEEP = 0, 1, 2
 
 
 class TptError(RuntimeError):
@@ -118,6 +121,14 @@ class BatchTuning(ctypes.Structure):
 _lib = None
 
 
+class VoxWorld(ctypes.Structure):
+    """tpt_vox_world: one 3-D world's device buffers."""
+
+    _fields_ = [(n, ctypes.c_void_p) for n in (
+        "voxel", "aux_tmp", "sim_list", "sim_count", "vx", "vy", "vz", "p", "p_tmp", "temp", "solid", "pv",
+        "grav_mass", "grav_potential", "grav_potential_tmp", "grav_force_x", "grav_force_y", "grav_force_z")]
+
+
 def build() -> None:
     """Compiles libtpt_field.so for sm_100a (nvcc cross-compiles without a GPU)."""
     subprocess.run(["make", "-s", "-j8", "-C", HERE], check=True)
@@ -155,6 +166,17 @@ def lib() -> ctypes.CDLL:
         L.tpt_batch_get_tuning.argtypes = [P, ctypes.POINTER(BatchTuning)]
         L.tpt_batch_set_tuning.argtypes = [P, ctypes.POINTER(BatchTuning)]
         L.tpt_batch_profile_phases.argtypes = [P, u32, P, ctypes.POINTER(BatchProfile)]
+        W = ctypes.POINTER(VoxWorld)
+        L.tpt_vox_plan_create.argtypes = [i32, ctypes.POINTER(P)]
+        L.tpt_vox_plan_destroy.argtypes = [P]
+        L.tpt_vox_plan_form.argtypes = [P]
+        L.tpt_vox_air_clear.argtypes = [W, P]
+        L.tpt_vox_air_gather.argtypes = [P, W, P]
+        L.tpt_vox_air_solve.argtypes = [P, W, u32, P]
+        L.tpt_vox_grav_solve.argtypes = [P, W, P]
+        L.tpt_vox_grav_clear_mass.argtypes = [P, W, P]
+        L.tpt_vox_grav_gather.argtypes = [P, W, P]
+        L.tpt_vox_field_step.argtypes = [P, W, u32, u32, P]
         L.tpt_last_error_string.restype = ctypes.c_char_p
         L.tpt_kernel_launch_count.restype = ctypes.c_uint64
         L.tpt_version.restype = ctypes.c_char_p

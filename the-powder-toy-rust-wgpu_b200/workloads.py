@@ -419,3 +419,82 @@ def gravity_state(xres: int, yres: int, seed: int) -> dict:
             "mass_prev": (st.u64(cells) % np.uint64(70000)).astype(np.int32),
             "tool_mass": tool, "override_mass": ovr.astype(np.int32), "override_set": ovr_set,
             "gx": np.zeros(cells, np.float32), "gy": np.zeros(cells, np.float32)}
+
+
+# ---------------------------------------------------------------- 3-D ----
+# The 3-D sandbox (crates/tpt-sim/src/voxel3d): a 64^3 coarse grid
+# ((y << 12) | (z << 6) | x) over 256^3 voxels ((y << 16) | (z << 8) | x) in
+# 8^3 bricks ((by << 10) | (bz << 5) | bx).
+VOX_AXIS = 64
+VOX_CELLS = 64 ** 3
+VOX_VOXELS = 256 ** 3
+VOX_BRICKS = 32 ** 3
+
+
+def voxel_world(seed: int, active: float = 0.3, fill: float = 0.4) -> dict:
+    """A seeded 3-D world for the field step, numpy arrays in the reference
+    layout and types:
+
+      voxel     u32 words ty | temp_q << 8 | life << 24 (step/mod.rs:125-133):
+                empty voxels (ty 0) with probability 1 - fill, else one of
+                the gravity elements GRVT..GPMP or another element id;
+                temp_q over the whole u16 range, life over u8 with 10 (the
+                GPMP trigger) and the GBMB thresholds frequent
+      aux_tmp   i32 per voxel: 0, inside and far outside the clamps
+      sim_list  `active` of the 32768 brick ids, in random order (the order
+                the device compaction's atomics give); sim_count [n, 1, 1]
+      vx vy vz  f32 in [-8, 8] (the advection clamp), some exact zeros
+      p p_tmp   f32 pressure pair, temp f32 250..600 K, solid k/64
+      pv        i32 in the +-262144 clamp, a few at the limits
+      grav_*    i32 mass on 2% of cells, f32 potential pair, stale forces
+    """
+    st = Stream(seed)
+    nv = VOX_VOXELS
+    kinds = np.array([1, 5, 27, PT_GRVT, PT_NBHL, PT_NWHL, PT_GBMB, PT_GPMP, 100, 255], np.uint32)
+    ty = kinds[(st.u64(nv) % np.uint64(len(kinds))).astype(np.int64)]
+    ty[st.uniform(0.0, 1.0, nv) >= fill] = 0
+    temp_q = (st.u64(nv) & np.uint64(0xFFFF)).astype(np.uint32)
+    warm = (st.u64(nv) % np.uint64(3)) == 0
+    temp_q[warm] = (2345 + (st.u64(int(warm.sum())) % np.uint64(800))).astype(np.uint32)
+    life = (st.u64(nv) & np.uint64(0xFF)).astype(np.uint32)
+    r = st.u64(nv) % np.uint64(6)
+    life[r == 0] = 10
+    life[r == 1] = 0
+    life[r == 2] = (st.u64(int((r == 2).sum())) % np.uint64(25)).astype(np.uint32)
+    voxel = ty | (temp_q << np.uint32(8)) | (life << np.uint32(24))
+    aux = (st.u64(nv) % np.uint64(120001)).astype(np.int64) - 60000
+    r = st.u64(nv) % np.uint64(4)
+    aux[r == 0] = 0
+    aux[r == 1] = aux[r == 1] % 201 - 100
+    n_active = int(round(active * VOX_BRICKS))
+    sim_list = st.choice_cells(VOX_BRICKS, n_active).astype(np.uint32)
+
+    nc = VOX_CELLS
+    v = [st.uniform(-8.0, 8.0, nc).astype(np.float32) for _ in range(3)]
+    for a in v:
+        a[(st.u64(nc) % np.uint64(10)) == 0] = 0.0
+    solid = ((st.u64(nc) % np.uint64(65)).astype(np.float32) * np.float32(1.0 / 64.0)).astype(np.float32)
+    solid[(st.u64(nc) % np.uint64(3)) != 0] = 0.0
+    pv = (st.u64(nc) % np.uint64(524289)).astype(np.int64) - 262144
+    r = st.u64(nc) % np.uint64(50)
+    pv[r == 0] = 262144
+    pv[r == 1] = -262144
+    mass = np.zeros(nc, np.int64)
+    hot = st.choice_cells(nc, nc // 50)
+    mass[hot] = (st.u64(len(hot)) % np.uint64(200001)).astype(np.int64) - 100000
+    return {
+        "voxel": voxel.astype(np.uint32), "aux_tmp": aux.astype(np.int32), "sim_list": sim_list,
+        "sim_count": np.array([n_active, 1, 1], np.uint32),
+        "vx": v[0], "vy": v[1], "vz": v[2],
+        "p": st.uniform(-2.0, 2.0, nc).astype(np.float32), "p_tmp": st.uniform(-2.0, 2.0, nc).astype(np.float32),
+        "temp": st.uniform(250.0, 600.0, nc).astype(np.float32), "solid": solid, "pv": pv.astype(np.int32),
+        "grav_mass": mass.astype(np.int32),
+        "grav_potential": st.uniform(-50.0, 50.0, nc).astype(np.float32),
+        "grav_potential_tmp": st.uniform(-50.0, 50.0, nc).astype(np.float32),
+        "grav_force_x": np.full(nc, 7.0, np.float32), "grav_force_y": np.full(nc, 7.0, np.float32),
+        "grav_force_z": np.full(nc, 7.0, np.float32),
+    }
+
+
+VOX_FIELDS = ("voxel", "aux_tmp", "sim_list", "sim_count", "vx", "vy", "vz", "p", "p_tmp", "temp", "solid", "pv",
+              "grav_mass", "grav_potential", "grav_potential_tmp", "grav_force_x", "grav_force_y", "grav_force_z")
