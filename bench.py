@@ -3,6 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload c1|c2|c4|c5] [--ticks T]
+    python bench.py --voxel3d [--worlds W] ...   (the 3-D sandbox's field step)
 
 Metric: cell-ticks/s = sum over instances of xcells*ycells * ticks / time;
 one tick is one air step plus one gravity solve of every instance (the
@@ -373,6 +374,205 @@ def run_ours(args, rank, world, local):
     batch.close()
 
 
+# -------------------------------------------------------------- 3-D ----
+VOX_NAME = ("3-D sandbox field step, 64^3 cells per world over 256^3 voxels with every brick active: air gather, "
+            "air solve (12 Jacobi sweeps), gravity solve (24 sweeps), clear mass, gravity gather")
+
+
+def _vox_cpu_rate(host: dict, target_s: float):
+    """The oracle's 3-D tick (single-threaded C++) on one world; returns
+    (cell-ticks/s, cores, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    d = {k: v.copy() for k, v in host.items()}
+
+    def tick():
+        O.vox_field_step(d, 12)
+        O.vox_grav_gather(d)
+
+    t0 = time.perf_counter()
+    tick()
+    t1 = time.perf_counter() - t0
+    n = max(1, min(50, int(target_s / max(t1, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(n):
+        tick()
+    dt = time.perf_counter() - t0
+    return 262144 * n / dt, 1, f"1 world x {n} ticks, oracle restatement of the five passes"
+
+
+def run_voxel3d(args, rank, world, local):
+    """The 3-D field step (tpt_vox_field_step + tpt_vox_grav_gather per tick),
+    `--worlds` worlds per rank, ticks captured in one CUDA graph per step.
+    Metric: cell-ticks/s over the 64^3 coarse cells of every world."""
+    import torch
+
+    import tpt_field as tf
+    import voxel3d as V
+    import workloads as W
+
+    tf.lib()
+    host = W.voxel_world(0x3D00, active=1.0)
+    nw = args.worlds
+    ticks = args.ticks or 100
+    stream = torch.cuda.Stream()
+    plans = {"cluster": V.Plan(tf.VOX_CLUSTER), "per_sweep": V.Plan(tf.VOX_PER_SWEEP)}
+    devs = [V.upload(host) for _ in range(nw)]
+    nonempty = int(np.count_nonzero(host["voxel"] & 0xFF))
+
+    def tick(plan):
+        V.field_step(plan, devs, 12, stream)
+        for b, _ in devs:
+            V.gravity_gather(plan, b, stream)
+
+    def graph_of(fn, n):
+        with torch.cuda.stream(stream):
+            for _ in range(2):
+                fn()
+        stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            for _ in range(n):
+                fn()
+        return g
+
+    def time_graph(g, reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(reps):
+                g.replay()
+            e1.record(stream)
+        stream.synchronize()
+        return e0.elapsed_time(e1)
+
+    L0 = tf.launch_count()
+    g_tick = graph_of(lambda: tick(plans["cluster"]), ticks)
+    launches_per_tick = (tf.launch_count() - L0) / (ticks + 2)  # two warm-up ticks, then the captured ones
+    for _ in range(args.warmup):
+        g_tick.replay()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = time_graph(g_tick, args.steps)
+    clk = clocks.stop()
+    barrier(world)
+    ms = max_over_ranks(ms, world)
+    value = 262144 * nw * world * ticks * args.steps / (ms / 1e3)
+
+    # phases, each alone in a graph of `ticks` launches (device time per launch)
+    reps = 3
+    phase = {}
+    g = graph_of(lambda: [V.AirState.gather(a, plans["cluster"], b, stream) for b, a in devs], ticks)
+    phase["air_gather"] = time_graph(g, reps) / (reps * ticks * nw)
+    g = graph_of(lambda: [V.gravity_gather(plans["cluster"], b, stream) for b, _ in devs], ticks)
+    phase["grav_gather"] = time_graph(g, reps) / (reps * ticks * nw)
+    g = graph_of(lambda: V.field_step(plans["cluster"], devs, 12, stream), ticks)
+    phase["field_step"] = time_graph(g, reps) / (reps * ticks)
+    phase["cluster_solve"] = phase["field_step"] - phase["air_gather"] * nw  # one launch, every world
+    g = graph_of(lambda: tick(plans["per_sweep"]), ticks)
+    per_sweep_ms = time_graph(g, reps) / (reps * ticks)
+    g = graph_of(lambda: V.field_step(plans["per_sweep"], devs, 12, stream), ticks)
+    per_sweep_solve = time_graph(g, reps) / (reps * ticks) - phase["air_gather"] * nw
+    del g
+
+    # end to end: host buffers in, ticks, fields out, through the public calls
+    in_keys = ("voxel", "aux_tmp", "vx", "vy", "vz", "p", "p_tmp", "temp", "solid", "pv", "grav_mass",
+               "grav_potential", "grav_potential_tmp")
+    out_keys = ("vx", "vy", "vz", "p", "pv", "grav_force_x", "grav_force_y", "grav_force_z")
+
+    def pinned(a):
+        t = torch.empty(a.size, dtype=torch.int32 if a.dtype != np.float32 else torch.float32, pin_memory=True)
+        t.numpy().view(a.dtype)[:] = a
+        return t
+
+    h_in = {k: pinned(host[k]) for k in in_keys}
+    h_out = [{k: torch.empty(262144, dtype=torch.int32 if k == "pv" else torch.float32, pin_memory=True)
+              for k in out_keys} for _ in range(nw)]
+
+    def dev_of(b, a, k):
+        if k == "voxel":
+            return b.voxel_a
+        if k == "temp":
+            return a.t
+        return getattr(b, k) if hasattr(b, k) else getattr(a, k)
+
+    def e2e_step():
+        with torch.cuda.stream(stream):
+            for b, a in devs:
+                for k, t in h_in.items():
+                    dev_of(b, a, k).copy_(t.view(dev_of(b, a, k).dtype), non_blocking=True)
+            g_tick.replay()
+            for (b, a), o in zip(devs, h_out):
+                for k, t in o.items():
+                    t.copy_(dev_of(b, a, k), non_blocking=True)
+
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
+    e2e_value = None
+    if e2e_steps:
+        e2e_step()
+        stream.synchronize()
+        barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(e2e_steps):
+                e2e_step()
+            e1.record(stream)
+        stream.synchronize()
+        barrier(world)
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        e2e_value = 262144 * nw * world * ticks * e2e_steps / (e2e_ms / 1e3)
+    h2d = sum(t.numel() * 4 for t in h_in.values()) * nw
+    d2h = sum(t.numel() * 4 for o in h_out for t in o.values())
+
+    hbm, bf16, bf16s, peak_src = load_peaks()
+    # algorithmic DRAM bytes of the gathers with every brick listed: the
+    # voxel words, the tmp words of the non-empty voxels, and the cell words
+    # written (air: solid + temp; gravity: read-modify-write of the mass)
+    b_air = 4 * W.VOX_VOXELS + 8 * W.VOX_CELLS
+    b_grav = 4 * W.VOX_VOXELS + 4 * nonempty + 8 * W.VOX_CELLS
+    gbs_air = b_air / (phase["air_gather"] / 1e3) / 1e9
+    gbs_grav = b_grav / (phase["grav_gather"] / 1e3) / 1e9
+    roof_grav = {"kernel": "k_grav_gather", "bound": "hbm", "achieved": round(gbs_grav, 1), "peak": hbm,
+                 "unit": "GB/s", "frac": round(gbs_grav / hbm, 4), "peak_source": peak_src,
+                 "algorithmic_bytes_per_launch": b_grav, "avg_launch_ms": round(phase["grav_gather"], 5),
+                 "traffic": None}
+    roof_air = {"kernel": "k_air_gather", "bound": "hbm", "achieved": round(gbs_air, 1), "peak": hbm,
+                "unit": "GB/s", "frac": round(gbs_air / hbm, 4), "peak_source": peak_src,
+                "algorithmic_bytes_per_launch": b_air, "avg_launch_ms": round(phase["air_gather"], 5),
+                "traffic": None}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, desc = _vox_cpu_rate(host, args.cpu_seconds)
+        cpu = {"value": rate, "unit": "cell-ticks/s", "cores": cores, "kind": "port", "sample": desc}
+    if rank == 0:
+        line = {
+            "metric": "cell-ticks/s", "value": value, "unit": "cell-ticks/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (i32 mass, pv)",
+            "data": "synthetic (seeded 3-D world, workloads.voxel_world)",
+            "config": {"workload": VOX_NAME, "worlds": nw, "ticks_per_step": ticks,
+                       "l2": "gather inputs 128 MiB per world > 126 MB L2, no flush", "form": "cluster"},
+            "e2e": {"value": e2e_value, "unit": "cell-ticks/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+            "gpu_launches": round(launches_per_tick * ticks * args.steps),
+            "roofline": roof_grav if phase["grav_gather"] >= phase["air_gather"] else roof_air,
+            "roofline_phases": {"air_gather": roof_air, "grav_gather": roof_grav},
+            "ms_per_world_tick": {k: round(v, 5) for k, v in phase.items()},
+            "per_sweep_form": {"ms_per_tick": round(per_sweep_ms, 5), "solve_ms_per_tick": round(per_sweep_solve, 5),
+                               "speedup_of_cluster_tick": round(per_sweep_ms / (ms / args.steps / ticks), 3)},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    for p in plans.values():
+        p.close()
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -396,6 +596,29 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_reference_voxel3d(args, rank, world):
+    if rank != 0:
+        return
+    import workloads as W
+
+    host = W.voxel_world(0x3D00, active=1.0)
+    rates = []
+    cores = desc = None
+    for _ in range(args.warmup + args.steps):
+        rate, cores, desc = _vox_cpu_rate(host, args.cpu_seconds / max(args.steps, 1))
+        rates.append(rate)
+    value = statistics.median(rates[args.warmup:])
+    line = {
+        "impl": "reference", "metric": "cell-ticks/s", "value": value, "unit": "cell-ticks/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (i32 mass, pv)", "data": "synthetic (seeded 3-D world, workloads.voxel_world)",
+        "config": {"workload": VOX_NAME, "worlds": 1},
+        "cpu_baseline": {"value": value, "unit": "cell-ticks/s", "cores": cores, "kind": "port", "sample": desc},
+        "e2e": {"value": value, "unit": "cell-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -411,17 +634,25 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer run (profiling captures)")
     ap.add_argument("--phase-ticks", type=int, default=200, help="even tick count of the per-phase timing")
+    ap.add_argument("--voxel3d", action="store_true", help="the 3-D sandbox's field step instead of the 2-D one")
+    ap.add_argument("--worlds", type=int, default=1, help="3-D worlds per rank (--voxel3d)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         world = int(os.environ.get("WORLD_SIZE", "1"))
-        run_reference(args, rank, world)
+        if args.voxel3d:
+            run_reference_voxel3d(args, rank, world)
+        else:
+            run_reference(args, rank, world)
         return
     rank, world, local = dist_setup(args.gpus)
     try:
-        run_ours(args, rank, world, local)
+        if args.voxel3d:
+            run_voxel3d(args, rank, world, local)
+        else:
+            run_ours(args, rank, world, local)
     finally:
         if world > 1:
             import torch.distributed as dist
