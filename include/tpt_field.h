@@ -395,11 +395,15 @@ enum {
 
 /* How a plan runs the Jacobi solves. */
 enum {
-    TPT_VOX_AUTO = 0,      /* the cluster form when the device can schedule it */
+    TPT_VOX_AUTO = 0,      /* TPT_VOX_BATCHED                                */
     TPT_VOX_CLUSTER = 1,   /* one 16-CTA cluster per field, the whole grid in
-                              distributed shared memory, one launch per step */
-    TPT_VOX_PER_SWEEP = 2  /* one launch per pass and per sweep, the
-                              reference's launch structure                  */
+                              distributed shared memory, one launch for every
+                              world's sweeps                                 */
+    TPT_VOX_PER_SWEEP = 2, /* one launch per pass and per sweep and world,
+                              the reference's launch structure               */
+    TPT_VOX_BATCHED = 3    /* one launch per sweep index for every world of
+                              a call, air and gravity in the same launch,
+                              programmatic dependent launches                */
 };
 
 /*
@@ -427,11 +431,11 @@ typedef struct tpt_vox_world {
 typedef struct tpt_vox_plan tpt_vox_plan;
 
 /*
- * Creates a plan running the solves in `form` (TPT_VOX_*). AUTO picks the
- * cluster form when the device can hold a 16-CTA cluster of the kernel and
- * the per-sweep form otherwise; CLUSTER fails with TPT_ERR_UNSUPPORTED
- * then. The plan owns the per-sweep form's scratch (the reference's
- * velocity snapshot, air.rs:78-79); no entry point below allocates.
+ * Creates a plan running the solves in `form` (TPT_VOX_*). CLUSTER fails
+ * with TPT_ERR_UNSUPPORTED where the device cannot hold a 16-CTA cluster of
+ * its kernel. The plan owns the forms' scratch (the reference's velocity
+ * snapshot, air.rs:78-79, and the batched form's per-world source fields,
+ * about 5 MiB per world for 16 worlds); no entry point below allocates.
  */
 int tpt_vox_plan_create(int form, tpt_vox_plan **out);
 int tpt_vox_plan_destroy(tpt_vox_plan *plan);

@@ -1,6 +1,7 @@
 """GPU 3-D field step (crates/tpt-sim/src/voxel3d) against the oracle's
-restatement of its kernels, bit-exact, on seeded 64^3 worlds, in both forms
-of the solve (the cluster launch and the reference's per-sweep launches):
+restatement of its kernels, bit-exact, on seeded 64^3 worlds, in the three forms
+of the solve (batched launches per sweep index, the cluster launch, and the
+reference's per-pass, per-sweep launches):
 
   air gather       solid and temp of the listed bricks' cells; the other
                    cells keep their values; empty and full brick lists
@@ -15,7 +16,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-FORMS = {"cluster": 1, "per_sweep": 2}
+FORMS = {"cluster": 1, "per_sweep": 2, "batched": 3}
 AIR_KEYS = ("pv", "p", "p_tmp", "vx", "vy", "vz")
 GRAV_KEYS = ("grav_potential", "grav_potential_tmp", "grav_force_x", "grav_force_y", "grav_force_z", "grav_mass")
 
@@ -47,10 +48,10 @@ def plans(tf, cuda):
     return {name: V.Plan(form) for name, form in FORMS.items()}
 
 
-def test_auto_plan_takes_the_cluster_form(tf, cuda):
+def test_auto_plan_takes_the_batched_form(tf, cuda):
     import voxel3d as V
 
-    assert V.Plan(tf.VOX_AUTO).form == tf.VOX_CLUSTER
+    assert V.Plan(tf.VOX_AUTO).form == tf.VOX_BATCHED
 
 
 @pytest.mark.parametrize("active", [0.0, 0.3, 1.0])

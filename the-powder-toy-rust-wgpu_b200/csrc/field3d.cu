@@ -26,18 +26,14 @@
 // kernels' order, so results are bit-identical to the reference arithmetic.
 #include <cooperative_groups.h>
 
-#include "common.cuh"
-#include "exact_div.cuh"
 #include "field3d.hpp"
+#include "field3d_cell.cuh"
 
 namespace cg = cooperative_groups;
 
 namespace tpt {
 namespace vox {
 
-constexpr int N = 64;
-constexpr int SZ = 64, SY = 4096;
-constexpr int CELLS = N * N * N;
 constexpr int CL = 16;            // CTAs per cluster
 constexpr int PL = N / CL;        // y planes per CTA
 constexpr int ROWS = 2;           // z rows per thread
@@ -47,161 +43,13 @@ constexpr int SLAB = PL * PLANE;  // floats per CTA slab
 constexpr size_t CLUSTER_SMEM = 3 * SLAB * sizeof(float);
 static_assert(ROWS * PL * 4 <= 32, "a thread's cells fit one 32-bit mask");
 
-// air_kernel.rs:55-71, 328-331
-constexpr float kAmbient = 293.15f;
-constexpr float kBuoyancy = 0.02f;
-constexpr float kDamping = 0.99f;
-constexpr float kNbrW = 0.1f, kKeepNbr = 1.0f - kNbrW;
-constexpr float kUpW = 0.25f, kKeepUp = 1.0f - kUpW;
-constexpr float kMaxSpeed = 8.0f;
-constexpr float kPvScale = 1024.0f;
-constexpr float kMaxPvQ = 256.0f * 1024.0f;
-// gravity.rs:55-59, 192
-constexpr float kMassScaleInv = 1.0f / 1024.0f;
-constexpr float kFourPiG = 8.385539f;
-constexpr float kSixth = 1.0f / 6.0f;
-
-// ------------------------------------------------------------ per cell ----
-
-__device__ __forceinline__ float seed_f32(float anchor, float v) { return anchor * 0.0f + v; }  // step/mod.rs:371
-
-__device__ __forceinline__ float clampf(float v, float lo, float hi) {  // step/mod.rs:425-435
-    float out = v;
-    if (out < lo) out = lo;
-    if (out > hi) out = hi;
-    return out;
-}
-
-__device__ __forceinline__ float clamp_speed(float v) {  // air_kernel.rs:80-91
-    float out = v;
-    if (out > kMaxSpeed) out = kMaxSpeed;
-    if (out < -kMaxSpeed) out = -kMaxSpeed;
-    return out;
-}
-
-// sum / count for the neighbour counts 4..7 of a six-neighbour average.
-__device__ __forceinline__ float div_count(float sum, int count) {
-    if (count == 7) return div_by_const(sum, 7.0f, 1.0f / 7.0f);
-    if (count == 6) return div_by_const(sum, 6.0f, 1.0f / 6.0f);
-    if (count == 5) return div_by_const(sum, 5.0f, 1.0f / 5.0f);
-    return div_by_const(sum, 4.0f, 0.25f);
-}
-
-// The TPT pressure update of one cell (air_kernel.rs:294-326); `dp` is the
-// six-neighbour velocity difference, used only off the two-cell rim.
-__device__ __forceinline__ int32_t pv_update(int32_t value, bool rim, float dp) {
-    if (rim) return __float2int_rz((float)value * 0.2f);
-    const float mixed = (float)value * 0.9999f;
-    const float next = mixed + dp * 0.3f * 0.5f * kPvScale;
-    if (next > kMaxPvQ) return (int32_t)kMaxPvQ;
-    if (next < -kMaxPvQ) return -(int32_t)kMaxPvQ;
-    return __float2int_rz(next);
-}
-
-// One pressure Jacobi update (air_kernel.rs:382-395).
-__device__ __forceinline__ float air_sweep_cell(float xm, float xp, float zm, float zp, float ym, float yp,
-                                                float divergence, bool fixed) {
-    const float nb = xm + xp + zm + zp + ym + yp;
-    return fixed ? 0.0f : div_by_const(nb - divergence, 6.0f, kSixth);
-}
-
-// One potential Jacobi update (gravity.rs:183-194); `src` = 4*pi*G*rho.
-__device__ __forceinline__ float grav_sweep_cell(float xm, float xp, float zm, float zp, float ym, float yp,
-                                                 float src, float self, bool boundary) {
-    const float sum = xm + xp + zm + zp + ym + yp;
-    return boundary ? seed_f32(self, 0.0f) : (sum - src) * kSixth;
-}
-
-__device__ __forceinline__ float grav_source(int32_t mass) {
-    return kFourPiG * ((float)mass * kMassScaleInv);
-}
-
-// Mean of a cell and its in-world neighbours in the reference's order
-// (air_kernel.rs:99-135, 438-464).
-__device__ __forceinline__ float nb_average(float c, float xm, float xp, float zm, float zp, float ym, float yp,
-                                            int x, int y, int z) {
-    float sum = c;
-    int n = 1;
-    if (x > 0) { sum += xm; ++n; }
-    if (x + 1 < N) { sum += xp; ++n; }
-    if (z > 0) { sum += zm; ++n; }
-    if (z + 1 < N) { sum += zp; ++n; }
-    if (y > 0) { sum += ym; ++n; }
-    if (y + 1 < N) { sum += yp; ++n; }
-    return div_count(sum, n);
-}
-
-// Donor-cell sample along `axis` (air_kernel.rs:142-176): lo / hi are the
-// cell's neighbours below / above along that axis, `c` its coordinate.
-__device__ __forceinline__ float upwind(float cur, float lo, float hi, int c) {
-    float s = cur;
-    if (cur > 0.0f) {
-        if (c > 0) s = lo;
-    } else if (cur < 0.0f) {
-        if (c + 1 < N) s = hi;
-    }
-    return s;
-}
-
-// The advection update of one velocity component of one non-solid cell
-// (air_kernel.rs:492-533): `c` the old value, the six neighbours of the old
-// component, `grad` the pressure gradient along the component's axis, `buoy`
-// the buoyancy (0 except for y).
-__device__ __forceinline__ float advect_cell(float c, float xm, float xp, float zm, float zp, float ym, float yp,
-                                             int axis, float grad, float buoy, int x, int y, int z) {
-    float next = axis == 1 ? (c + buoy - grad) * kDamping : (c - grad) * kDamping;
-    const float avg = nb_average(c, xm, xp, zm, zp, ym, yp, x, y, z);
-    next = next * kKeepNbr + avg * kNbrW;
-    float up;
-    if (axis == 0) up = upwind(c, xm, xp, x);
-    else if (axis == 1) up = upwind(c, ym, yp, y);
-    else up = upwind(c, zm, zp, z);
-    next = next * kKeepUp + up * kUpW;
-    return clamp_speed(next);
-}
-
-// One-sided at the world faces, central inside (air_kernel.rs:466-494).
-__device__ __forceinline__ float pressure_grad(float lo, float hi, float self, int c) {
-    const float l = c > 0 ? lo : self, h = c + 1 < N ? hi : self;
-    return (h - l) * 0.5f;
-}
-
-// Fixed-point mass of one voxel (gravity.rs:74-109).
-__device__ __forceinline__ int32_t voxel_mass(uint32_t ty, uint32_t life, int32_t tmp, float temp_k) {
-    int32_t out = 0;
-    if (ty == 39u) {  // GRVT
-        const int32_t t = __float2int_rz(clampf((float)tmp, -100.0f, 100.0f));
-        out = __float2int_rz(0.2f * (float)t * 1024.0f);
-    } else if (ty == 40u || ty == 41u) {  // NBHL, NWHL
-        float add = seed_f32(temp_k, 0.1f);
-        if (tmp != 0) add = clampf(0.001f * (float)tmp, 0.1f, 51.2f);
-        out = ty == 40u ? __float2int_rz(add * 1024.0f) : __float2int_rz(-add * 1024.0f);
-    } else if (ty == 42u) {  // GBMB
-        if (life > 20u) out = 20480;
-        else if (life >= 1u) out = -81920;
-    } else if (ty == 43u) {  // GPMP
-        if (life == 10u) out = __float2int_rz(0.2f * (temp_k - 273.15f) * 1024.0f);
-    }
-    return out;
-}
-
-__device__ __forceinline__ float f4(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
-__device__ __forceinline__ void f4set(float4 &v, int k, float s) {
-    if (k == 0) v.x = s;
-    else if (k == 1) v.y = s;
-    else if (k == 2) v.z = s;
-    else v.w = s;
-}
-__device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
-__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
-__device__ __forceinline__ float4 zero4() { return make_float4(0.0f, 0.0f, 0.0f, 0.0f); }
-
 // ------------------------------------------------------------- gathers ----
-// One warp per listed brick. Lane l loads the 16 bytes of voxels
-// x = 4*(l & 1) .. +3 of row z = (l >> 1) & 7, y = 2j + (l >> 4) of the brick
-// in load j = 0..3, so every 32-byte sector a load touches is used whole.
-// Lane l's words lie in cell (cx, cy, cz) = (l & 1, j >> 1, (l >> 3) & 1); the
-// xor-shuffles over lane bits 1, 2 and 4 sum the eight lanes of a cell.
+// One warp per listed brick, persistent warps taking the list in order. Lane
+// l loads the 16 bytes of voxels x = 4*(l & 1) .. +3 of row z = (l >> 1) & 7,
+// y = 2j + (l >> 4) of the brick in load j = 0..3, so every 32-byte sector a
+// load touches is used whole. Lane l's words lie in cell (cx, cy, cz) =
+// (l & 1, j >> 1, (l >> 3) & 1); the xor-shuffles over lane bits 1, 2 and 4
+// sum the eight lanes of a cell.
 __device__ __forceinline__ uint32_t brick_base(uint32_t brick) {
     const uint32_t bx = brick & 31u, bz = (brick >> 5) & 31u, by = (brick >> 10) & 31u;
     return ((by * 8u) << 16) | ((bz * 8u) << 8) | (bx * 8u);
@@ -263,9 +111,12 @@ __global__ void __launch_bounds__(256) k_air_gather(const uint32_t *__restrict__
     }
 }
 
-// gravity_gather_kernel (gravity.rs:125-166): the tmp words are read only
-// for loads that hold a non-empty voxel; integer sums wrap like the
-// reference's i32 accumulator and atomic add.
+// gravity_gather_kernel (gravity.rs:125-166). Only GRVT (39) .. GPMP (43)
+// carry mass, and only GRVT, NBHL and NWHL (39..41) read tmp: a tmp word
+// group is loaded only where its voxel group holds one of those, and each
+// lane runs the mass arithmetic for its gravity voxels only (a loop over a
+// bit mask of them). Integer sums wrap like the reference's i32 accumulator
+// and atomic add.
 __global__ void __launch_bounds__(256) k_grav_gather(const uint32_t *__restrict__ voxel,
                                                      const int32_t *__restrict__ aux,
                                                      const uint32_t *__restrict__ list,
@@ -276,23 +127,46 @@ __global__ void __launch_bounds__(256) k_grav_gather(const uint32_t *__restrict_
     for (uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < n; b += nwarps) {
         const uint32_t brick = __ldg(list + b) & (TPT_VOX_BRICKS - 1u);
         const uint32_t base = brick_base(brick);
-        uint4 w[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) w[j] = __ldg(reinterpret_cast<const uint4 *>(voxel + base + lane_offset(lane, j)));
-        uint32_t acc[2] = {0u, 0u};
+        uint32_t ws[16];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const uint32_t ws[4] = {w[j].x, w[j].y, w[j].z, w[j].w};
-            if (((ws[0] | ws[1] | ws[2] | ws[3]) & 0xFFu) == 0u) continue;  // four empty voxels
-            const int4 t = __ldg(reinterpret_cast<const int4 *>(aux + base + lane_offset(lane, j)));
-            const int32_t ts[4] = {t.x, t.y, t.z, t.w};
+            const uint4 w = __ldg(reinterpret_cast<const uint4 *>(voxel + base + lane_offset(lane, j)));
+            ws[4 * j] = w.x;
+            ws[4 * j + 1] = w.y;
+            ws[4 * j + 2] = w.z;
+            ws[4 * j + 3] = w.w;
+        }
+        uint32_t gmask = 0u, tmask = 0u;  // gravity voxels; groups whose tmp is read
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const uint32_t ty = ws[k] & 0xFFu;
-                if (ty != 0u)
-                    acc[j >> 1] += (uint32_t)voxel_mass(ty, (ws[k] >> 24) & 0xFFu, ts[k],
-                                                        (float)((ws[k] >> 8) & 0xFFFFu) * 0.125f);
-            }
+        for (int v = 0; v < 16; ++v) {
+            const uint32_t e = (ws[v] & 0xFFu) - 39u;
+            gmask |= (uint32_t)(e < 5u) << v;
+            tmask |= (uint32_t)(e < 3u) << (v >> 2);
+        }
+        int32_t ts[16];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            int4 t = make_int4(0, 0, 0, 0);
+            if ((tmask >> j) & 1u) t = __ldg(reinterpret_cast<const int4 *>(aux + base + lane_offset(lane, j)));
+            ts[4 * j] = t.x;
+            ts[4 * j + 1] = t.y;
+            ts[4 * j + 2] = t.z;
+            ts[4 * j + 3] = t.w;
+        }
+        uint32_t acc[2] = {0u, 0u};
+        while (gmask) {
+            const int v = __ffs(gmask) - 1;
+            gmask &= gmask - 1u;
+            uint32_t word = 0u;
+            int32_t tmp = 0;
+#pragma unroll
+            for (int u = 0; u < 16; ++u)
+                if (u == v) {
+                    word = ws[u];
+                    tmp = ts[u];
+                }
+            acc[v >> 3] += (uint32_t)voxel_mass(word & 0xFFu, (word >> 24) & 0xFFu, tmp,
+                                                (float)((word >> 8) & 0xFFFFu) * 0.125f);
         }
 #pragma unroll
         for (int cy = 0; cy < 2; ++cy) acc[cy] = cell_sum(acc[cy]);
@@ -322,24 +196,36 @@ __global__ void __launch_bounds__(256) k_air_clear(float *vx, float *vy, float *
 }
 
 // ------------------------------------------------------- cluster form ----
-// Shared memory of a CTA: three slabs (A, B, C) of PL planes each. Buffers
-// are named by their float offset in it; a neighbouring CTA's slab is read
-// through its 32-bit shared::cluster address (mapa of this CTA's base).
+// Shared memory of a CTA: the Jacobi pair, slabs A and B of PL planes each,
+// and slab H of halo planes: the plane below and the plane above this CTA's
+// slab, for A and for B. A CTA writes its edge planes straight into its
+// neighbours' halo planes (a store to another CTA's shared memory through
+// its 32-bit shared::cluster address, mapa of the same offset), so every
+// load of a sweep is local.
 
-enum : int { SA = 0, SB = SLAB, SC = 2 * SLAB };
+enum : int { SA = 0, SB = SLAB, SH = 2 * SLAB };
+// Halo plane of buffer `buf` (SA or SB): below (0) or above (1) this slab.
+__device__ __forceinline__ int halo(int buf, int above) { return SH + (buf == SA ? 0 : 2 * PLANE) + above * PLANE; }
 
 __device__ __forceinline__ uint32_t mapa(uint32_t addr, uint32_t rank) {
     uint32_t out;
     asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(out) : "r"(addr), "r"(rank));
     return out;
 }
-__device__ __forceinline__ float4 ld4_cluster(uint32_t addr) {
-    float4 v;
-    asm volatile("ld.shared::cluster.v4.f32 {%0, %1, %2, %3}, [%4];"
-                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-                 : "r"(addr)
-                 : "memory");
-    return v;
+// A store to another CTA's shared memory. Volatile: it stays between the
+// cluster barriers around it (also volatile asm), whose release / acquire
+// make it visible to that CTA.
+__device__ __forceinline__ void st4_cluster(uint32_t addr, float4 v) {
+    asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(v.x), "f"(v.y), "f"(v.z),
+                 "f"(v.w));
+}
+// The two halves of the cluster barrier: arrive releases this thread's
+// earlier shared-memory writes to the cluster, wait acquires the others'.
+__device__ __forceinline__ void cluster_arrive() {
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void cluster_wait() {
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
 // This thread's place in the cluster: rank, quad, first row, and the
@@ -355,66 +241,80 @@ struct Ctx {
 };
 __device__ __forceinline__ int bit(int j, int pl, int k) { return (j * PL + pl) * 4 + k; }
 
-// Plane PL-1 of the slab at `buf` in rank r-1 / plane 0 of rank r+1, at
-// in-plane offset `off`.
-__device__ __forceinline__ float4 ld_below(const Ctx &c, int buf, int off) {
-    return c.has_below ? ld4_cluster(c.below + (uint32_t)(buf + (PL - 1) * PLANE + off) * 4u) : zero4();
-}
-__device__ __forceinline__ float4 ld_above(const Ctx &c, int buf, int off) {
-    return c.has_above ? ld4_cluster(c.above + (uint32_t)(buf + off) * 4u) : zero4();
+// Writes an edge plane's quad into the neighbour that reads it: plane 0 of
+// buffer `buf` is the plane above rank r-1's slab, plane PL-1 the plane below
+// rank r+1's.
+__device__ __forceinline__ void push_edge(const Ctx &c, int buf, int pl, int off, float4 v) {
+    if (pl == 0 && c.has_below) st4_cluster(c.below + (uint32_t)(halo(buf, 1) + off) * 4u, v);
+    if (pl == PL - 1 && c.has_above) st4_cluster(c.above + (uint32_t)(halo(buf, 0) + off) * 4u, v);
 }
 
-// A Jacobi sweep of this CTA's slab, S -> T. `fixed` marks the pinned
-// cells. The per-cell source is the gravity's 4*pi*G*rho in registers (src)
-// or the air's divergence in slab C of shared memory. The thread's rows are
+// One plane of a Jacobi sweep, S -> T, from the planes below / at / above it
+// (ym, c, yp per row); an edge plane is also written into the neighbour that
+// reads it. `fixed` marks the pinned cells; src holds the per-cell source
+// (the gravity's 4*pi*G*rho or the air's divergence). The thread's rows are
 // adjacent in z, so only the outer z neighbours are loaded.
 template <bool GRAV>
-__device__ __forceinline__ void sweep(const Ctx &cx, int S, int T, const float4 (&src)[ROWS][PL], uint32_t fixed) {
+__device__ __forceinline__ void sweep_plane(const Ctx &cx, int S, int T, int pl, const float4 (&ym)[ROWS],
+                                            const float4 (&c)[ROWS], const float4 (&yp)[ROWS],
+                                            const float4 (&src)[ROWS][PL], uint32_t fixed) {
     const float *s = cx.sm + S;
-    float4 ym[ROWS], c[ROWS];
+    float *t = cx.sm + T;
+    const float4 zlo = ld4(s + pl * PLANE + cx.zlo), zhi = ld4(s + pl * PLANE + cx.zhi);
 #pragma unroll
     for (int j = 0; j < ROWS; ++j) {
-        ym[j] = ld_below(cx, S, cx.o + j * N);
-        c[j] = ld4(s + cx.o + j * N);
+        const float4 zm = j == 0 ? zlo : c[j - 1], zp = j == ROWS - 1 ? zhi : c[j + 1];
+        const float l = __shfl_up_sync(0xFFFFFFFFu, c[j].w, 1, 16);
+        const float r = __shfl_down_sync(0xFFFFFFFFu, c[j].x, 1, 16);
+        const uint32_t pins = (fixed >> bit(j, pl, 0)) & 0xFu;
+        float4 out;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float xm = k == 0 ? l : f4(c[j], k - 1), xp = k == 3 ? r : f4(c[j], k + 1);
+            const bool fx = (pins >> k) & 1u;
+            f4set(out, k,
+                  GRAV ? grav_sweep_cell(xm, xp, f4(zm, k), f4(zp, k), f4(ym[j], k), f4(yp[j], k),
+                                         f4(src[j][pl], k), f4(c[j], k), pins != 0u && fx)
+                       : air_sweep_cell(xm, xp, f4(zm, k), f4(zp, k), f4(ym[j], k), f4(yp[j], k),
+                                        f4(src[j][pl], k), pins != 0u && fx));
+        }
+        st4(t + pl * PLANE + cx.o + j * N, out);
+        push_edge(cx, T, pl, cx.o + j * N, out);
     }
+}
+
+// One Jacobi sweep of this CTA's slab, S -> T, with the cluster barrier
+// split around it: the edge planes (0 and PL-1, the only ones other CTAs
+// need) are computed and pushed first and released with `arrive`; the inner
+// planes are computed while the barrier completes; `wait` then acquires the
+// neighbours' pushes for the next sweep, and a CTA barrier publishes this
+// CTA's inner planes. On entry S and its halo planes are complete.
+template <bool GRAV>
+__device__ __forceinline__ void sweep(const Ctx &cx, int S, int T, const float4 (&src)[ROWS][PL], uint32_t fixed) {
+    static_assert(PL == 4, "edge planes 0 and 3, inner planes 1 and 2");
+    const float *s = cx.sm + S;
+    float4 below[ROWS], above[ROWS], p0[ROWS], p1[ROWS], p2[ROWS], p3[ROWS];
 #pragma unroll
-    for (int pl = 0; pl < PL; ++pl) {
-        float4 yp[ROWS];
-#pragma unroll
-        for (int j = 0; j < ROWS; ++j) {
-            if (pl + 1 < PL) yp[j] = ld4(s + (pl + 1) * PLANE + cx.o + j * N);
-            else yp[j] = ld_above(cx, S, cx.o + j * N);
-        }
-        const float4 zlo = ld4(s + pl * PLANE + cx.zlo), zhi = ld4(s + pl * PLANE + cx.zhi);
-#pragma unroll
-        for (int j = 0; j < ROWS; ++j) {
-            const float4 zm = j == 0 ? zlo : c[j - 1], zp = j == ROWS - 1 ? zhi : c[j + 1];
-            const float l = __shfl_up_sync(0xFFFFFFFFu, c[j].w, 1, 16);
-            const float r = __shfl_down_sync(0xFFFFFFFFu, c[j].x, 1, 16);
-            const float4 dv = GRAV ? zero4() : ld4(cx.sm + SC + pl * PLANE + cx.o + j * N);
-            float4 out;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const float xm = k == 0 ? l : f4(c[j], k - 1), xp = k == 3 ? r : f4(c[j], k + 1);
-                const bool fx = (fixed >> bit(j, pl, k)) & 1u;
-                f4set(out, k,
-                      GRAV ? grav_sweep_cell(xm, xp, f4(zm, k), f4(zp, k), f4(ym[j], k), f4(yp[j], k),
-                                             f4(src[j][pl], k), f4(c[j], k), fx)
-                           : air_sweep_cell(xm, xp, f4(zm, k), f4(zp, k), f4(ym[j], k), f4(yp[j], k),
-                                            f4(dv, k), fx));
-            }
-            st4(cx.sm + T + pl * PLANE + cx.o + j * N, out);
-        }
-#pragma unroll
-        for (int j = 0; j < ROWS; ++j) {
-            ym[j] = c[j];
-            c[j] = yp[j];
-        }
+    for (int j = 0; j < ROWS; ++j) {
+        const int o = cx.o + j * N;
+        below[j] = ld4(cx.sm + halo(S, 0) + o);
+        above[j] = ld4(cx.sm + halo(S, 1) + o);
+        p0[j] = ld4(s + o);
+        p1[j] = ld4(s + PLANE + o);
+        p2[j] = ld4(s + 2 * PLANE + o);
+        p3[j] = ld4(s + 3 * PLANE + o);
     }
+    sweep_plane<GRAV>(cx, S, T, 0, below, p0, p1, src, fixed);
+    sweep_plane<GRAV>(cx, S, T, 3, p2, p3, above, src, fixed);
+    cluster_arrive();
+    sweep_plane<GRAV>(cx, S, T, 1, p0, p1, p2, src, fixed);
+    sweep_plane<GRAV>(cx, S, T, 2, p1, p2, p3, src, fixed);
+    cluster_wait();
+    __syncthreads();
 }
 
 // The six neighbours of the quad of row j on plane `pl` of a slab buffer
-// (zeros beyond the world's y faces).
+// (its halo planes beyond the slab).
 struct Hood {
     float4 c, zm, zp, ym, yp;
     float l, r;
@@ -426,22 +326,8 @@ __device__ __forceinline__ Hood hood(const Ctx &cx, int buf, int pl, int j) {
     h.c = ld4(v + pl * PLANE + o);
     h.zm = ld4(v + pl * PLANE + max(z - 1, 0) * N + cx.x0);
     h.zp = ld4(v + pl * PLANE + min(z + 1, N - 1) * N + cx.x0);
-    if (pl > 0) h.ym = ld4(v + (pl - 1) * PLANE + o);
-    else h.ym = ld_below(cx, buf, o);
-    if (pl + 1 < PL) h.yp = ld4(v + (pl + 1) * PLANE + o);
-    else h.yp = ld_above(cx, buf, o);
-    h.l = __shfl_up_sync(0xFFFFFFFFu, h.c.w, 1, 16);
-    h.r = __shfl_down_sync(0xFFFFFFFFu, h.c.x, 1, 16);
-    return h;
-}
-// The same from a field in global memory (cell index g of the quad's first cell).
-__device__ __forceinline__ Hood hood_global(const float *V, size_t g, int y, int z) {
-    Hood h;
-    h.c = ld4(V + g);
-    h.zm = z > 0 ? ld4(V + g - SZ) : zero4();
-    h.zp = z + 1 < N ? ld4(V + g + SZ) : zero4();
-    h.ym = y > 0 ? ld4(V + g - SY) : zero4();
-    h.yp = y + 1 < N ? ld4(V + g + SY) : zero4();
+    h.ym = ld4(pl > 0 ? v + (pl - 1) * PLANE + o : cx.sm + halo(buf, 0) + o);
+    h.yp = ld4(pl + 1 < PL ? v + (pl + 1) * PLANE + o : cx.sm + halo(buf, 1) + o);
     h.l = __shfl_up_sync(0xFFFFFFFFu, h.c.w, 1, 16);
     h.r = __shfl_down_sync(0xFFFFFFFFu, h.c.x, 1, 16);
     return h;
@@ -449,164 +335,67 @@ __device__ __forceinline__ Hood hood_global(const float *V, size_t g, int y, int
 __device__ __forceinline__ float hx_m(const Hood &h, int k) { return k == 0 ? h.l : f4(h.c, k - 1); }
 __device__ __forceinline__ float hx_p(const Hood &h, int k) { return k == 3 ? h.r : f4(h.c, k + 1); }
 
-// New values of velocity component AXIS for the quad of row j on plane `pl`:
-// V is the staged old component, P the solved pressure. The buoyancy and the
-// gradient are formed first so that one neighbourhood is live at a time.
-template <int AXIS>
-__device__ __forceinline__ float4 advect_quad(const Ctx &cx, int V, int P, const float *temp, int pl, int j,
-                                              uint32_t solid) {
-    const int y = cx.r * PL + pl, z = cx.z0 + j, o = cx.o + j * N;
-    float4 buoy = zero4(), grad;
-    if (AXIS == 1) {
-        const Hood t = hood_global(temp, cx.g0 + (size_t)pl * PLANE + (size_t)j * N, y, z);
+// Stages buffer A from global memory, pushes its edge planes into the
+// neighbours' halo planes of A and zeroes the halo planes beyond the world's
+// y faces (they feed only pinned cells).
+__device__ __forceinline__ void stage_a(const Ctx &cx, const float *src) {
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const float lt = nb_average(f4(t.c, k), hx_m(t, k), hx_p(t, k), f4(t.zm, k), f4(t.zp, k), f4(t.ym, k),
-                                        f4(t.yp, k), cx.x0 + k, y, z);
-            f4set(buoy, k, (lt - kAmbient) * kBuoyancy);
+    for (int j = 0; j < ROWS; ++j) {
+        const int o = cx.o + j * N;
+#pragma unroll
+        for (int pl = 0; pl < PL; ++pl) {
+            const float4 v = ld4(src + cx.g0 + (size_t)pl * PLANE + (size_t)j * N);
+            st4(cx.sm + SA + pl * PLANE + o, v);
+            push_edge(cx, SA, pl, o, v);
+        }
+        if (!cx.has_below) {
+            st4(cx.sm + halo(SA, 0) + o, zero4());
+            st4(cx.sm + halo(SB, 0) + o, zero4());
+        }
+        if (!cx.has_above) {
+            st4(cx.sm + halo(SA, 1) + o, zero4());
+            st4(cx.sm + halo(SB, 1) + o, zero4());
         }
     }
-    {
-        const float *p = cx.sm + P;
-        const float4 pc = ld4(p + pl * PLANE + o);
-        if (AXIS == 0) {
-            const float l = __shfl_up_sync(0xFFFFFFFFu, pc.w, 1, 16), r = __shfl_down_sync(0xFFFFFFFFu, pc.x, 1, 16);
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                f4set(grad, k,
-                      pressure_grad(k == 0 ? l : f4(pc, k - 1), k == 3 ? r : f4(pc, k + 1), f4(pc, k), cx.x0 + k));
-        } else if (AXIS == 1) {
-            float4 lo, hi;
-            if (pl > 0) lo = ld4(p + (pl - 1) * PLANE + o);
-            else lo = ld_below(cx, P, o);
-            if (pl + 1 < PL) hi = ld4(p + (pl + 1) * PLANE + o);
-            else hi = ld_above(cx, P, o);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) f4set(grad, k, pressure_grad(f4(lo, k), f4(hi, k), f4(pc, k), y));
-        } else {
-            const float4 lo = ld4(p + pl * PLANE + max(z - 1, 0) * N + cx.x0);
-            const float4 hi = ld4(p + pl * PLANE + min(z + 1, N - 1) * N + cx.x0);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) f4set(grad, k, pressure_grad(f4(lo, k), f4(hi, k), f4(pc, k), z));
-        }
-    }
-    const Hood v = hood(cx, V, pl, j);
-    float4 out;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const float nv = advect_cell(f4(v.c, k), hx_m(v, k), hx_p(v, k), f4(v.zm, k), f4(v.zp, k), f4(v.ym, k),
-                                     f4(v.yp, k), AXIS, f4(grad, k), f4(buoy, k), cx.x0 + k, y, z);
-        f4set(out, k, ((solid >> bit(j, pl, k)) & 1u) ? 0.0f : nv);
-    }
-    return out;
 }
 
-// AirState::solve (air.rs:162-222) for one world.
+// The Jacobi sweeps of AirState::solve (air_kernel.rs:361-398, air.rs:
+// 195-213) for one world; the pv update, divergence and velocity snapshot
+// before them and the advection after them run as grid-wide kernels.
 __device__ __forceinline__ void air_job(const Job &jb, const Ctx &cx, cg::cluster_group &cl) {
-    float *vx = jb.f[0], *vy = jb.f[1], *vz = jb.f[2], *p = jb.f[3], *p_tmp = jb.f[4];
-    const float *temp = jb.f[5], *solid = jb.f[6];
-    int32_t *pv = jb.i0;
+    float *p = jb.f[0], *p_tmp = jb.f[1];
+    const float *dsrc = jb.f[2], *solid = jb.f[3];
     float *sm = cx.sm;
     const int y0 = cx.r * PL;
 
-    // Stage p (A), vy (B) and vz (C); mark pinned and solid cells.
-    uint32_t fixed = 0u, solid_bits = 0u;
+    // Stage p (A) and the divergence (registers); mark the pinned cells.
+    stage_a(cx, p);
+    float4 div[ROWS][PL];
+    uint32_t fixed = 0u;
 #pragma unroll
     for (int j = 0; j < ROWS; ++j)
 #pragma unroll
         for (int pl = 0; pl < PL; ++pl) {
-            const int so = pl * PLANE + cx.o + j * N;
             const size_t g = cx.g0 + (size_t)pl * PLANE + (size_t)j * N;
-            st4(sm + SA + so, ld4(p + g));
-            st4(sm + SB + so, ld4(vy + g));
-            st4(sm + SC + so, ld4(vz + g));
-            const float4 s = ld4(solid + g);
+            div[j][pl] = ld4(dsrc + g);
+            const float4 sd = ld4(solid + g);
             const int y = y0 + pl, z = cx.z0 + j;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 const int x = cx.x0 + k;
                 const bool boundary = x == 0 || y == 0 || z == 0 || x == N - 1 || y == N - 1 || z == N - 1;
-                const bool sol = f4(s, k) > 0.5f;
-                solid_bits |= (uint32_t)sol << bit(j, pl, k);
-                fixed |= (uint32_t)(boundary || sol) << bit(j, pl, k);
+                fixed |= (uint32_t)(boundary || f4(sd, k) > 0.5f) << bit(j, pl, k);
             }
         }
     cl.sync();
 
-    // pv update (air_kernel.rs:294-326) and the sweeps' divergence
-    // (air_kernel.rs:385-388), both from the velocities before the solve; vx
-    // comes from global memory, vy from slab B, vz from slab C. The
-    // divergence then replaces vz in slab C, once every thread of the CTA
-    // has read its vz rows.
-#pragma unroll 1
-    for (int c = 0; c < ROWS * PL; ++c) {
-        const int j = c / PL, pl = c % PL;
-        const int so = pl * PLANE + cx.o + j * N, z = cx.z0 + j, y = y0 + pl;
-        const size_t g = cx.g0 + (size_t)pl * PLANE + (size_t)j * N;
-        const float4 xc = ld4(vx + g);
-        const float xl = __shfl_up_sync(0xFFFFFFFFu, xc.w, 1, 16);
-        const float xr = __shfl_down_sync(0xFFFFFFFFu, xc.x, 1, 16);
-        const float4 ym = pl > 0 ? ld4(sm + SB + so - PLANE) : ld_below(cx, SB, cx.o + j * N);
-        const float4 yp = pl + 1 < PL ? ld4(sm + SB + so + PLANE) : ld_above(cx, SB, cx.o + j * N);
-        const float4 zm = ld4(sm + SC + pl * PLANE + max(z - 1, 0) * N + cx.x0);
-        const float4 zp = ld4(sm + SC + pl * PLANE + min(z + 1, N - 1) * N + cx.x0);
-        const int4 pv4 = *reinterpret_cast<const int4 *>(pv + g);
-        int32_t pvs[4] = {pv4.x, pv4.y, pv4.z, pv4.w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int x = cx.x0 + k;
-            const float xm = k == 0 ? xl : f4(xc, k - 1), xp = k == 3 ? xr : f4(xc, k + 1);
-            const bool rim = x < 2 || x >= N - 2 || y < 2 || y >= N - 2 || z < 2 || z >= N - 2;
-            const float dp = (xm - xp) + (f4(ym, k) - f4(yp, k)) + (f4(zm, k) - f4(zp, k));
-            pvs[k] = pv_update(pvs[k], rim, dp);
-        }
-        *reinterpret_cast<int4 *>(pv + g) = make_int4(pvs[0], pvs[1], pvs[2], pvs[3]);
-    }
-    {
-        float4 div[ROWS][PL];
-#pragma unroll
-        for (int j = 0; j < ROWS; ++j)
-#pragma unroll
-            for (int pl = 0; pl < PL; ++pl) {
-                const int so = pl * PLANE + cx.o + j * N, z = cx.z0 + j;
-                const size_t g = cx.g0 + (size_t)pl * PLANE + (size_t)j * N;
-                const float4 xc = ld4(vx + g);
-                const float xl = __shfl_up_sync(0xFFFFFFFFu, xc.w, 1, 16);
-                const float xr = __shfl_down_sync(0xFFFFFFFFu, xc.x, 1, 16);
-                float4 ym, yp;
-                if (pl > 0) ym = ld4(sm + SB + so - PLANE);
-                else ym = ld_below(cx, SB, cx.o + j * N);
-                if (pl + 1 < PL) yp = ld4(sm + SB + so + PLANE);
-                else yp = ld_above(cx, SB, cx.o + j * N);
-                const float4 zm = ld4(sm + SC + pl * PLANE + max(z - 1, 0) * N + cx.x0);
-                const float4 zp = ld4(sm + SC + pl * PLANE + min(z + 1, N - 1) * N + cx.x0);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const float xm = k == 0 ? xl : f4(xc, k - 1), xp = k == 3 ? xr : f4(xc, k + 1);
-                    f4set(div[j][pl], k, 0.5f * ((xp - xm) + (f4(yp, k) - f4(ym, k)) + (f4(zp, k) - f4(zm, k))));
-                }
-            }
-        __syncthreads();
-#pragma unroll
-        for (int j = 0; j < ROWS; ++j)
-#pragma unroll
-            for (int pl = 0; pl < PL; ++pl) st4(sm + SC + pl * PLANE + cx.o + j * N, div[j][pl]);
-    }
-    cl.sync();
-
-    // Jacobi sweeps (air_kernel.rs:361-398): odd sweeps write B (the
-    // reference's p_tmp), even ones A (p).
-    const float4 no_src[ROWS][PL] = {};
+    // Odd sweeps write B (the reference's p_tmp), even ones A (p).
     const uint32_t n = jb.iterations;
     for (uint32_t it = 0; it < n; ++it) {
-        if ((it & 1u) == 0u) sweep<false>(cx, SA, SB, no_src, fixed);  // the divergence is in slab C
-        else sweep<false>(cx, SB, SA, no_src, fixed);
-        cl.sync();
+        if ((it & 1u) == 0u) sweep<false>(cx, SA, SB, div, fixed);
+        else sweep<false>(cx, SB, SA, div, fixed);
     }
-    const int P = (n & 1u) ? SB : SA, F = (n & 1u) ? SA : SB;
-
-    // Publish the pair as the reference's alternation leaves it; stage vx
-    // (F) and vy (C) for the advection (air_kernel.rs:414-536).
+    // Publish the pair as the reference's alternation leaves it.
 #pragma unroll
     for (int j = 0; j < ROWS; ++j)
 #pragma unroll
@@ -615,29 +404,7 @@ __device__ __forceinline__ void air_job(const Job &jb, const Ctx &cx, cg::cluste
             const size_t g = cx.g0 + (size_t)pl * PLANE + (size_t)j * N;
             if (n >= 2u) st4(p + g, ld4(sm + SA + so));
             if (n >= 1u) st4(p_tmp + g, ld4(sm + SB + so));
-            st4(sm + F + so, ld4(vx + g));
-            st4(sm + SC + so, ld4(vy + g));
         }
-    cl.sync();
-#pragma unroll 1
-    for (int c = 0; c < ROWS * PL; ++c) {
-        const int j = c / PL, pl = c % PL;
-        const size_t g = cx.g0 + (size_t)pl * PLANE + (size_t)j * N;
-        st4(vx + g, advect_quad<0>(cx, F, P, temp, pl, j, solid_bits));
-        st4(vy + g, advect_quad<1>(cx, SC, P, temp, pl, j, solid_bits));
-    }
-    cl.sync();
-#pragma unroll
-    for (int j = 0; j < ROWS; ++j)
-#pragma unroll
-        for (int pl = 0; pl < PL; ++pl)
-            st4(sm + F + pl * PLANE + cx.o + j * N, ld4(vz + cx.g0 + (size_t)pl * PLANE + (size_t)j * N));
-    cl.sync();
-#pragma unroll 1
-    for (int c = 0; c < ROWS * PL; ++c) {
-        const int j = c / PL, pl = c % PL;
-        st4(vz + cx.g0 + (size_t)pl * PLANE + (size_t)j * N, advect_quad<2>(cx, F, P, temp, pl, j, solid_bits));
-    }
     cl.sync();
 }
 
@@ -649,6 +416,7 @@ __device__ __forceinline__ void grav_job(const Job &jb, const Ctx &cx, cg::clust
     float *sm = cx.sm;
     const int y0 = cx.r * PL;
 
+    stage_a(cx, pot);
     float4 src[ROWS][PL];
     uint32_t fixed = 0u;
 #pragma unroll
@@ -656,7 +424,6 @@ __device__ __forceinline__ void grav_job(const Job &jb, const Ctx &cx, cg::clust
 #pragma unroll
         for (int pl = 0; pl < PL; ++pl) {
             const size_t g = cx.g0 + (size_t)pl * PLANE + (size_t)j * N;
-            st4(sm + SA + pl * PLANE + cx.o + j * N, ld4(pot + g));
             const int4 m = *reinterpret_cast<const int4 *>(mass + g);
             src[j][pl] = make_float4(grav_source(m.x), grav_source(m.y), grav_source(m.z), grav_source(m.w));
             if (jb.clear_mass) *reinterpret_cast<int4 *>(mass + g) = make_int4(0, 0, 0, 0);
@@ -674,7 +441,6 @@ __device__ __forceinline__ void grav_job(const Job &jb, const Ctx &cx, cg::clust
     for (uint32_t it = 0; it < n; ++it) {
         if ((it & 1u) == 0u) sweep<true>(cx, SA, SB, src, fixed);
         else sweep<true>(cx, SB, SA, src, fixed);
-        cl.sync();
     }
     // The last sweep is grav_potential and the one before grav_potential_tmp
     // (the reference swaps the two handles after every sweep).
@@ -725,6 +491,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_field_cluster(const __grid_const
     cx.zhi = min(cx.z0 + ROWS, N - 1) * N + cx.x0;
     cx.g0 = (size_t)(cx.r * PL) * PLANE + cx.o;
     const Job &jb = J.job[blockIdx.x / CL];
+    cl.sync();  // every CTA of the cluster is running before any writes into another's shared memory
     if (jb.kind == JOB_AIR) air_job(jb, cx, cl);
     else grav_job(jb, cx, cl);
 }
@@ -732,11 +499,6 @@ __global__ void __launch_bounds__(THREADS, 1) k_field_cluster(const __grid_const
 // ----------------------------------------------------- per-sweep form ----
 // One thread per cell, one launch per reference pass.
 
-__device__ __forceinline__ void coords(int i, int &x, int &y, int &z) {
-    x = i & 63;
-    z = (i >> 6) & 63;
-    y = i >> 12;
-}
 
 __global__ void __launch_bounds__(256) k_ps_pressure_volume(const float *__restrict__ vx, const float *__restrict__ vy,
                                                             const float *__restrict__ vz, int32_t *__restrict__ pv) {
@@ -748,6 +510,33 @@ __global__ void __launch_bounds__(256) k_ps_pressure_volume(const float *__restr
     float dp = 0.0f;
     if (!rim) dp = (vx[i - 1] - vx[i + 1]) + (vy[i - SY] - vy[i + SY]) + (vz[i - SZ] - vz[i + SZ]);
     pv[i] = pv_update(pv[i], rim, dp);
+}
+
+// The grid-wide passes of the cluster form's air solve before the sweeps:
+// the pv update (air_kernel.rs:294-326), the velocity snapshot (:338-351)
+// and the sweeps' divergence (:385-388), which the reference recomputes in
+// every sweep from the velocities the sweeps leave unchanged.
+__global__ void __launch_bounds__(256) k_air_prep(const float *__restrict__ vx, const float *__restrict__ vy,
+                                                  const float *__restrict__ vz, int32_t *__restrict__ pv,
+                                                  float *__restrict__ div, float *__restrict__ snap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= CELLS) return;
+    int x, y, z;
+    coords(i, x, y, z);
+    snap[i] = vx[i];
+    snap[CELLS + i] = vy[i];
+    snap[2 * CELLS + i] = vz[i];
+    const bool inner = x > 0 && y > 0 && z > 0 && x < N - 1 && y < N - 1 && z < N - 1;
+    const bool rim = x < 2 || x >= N - 2 || y < 2 || y >= N - 2 || z < 2 || z >= N - 2;
+    float dp = 0.0f, d = 0.0f;
+    if (inner) {
+        const float xm = vx[i - 1], xp = vx[i + 1], ym = vy[i - SY], yp = vy[i + SY], zm = vz[i - SZ],
+                    zp = vz[i + SZ];
+        dp = (xm - xp) + (ym - yp) + (zm - zp);
+        d = 0.5f * ((xp - xm) + (yp - ym) + (zp - zm));
+    }
+    div[i] = d;
+    pv[i] = pv_update(pv[i], rim, dp);  // the rim holds every cell outside `inner`
 }
 
 __global__ void __launch_bounds__(256) k_ps_snapshot(const float *__restrict__ vx, const float *__restrict__ vy,
@@ -851,36 +640,32 @@ __global__ void __launch_bounds__(256) k_grav_clear(int32_t *mass) {
 
 // --------------------------------------------------------------- host ----
 
-static int g_gather_blocks = 0;
-
-static int gather_blocks() {
-    if (g_gather_blocks == 0) {
-        int dev = 0, sms = 0;
-        TPT_CUDA(cudaGetDevice(&dev));
-        TPT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        g_gather_blocks = sms * 8;  // 8 resident blocks of 256 threads per SM
-    }
-    return g_gather_blocks;
-}
-
 int launch_air_clear(const World &w, cudaStream_t st) {
     k_air_clear<<<CELLS / 4 / 256, 256, 0, st>>>(w.vx, w.vy, w.vz, w.p, w.p_tmp, w.temp, w.solid, w.pv);
     TPT_LAUNCHED();
     return TPT_OK;
 }
 
+// Persistent gather grid: 256-thread blocks, `per_sm` per SM.
+static int gather_blocks(int per_sm) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            sms = 148;
+    }
+    return sms * per_sm;
+}
+
 int launch_air_gather(const World &w, cudaStream_t st) {
-    const int blocks = gather_blocks();
-    if (blocks <= 0) return TPT_ERR_CUDA;
-    k_air_gather<<<blocks, 256, 0, st>>>(w.voxel, w.sim_list, w.sim_count, w.solid, w.temp);
+    k_air_gather<<<gather_blocks(8), 256, 0, st>>>(w.voxel, w.sim_list, w.sim_count, w.solid, w.temp);
     TPT_LAUNCHED();
     return TPT_OK;
 }
 
 int launch_grav_gather(const World &w, cudaStream_t st) {
-    const int blocks = gather_blocks();
-    if (blocks <= 0) return TPT_ERR_CUDA;
-    k_grav_gather<<<blocks, 256, 0, st>>>(w.voxel, w.aux_tmp, w.sim_list, w.sim_count, w.grav_mass);
+    k_grav_gather<<<gather_blocks(4), 256, 0, st>>>(w.voxel, w.aux_tmp, w.sim_list, w.sim_count, w.grav_mass);
     TPT_LAUNCHED();
     return TPT_OK;
 }
@@ -970,19 +755,28 @@ int launch_grav_per_sweep(const World &w, cudaStream_t st) {
     return TPT_OK;
 }
 
-Job air_job_of(const World &w, uint32_t iterations) {
+Job air_job_of(const World &w, uint32_t iterations, const AirScratch &sc) {
     Job j{};
-    j.f[0] = w.vx;
-    j.f[1] = w.vy;
-    j.f[2] = w.vz;
-    j.f[3] = w.p;
-    j.f[4] = w.p_tmp;
-    j.f[5] = w.temp;
-    j.f[6] = w.solid;
-    j.i0 = w.pv;
+    j.f[0] = w.p;
+    j.f[1] = w.p_tmp;
+    j.f[2] = sc.div;
+    j.f[3] = w.solid;
     j.kind = JOB_AIR;
     j.iterations = iterations;
     return j;
+}
+
+int launch_air_prep(const World &w, const AirScratch &sc, cudaStream_t st) {
+    k_air_prep<<<CELLS / 256, 256, 0, st>>>(w.vx, w.vy, w.vz, w.pv, sc.div, sc.snap);
+    TPT_LAUNCHED();
+    return TPT_OK;
+}
+
+int launch_air_advect(const World &w, uint32_t iterations, const AirScratch &sc, cudaStream_t st) {
+    const float *pr = (iterations & 1u) ? w.p_tmp : w.p;  // the last sweep's buffer
+    k_ps_air_advect<<<CELLS / 256, 256, 0, st>>>(sc.snap, pr, w.temp, w.solid, w.vx, w.vy, w.vz);
+    TPT_LAUNCHED();
+    return TPT_OK;
 }
 
 Job grav_job_of(const World &w, bool clear_mass) {

@@ -8,7 +8,38 @@ using namespace tpt;
 
 struct tpt_vox_plan {
     int form = TPT_VOX_PER_SWEEP;
-    float *snapshot = nullptr;  // the per-sweep form's velocity snapshot (3 fields)
+    // Per-sweep form: the reference's velocity snapshot (3 fields).
+    // Cluster form: one AirScratch (4 fields) per world of a launch.
+    // Batched form: BATCH_SCRATCH_BYTES per world of a launch.
+    float *scratch = nullptr;
+    tpt::vox::AirScratch slot(uint32_t i) const {
+        float *b = scratch + (size_t)i * tpt::vox::AIR_SCRATCH_FLOATS;
+        return {b, b + TPT_VOX_CELLS};
+    }
+    tpt::vox::BWorld bworld(uint32_t i, const tpt_vox_world &w) const {
+        char *b = reinterpret_cast<char *>(scratch) + (size_t)i * tpt::vox::BATCH_SCRATCH_BYTES;
+        float *f = reinterpret_cast<float *>(b);
+        tpt::vox::BWorld o{};
+        o.vx = w.vx;
+        o.vy = w.vy;
+        o.vz = w.vz;
+        o.p = w.p;
+        o.p_tmp = w.p_tmp;
+        o.temp = w.temp;
+        o.solid = w.solid;
+        o.pv = w.pv;
+        o.mass = w.grav_mass;
+        o.pot = w.grav_potential;
+        o.pot_tmp = w.grav_potential_tmp;
+        o.fx = w.grav_force_x;
+        o.fy = w.grav_force_y;
+        o.fz = w.grav_force_z;
+        o.div = f;
+        o.snap = f + TPT_VOX_CELLS;
+        o.src = f + 4 * TPT_VOX_CELLS;
+        o.pin = reinterpret_cast<uint8_t *>(f + 5 * TPT_VOX_CELLS);
+        return o;
+    }
 };
 
 namespace {
@@ -62,15 +93,33 @@ int check_gather(const tpt_vox_world *w) {
     return check_ptrs("gather", {w->voxel});
 }
 
+// One batched launch sequence of `fields` for worlds [first, first + n).
+int run_batch(tpt_vox_plan *plan, const tpt_vox_world *worlds, uint32_t n, uint32_t fields, uint32_t air_iterations,
+              bool clear_mass, cudaStream_t st) {
+    vox::Batch b{};
+    b.n = n;
+    b.fields = fields;
+    b.air_iters = air_iterations;
+    b.clear_mass = clear_mass ? 1u : 0u;
+    for (uint32_t i = 0; i < n; ++i) b.w[i] = plan->bworld(i, worlds[i]);
+    return vox::launch_batch(b, st);
+}
+
 int run_air_solve(tpt_vox_plan *plan, const tpt_vox_world *w, uint32_t iterations, cudaStream_t st) {
+    if (plan->form == TPT_VOX_BATCHED) return run_batch(plan, w, 1, 1u, iterations, false, st);
     const vox::World v = world_of(*w);
     if (plan->form == TPT_VOX_CLUSTER) {
+        const vox::AirScratch sc = plan->slot(0);
+        int rc = vox::launch_air_prep(v, sc, st);
+        if (rc) return rc;
         vox::Jobs jobs{};
         jobs.n = 1;
-        jobs.job[0] = vox::air_job_of(v, iterations);
-        return vox::launch_cluster(jobs, st);
+        jobs.job[0] = vox::air_job_of(v, iterations, sc);
+        rc = vox::launch_cluster(jobs, st);
+        if (rc) return rc;
+        return vox::launch_air_advect(v, iterations, sc, st);
     }
-    return vox::launch_air_per_sweep(v, iterations, plan->snapshot, st);
+    return vox::launch_air_per_sweep(v, iterations, plan->scratch, st);
 }
 
 }  // namespace
@@ -80,27 +129,27 @@ extern "C" {
 int tpt_vox_plan_create(int form, tpt_vox_plan **out) {
     if (!out) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_plan_create: out is NULL");
     *out = nullptr;
-    if (form != TPT_VOX_AUTO && form != TPT_VOX_CLUSTER && form != TPT_VOX_PER_SWEEP)
+    if (form != TPT_VOX_AUTO && form != TPT_VOX_CLUSTER && form != TPT_VOX_PER_SWEEP && form != TPT_VOX_BATCHED)
         TPT_FAIL(TPT_ERR_INVALID_ARG, "tpt_vox_plan_create: unknown form %d", form);
     int rc = require_sm100();
     if (rc) return rc;
-    bool cluster_ok = false;
-    if (form != TPT_VOX_PER_SWEEP) {
+    if (form == TPT_VOX_CLUSTER) {
+        bool cluster_ok = false;
         rc = vox::cluster_supported(&cluster_ok);
         if (rc) return rc;
-        if (form == TPT_VOX_CLUSTER && !cluster_ok)
-            TPT_FAIL(TPT_ERR_UNSUPPORTED, "the device cannot schedule a 16-CTA cluster of the field kernel");
+        if (!cluster_ok) TPT_FAIL(TPT_ERR_UNSUPPORTED, "the device cannot schedule a 16-CTA cluster of the field kernel");
     }
     tpt_vox_plan *p = new (std::nothrow) tpt_vox_plan();
     if (!p) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "host allocation failed");
-    p->form = cluster_ok ? TPT_VOX_CLUSTER : TPT_VOX_PER_SWEEP;
-    if (p->form == TPT_VOX_PER_SWEEP) {
-        cudaError_t e = cudaMalloc(&p->snapshot, 3ull * TPT_VOX_CELLS * sizeof(float));
-        if (e != cudaSuccess) {
-            delete p;
-            TPT_FAIL(e == cudaErrorMemoryAllocation ? TPT_ERR_OUT_OF_MEMORY : TPT_ERR_CUDA,
-                     "tpt_vox_plan_create: snapshot allocation failed: %s", cudaGetErrorString(e));
-        }
+    p->form = form == TPT_VOX_AUTO ? TPT_VOX_BATCHED : form;
+    size_t bytes = 3ull * TPT_VOX_CELLS * sizeof(float);
+    if (p->form == TPT_VOX_CLUSTER) bytes = (size_t)(vox::MAX_JOBS / 2) * vox::AIR_SCRATCH_FLOATS * sizeof(float);
+    if (p->form == TPT_VOX_BATCHED) bytes = (size_t)vox::MAX_BWORLDS * vox::BATCH_SCRATCH_BYTES;
+    cudaError_t e = cudaMalloc(&p->scratch, bytes);
+    if (e != cudaSuccess) {
+        delete p;
+        TPT_FAIL(e == cudaErrorMemoryAllocation ? TPT_ERR_OUT_OF_MEMORY : TPT_ERR_CUDA,
+                 "tpt_vox_plan_create: scratch allocation failed: %s", cudaGetErrorString(e));
     }
     *out = p;
     return TPT_OK;
@@ -108,7 +157,7 @@ int tpt_vox_plan_create(int form, tpt_vox_plan **out) {
 
 int tpt_vox_plan_destroy(tpt_vox_plan *plan) {
     if (!plan) return TPT_OK;
-    if (plan->snapshot) cudaFree(plan->snapshot);
+    if (plan->scratch) cudaFree(plan->scratch);
     delete plan;
     return TPT_OK;
 }
@@ -147,6 +196,7 @@ int tpt_vox_grav_solve(tpt_vox_plan *plan, const tpt_vox_world *w, tpt_stream_t 
     int rc = check_grav_solve(w);
     if (rc) return rc;
     const vox::World v = world_of(*w);
+    if (plan->form == TPT_VOX_BATCHED) return run_batch(plan, w, 1, 2u, 0u, false, (cudaStream_t)stream);
     if (plan->form == TPT_VOX_CLUSTER) {
         vox::Jobs jobs{};
         jobs.n = 1;
@@ -186,32 +236,52 @@ int tpt_vox_field_step(tpt_vox_plan *plan, const tpt_vox_world *worlds, uint32_t
         if (rc) return rc;
     }
     cudaStream_t st = (cudaStream_t)stream;
+    if (plan->form == TPT_VOX_BATCHED) {
+        // per group of up to MAX_BWORLDS worlds: every world's gather, then
+        // one batched launch sequence of air and gravity for all of them
+        for (uint32_t first = 0; first < n; first += vox::MAX_BWORLDS) {
+            const uint32_t m = n - first < vox::MAX_BWORLDS ? n - first : vox::MAX_BWORLDS;
+            for (uint32_t i = first; i < first + m; ++i) {
+                int rc = vox::launch_air_gather(world_of(worlds[i]), st);
+                if (rc) return rc;
+            }
+            int rc = run_batch(plan, worlds + first, m, 3u, air_iterations, true, st);
+            if (rc) return rc;
+        }
+        return TPT_OK;
+    }
     if (plan->form != TPT_VOX_CLUSTER) {
         for (uint32_t i = 0; i < n; ++i) {
             const vox::World v = world_of(worlds[i]);
             int rc = vox::launch_air_gather(v, st);
-            if (!rc) rc = vox::launch_air_per_sweep(v, air_iterations, plan->snapshot, st);
+            if (!rc) rc = vox::launch_air_per_sweep(v, air_iterations, plan->scratch, st);
             if (!rc) rc = vox::launch_grav_per_sweep(v, st);
             if (!rc) rc = vox::launch_grav_clear(v, st);
             if (rc) return rc;
         }
         return TPT_OK;
     }
-    // Cluster form: every world's gather, then the solves of up to
-    // MAX_JOBS / 2 worlds per launch, air and gravity side by side.
-    for (uint32_t i = 0; i < n; ++i) {
-        int rc = vox::launch_air_gather(world_of(worlds[i]), st);
-        if (rc) return rc;
-    }
+    // Cluster form, per group of up to MAX_JOBS / 2 worlds: each world's
+    // gather and pre-sweep pass, one launch of every world's air sweeps and
+    // gravity solve side by side, then each world's advection.
     for (uint32_t first = 0; first < n; first += vox::MAX_JOBS / 2) {
+        const uint32_t last = n - first < vox::MAX_JOBS / 2 ? n : first + vox::MAX_JOBS / 2;
         vox::Jobs jobs{};
-        for (uint32_t i = first; i < n && jobs.n < vox::MAX_JOBS; ++i) {
+        for (uint32_t i = first; i < last; ++i) {
             const vox::World v = world_of(worlds[i]);
-            jobs.job[jobs.n++] = vox::air_job_of(v, air_iterations);
+            const vox::AirScratch sc = plan->slot(i - first);
+            int rc = vox::launch_air_gather(v, st);
+            if (!rc) rc = vox::launch_air_prep(v, sc, st);
+            if (rc) return rc;
+            jobs.job[jobs.n++] = vox::air_job_of(v, air_iterations, sc);
             jobs.job[jobs.n++] = vox::grav_job_of(v, true);
         }
         int rc = vox::launch_cluster(jobs, st);
         if (rc) return rc;
+        for (uint32_t i = first; i < last; ++i) {
+            rc = vox::launch_air_advect(world_of(worlds[i]), air_iterations, plan->slot(i - first), st);
+            if (rc) return rc;
+        }
     }
     return TPT_OK;
 }

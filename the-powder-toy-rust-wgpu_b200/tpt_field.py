@@ -52,7 +52,7 @@ EXPORTS = [
     "tpt_vox_grav_clear_mass", "tpt_vox_grav_gather", "tpt_vox_field_step", "tpt_check_device_errors",
     "tpt_last_error_string", "tpt_kernel_launch_count", "tpt_version",
 ]
-VOX_AUTO, VOX_CLUSTER, VOX_PER_SWEEP = 0, 1, 2
+VOX_AUTO, VOX_CLUSTER, VOX_PER_SWEEP, VOX_BATCHED = 0, 1, 2, 3
 
 
 class TptError(RuntimeError):

@@ -33,9 +33,11 @@ GRAVITY_ITERATIONS = 24      # gravity.rs:49
 
 
 class Plan:
-    """How the Jacobi solves run: `tf.VOX_CLUSTER` (one 16-CTA cluster per
-    field, one launch per step), `tf.VOX_PER_SWEEP` (one launch per pass and
-    sweep) or `tf.VOX_AUTO` (the cluster form when the device can hold it)."""
+    """How the Jacobi solves run: `tf.VOX_BATCHED` (one launch per sweep
+    index for every world of a call, air and gravity together; what
+    `tf.VOX_AUTO` picks), `tf.VOX_CLUSTER` (one 16-CTA cluster per field, the
+    grid in distributed shared memory) or `tf.VOX_PER_SWEEP` (the
+    reference's launch structure: one launch per pass, sweep and world)."""
 
     def __init__(self, form: int = tf.VOX_AUTO):
         h = ctypes.c_void_p()
