@@ -4,6 +4,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload c1|c2|c4|c5] [--ticks T]
     python bench.py --voxel3d [--worlds W] ...   (the 3-D sandbox's field step)
+    python bench.py --save-io                    (the .tptrs save codec, host only)
 
 Metric: cell-ticks/s = sum over instances of xcells*ycells * ticks / time;
 one tick is one air step plus one gravity solve of every instance (the
@@ -597,6 +598,57 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_save_io(args):
+    """Host timing of the `.tptrs` codec (crates/tpt-save/src/lib.rs) on a
+    C2-sized save: a 1600x900 canvas (90,000 cells, eight grids) with 50,000
+    particle records. One step decodes the file, restores the field-step
+    instance from it and encodes it again. Metric: decoded payload bytes per
+    second."""
+    import tpt_field as tf
+    import workloads as W
+
+    inst = W.make_stress_instance(400, 225, 77)
+    sv = tf.SaveData.new(1600, 900)
+    for name, key in (("air_pv", "pv"), ("air_vx", "vx"), ("air_vy", "vy"), ("air_hv", "hv"), ("fan_vx", "fan_vx"),
+                      ("fan_vy", "fan_vy"), ("wall_bmap", "wall"), ("wall_emap", "emap")):
+        sv.set_grid(name, getattr(inst, key))
+    st = W.Stream(78)
+    parts = np.zeros((50000, 16), np.uint32)
+    parts[:, 0] = (st.u64(50000) % np.uint64(180) + np.uint64(1)).astype(np.uint32)
+    parts[:, 3] = st.uniform(0, 1600, 50000).astype(np.float32).view(np.uint32)
+    parts[:, 4] = st.uniform(0, 900, 50000).astype(np.float32).view(np.uint32)
+    parts[:, 7] = st.uniform(250, 400, 50000).astype(np.float32).view(np.uint32)
+    sv.set_particles(parts)
+    data = sv.to_bytes()
+    import zlib
+    payload = len(zlib.decompress(data[8:]))
+
+    def step():
+        s2 = tf.SaveData.from_bytes(data)
+        s2.to_instance()
+        return s2.to_bytes()
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        tf.SaveData.from_bytes(data)
+    dec = (time.perf_counter() - t0) / args.steps
+    line = {
+        "metric": "save payload bytes/s (decode + restore + encode)", "value": payload / dt, "unit": "B/s",
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
+        "higher_is_better": True, "scaling": "none", "vs_baseline": None, "dtype": "bytes",
+        "data": "synthetic (a C2 stress sandbox and 50,000 particle records)",
+        "config": {"workload": ".tptrs codec, 1600x900 canvas, 50000 particles", "file_bytes": len(data),
+                   "payload_bytes": payload, "decode_ms": dec * 1e3, "threads": 1},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference_voxel3d(args, rank, world):
     if rank != 0:
         return
@@ -637,7 +689,11 @@ def main():
     ap.add_argument("--phase-ticks", type=int, default=200, help="even tick count of the per-phase timing")
     ap.add_argument("--voxel3d", action="store_true", help="the 3-D sandbox's field step instead of the 2-D one")
     ap.add_argument("--worlds", type=int, default=1, help="3-D worlds per rank (--voxel3d)")
+    ap.add_argument("--save-io", action="store_true", help="host timing of the .tptrs save codec")
     args = ap.parse_args()
+    if args.save_io:
+        run_save_io(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

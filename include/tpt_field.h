@@ -477,6 +477,105 @@ int tpt_vox_field_step(tpt_vox_plan *plan, const tpt_vox_world *worlds,
                        uint32_t n, uint32_t air_iterations,
                        tpt_stream_t stream);
 
+/* ---- save files (crates/tpt-save/src/lib.rs) ---------------------------
+ *
+ * A `.tptrs` file is the 8-byte magic "TPTRS001" followed by
+ * zlib(bincode(SaveData)) (lib.rs:3-9, 355-372), bincode 1.3.3 with its
+ * default options: little-endian fixed-width integers, u64 lengths for
+ * vectors and strings, u32 enum variant indices, bool and Option tags as one
+ * byte. SaveData (lib.rs:67-97) holds the SimulationConfig, the particles,
+ * the eight cell grids below, the rigid bodies and (version 2) the signs.
+ * These calls decode and encode it on the host, so real saves can seed the
+ * field step (tpt_air_step buffers or a tpt_batch instance) and its grids
+ * can be written back. Particles travel as raw 64-byte records; rigid bodies
+ * and signs are kept as they were read and written back unchanged.
+ */
+typedef struct tpt_save tpt_save;
+
+/* Every serialised field of SimulationConfig (crates/tpt-core/src/particle.rs:
+ * 166-222) in its order; bools as 0/1 bytes, enums as their discriminant,
+ * Option<f32> as a presence byte plus the value. */
+typedef struct tpt_save_config {
+    uint32_t xres, yres;
+    uint8_t paused, aheat_enable, pretty_powder, _pad0;
+    uint32_t edge_mode;    /* EdgeMode: 0 void, 1 solid, 2 loop */
+    uint32_t gravity_mode; /* TPT_GRAVITY_* */
+    uint32_t air_mode;     /* TPT_AIR_*     */
+    float ambient_air_temp, edge_pressure;
+    uint32_t display_mode, colour_mode, render_mode;
+    float fire_intensity;
+    uint8_t heat_enable, newton_grav, water_equal_test, _pad1;
+    float vorticity_coeff;
+    uint32_t convection_mode;
+    float edge_velocity_x, edge_velocity_y, custom_gravity_x, custom_gravity_y;
+    uint32_t temperature_scale;
+    uint8_t decorations, _pad2[3];
+    int32_t mouse_x, mouse_y;
+    uint8_t gravity_field_enabled, gravity_zones_enabled, grid, _pad3;
+    int32_t grid_size;
+    uint8_t grid_checkerboard, hud, debug_hud, show_brush;
+    uint8_t zoom_enabled, _pad4[3];
+    int32_t zoom_window_x, zoom_window_y, zoom_factor, zoom_scope_x, zoom_scope_y, zoom_scope_size;
+    uint8_t has_heat_display_limit_min, has_heat_display_limit_max, _pad5[2];
+    float heat_display_limit_min, heat_display_limit_max;
+    int32_t heat_display_auto_x, heat_display_auto_y, heat_display_auto_w, heat_display_auto_h;
+} tpt_save_config;
+
+/* The cell grids of a save, in SaveData order. */
+enum {
+    TPT_SAVE_AIR_VX = 0, TPT_SAVE_AIR_VY, TPT_SAVE_AIR_PV, TPT_SAVE_AIR_HV,
+    TPT_SAVE_FAN_VX, TPT_SAVE_FAN_VY, TPT_SAVE_WALL_BMAP, TPT_SAVE_WALL_EMAP,
+    TPT_SAVE_GRIDS
+};
+enum { TPT_SAVE_VERSION = 2, TPT_SAVE_MAX_CANVAS_DIM = 16384, TPT_SAVE_PARTICLE_BYTES = 64 };
+
+typedef struct tpt_save_info {
+    uint32_t version;
+    uint32_t xcells, ycells;  /* xres / 4, yres / 4 */
+    uint64_t n_particles, n_rigid_bodies, n_signs;
+    uint64_t grid_len[TPT_SAVE_GRIDS]; /* elements; 0 where absent (the air
+                                          grids of a pressureless save)   */
+} tpt_save_info;
+
+/* SimulationConfig::new(xres, yres) (particle.rs:224-281): the canvas
+ * rounded up to a multiple of 4 and at least 64, and the defaults. */
+void tpt_save_config_default(tpt_save_config *c, uint32_t xres, uint32_t yres);
+/* A version-2 save of `config` with zeroed grids of its cell count and no
+ * particles, rigid bodies or signs. */
+int tpt_save_create(const tpt_save_config *config, tpt_save **out);
+/* SaveData::from_bytes (lib.rs:374-421): magic, zlib, version 1 or 2,
+ * canvas 1..16384 on each side; every malformed input is an error
+ * (TPT_ERR_INVALID_ARG), never a crash. */
+int tpt_save_decode(const void *bytes, size_t len, tpt_save **out);
+/* SaveData::to_bytes (lib.rs:355-372): the version-2 layout, zlib at the
+ * default level. `*bytes` belongs to the save and stays valid until the
+ * next encode or the destroy. */
+int tpt_save_encode(tpt_save *s, const void **bytes, size_t *len);
+int tpt_save_destroy(tpt_save *s);
+int tpt_save_get_info(const tpt_save *s, tpt_save_info *out);
+int tpt_save_get_config(const tpt_save *s, tpt_save_config *out);
+int tpt_save_set_config(tpt_save *s, const tpt_save_config *config);
+int tpt_save_set_version(tpt_save *s, uint32_t version);
+/* A grid as stored (`bytes` must be grid_len * 4) / replaced by `bytes / 4`
+ * elements (0 allowed). */
+int tpt_save_grid_read(const tpt_save *s, int grid, void *host, size_t bytes);
+int tpt_save_grid_write(tpt_save *s, int grid, const void *host, size_t bytes);
+/* The grid as SaveData::restore_into loads it (lib.rs:318-330, fit_f32 /
+ * fit_u32): `cells` elements, the stored grid when its length is the
+ * restored canvas's cell count, zeros otherwise. */
+int tpt_save_grid_restore(const tpt_save *s, int grid, void *host, uint64_t cells);
+/* Particle records (bincode of GpuParticle, particle.rs:27-44): n * 64 bytes. */
+int tpt_save_particles_read(const tpt_save *s, void *host, size_t bytes);
+int tpt_save_particles_write(tpt_save *s, const void *host, size_t bytes);
+/* SaveData::retain_air_pressure (lib.rs:247-255): include == 0 empties the
+ * four air grids. */
+int tpt_save_retain_air_pressure(tpt_save *s, int include);
+/* The field-step configuration SaveData::restore_into gives the engine
+ * (lib.rs:262-281): SimulationConfig::new of the saved canvas with the saved
+ * paused/aheat/edge/gravity/air modes, ambient temperature and edge pressure;
+ * the other air fields and newton_grav at their defaults. */
+int tpt_save_instance_desc(const tpt_save *s, tpt_instance_desc *out);
+
 /* ---- diagnostics ------------------------------------------------------- */
 
 /*

@@ -49,9 +49,14 @@ EXPORTS = [
     "tpt_batch_write", "tpt_batch_read", "tpt_batch_step", "tpt_batch_tune", "tpt_batch_get_tuning",
     "tpt_batch_set_tuning", "tpt_batch_profile_phases", "tpt_vox_plan_create", "tpt_vox_plan_destroy",
     "tpt_vox_plan_form", "tpt_vox_air_clear", "tpt_vox_air_gather", "tpt_vox_air_solve", "tpt_vox_grav_solve",
-    "tpt_vox_grav_clear_mass", "tpt_vox_grav_gather", "tpt_vox_field_step", "tpt_check_device_errors",
+    "tpt_vox_grav_clear_mass", "tpt_vox_grav_gather", "tpt_vox_field_step", "tpt_save_config_default",
+    "tpt_save_create", "tpt_save_decode", "tpt_save_encode", "tpt_save_destroy", "tpt_save_get_info",
+    "tpt_save_get_config", "tpt_save_set_config", "tpt_save_set_version", "tpt_save_grid_read",
+    "tpt_save_grid_write", "tpt_save_grid_restore", "tpt_save_particles_read", "tpt_save_particles_write",
+    "tpt_save_retain_air_pressure", "tpt_save_instance_desc", "tpt_check_device_errors",
     "tpt_last_error_string", "tpt_kernel_launch_count", "tpt_version",
 ]
+SAVE_GRIDS = ("air_vx", "air_vy", "air_pv", "air_hv", "fan_vx", "fan_vy", "wall_bmap", "wall_emap")
 VOX_AUTO, VOX_CLUSTER, VOX_PER_SWEEP, VOX_BATCHED = 0, 1, 2, 3
 
 
@@ -129,6 +134,34 @@ class VoxWorld(ctypes.Structure):
         "grav_mass", "grav_potential", "grav_potential_tmp", "grav_force_x", "grav_force_y", "grav_force_z")]
 
 
+class SaveConfig(ctypes.Structure):
+    """tpt_save_config: every serialised SimulationConfig field, in order."""
+
+    u8, u32, i32, f32 = ctypes.c_uint8, ctypes.c_uint32, ctypes.c_int32, ctypes.c_float
+    _fields_ = [
+        ("xres", u32), ("yres", u32), ("paused", u8), ("aheat_enable", u8), ("pretty_powder", u8), ("_pad0", u8),
+        ("edge_mode", u32), ("gravity_mode", u32), ("air_mode", u32), ("ambient_air_temp", f32),
+        ("edge_pressure", f32), ("display_mode", u32), ("colour_mode", u32), ("render_mode", u32),
+        ("fire_intensity", f32), ("heat_enable", u8), ("newton_grav", u8), ("water_equal_test", u8), ("_pad1", u8),
+        ("vorticity_coeff", f32), ("convection_mode", u32), ("edge_velocity_x", f32), ("edge_velocity_y", f32),
+        ("custom_gravity_x", f32), ("custom_gravity_y", f32), ("temperature_scale", u32), ("decorations", u8),
+        ("_pad2", u8 * 3), ("mouse_x", i32), ("mouse_y", i32), ("gravity_field_enabled", u8),
+        ("gravity_zones_enabled", u8), ("grid", u8), ("_pad3", u8), ("grid_size", i32), ("grid_checkerboard", u8),
+        ("hud", u8), ("debug_hud", u8), ("show_brush", u8), ("zoom_enabled", u8), ("_pad4", u8 * 3),
+        ("zoom_window_x", i32), ("zoom_window_y", i32), ("zoom_factor", i32), ("zoom_scope_x", i32),
+        ("zoom_scope_y", i32), ("zoom_scope_size", i32), ("has_heat_display_limit_min", u8),
+        ("has_heat_display_limit_max", u8), ("_pad5", u8 * 2), ("heat_display_limit_min", f32),
+        ("heat_display_limit_max", f32), ("heat_display_auto_x", i32), ("heat_display_auto_y", i32),
+        ("heat_display_auto_w", i32), ("heat_display_auto_h", i32),
+    ]
+
+
+class SaveInfo(ctypes.Structure):
+    _fields_ = [("version", ctypes.c_uint32), ("xcells", ctypes.c_uint32), ("ycells", ctypes.c_uint32),
+                ("n_particles", ctypes.c_uint64), ("n_rigid_bodies", ctypes.c_uint64), ("n_signs", ctypes.c_uint64),
+                ("grid_len", ctypes.c_uint64 * 8)]
+
+
 def build() -> None:
     """Compiles libtpt_field.so for sm_100a (nvcc cross-compiles without a GPU)."""
     subprocess.run(["make", "-s", "-j8", "-C", HERE], check=True)
@@ -177,6 +210,24 @@ def lib() -> ctypes.CDLL:
         L.tpt_vox_grav_clear_mass.argtypes = [P, W, P]
         L.tpt_vox_grav_gather.argtypes = [P, W, P]
         L.tpt_vox_field_step.argtypes = [P, W, u32, u32, P]
+        SC, S = ctypes.POINTER(SaveConfig), P
+        L.tpt_save_config_default.argtypes = [SC, u32, u32]
+        L.tpt_save_config_default.restype = None
+        L.tpt_save_create.argtypes = [SC, ctypes.POINTER(P)]
+        L.tpt_save_decode.argtypes = [P, ctypes.c_size_t, ctypes.POINTER(P)]
+        L.tpt_save_encode.argtypes = [S, ctypes.POINTER(P), ctypes.POINTER(ctypes.c_size_t)]
+        L.tpt_save_destroy.argtypes = [S]
+        L.tpt_save_get_info.argtypes = [S, ctypes.POINTER(SaveInfo)]
+        L.tpt_save_get_config.argtypes = [S, SC]
+        L.tpt_save_set_config.argtypes = [S, SC]
+        L.tpt_save_set_version.argtypes = [S, u32]
+        L.tpt_save_grid_read.argtypes = [S, i32, P, ctypes.c_size_t]
+        L.tpt_save_grid_write.argtypes = [S, i32, P, ctypes.c_size_t]
+        L.tpt_save_grid_restore.argtypes = [S, i32, P, ctypes.c_uint64]
+        L.tpt_save_particles_read.argtypes = [S, P, ctypes.c_size_t]
+        L.tpt_save_particles_write.argtypes = [S, P, ctypes.c_size_t]
+        L.tpt_save_retain_air_pressure.argtypes = [S, i32]
+        L.tpt_save_instance_desc.argtypes = [S, ctypes.POINTER(InstanceDesc)]
         L.tpt_last_error_string.restype = ctypes.c_char_p
         L.tpt_kernel_launch_count.restype = ctypes.c_uint64
         L.tpt_version.restype = ctypes.c_char_p
@@ -529,6 +580,146 @@ class Batch:
     def close(self):
         if self._h:
             lib().tpt_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------ save files --
+
+class SaveData:
+    """A `.tptrs` save (crates/tpt-save/src/lib.rs:67-97), decoded and encoded by
+    the library on the host: `SaveData.from_bytes` / `to_bytes` mirror the
+    reference's calls, `grid(name)` / `set_grid(name, array)` give the eight
+    cell grids (names in SAVE_GRIDS), `particles()` the raw 64-byte records
+    (numpy uint32, 16 words each), `instance_desc()` the field-step
+    configuration restore_into gives the engine, `restore_grid(name)` the
+    grid restore_into loads (zeros on a cell-count mismatch)."""
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self._h = handle
+
+    @classmethod
+    def from_bytes(cls, data: bytes) -> "SaveData":
+        h = ctypes.c_void_p()
+        buf = ctypes.create_string_buffer(bytes(data), len(data))
+        check(lib().tpt_save_decode(buf, len(data), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def new(cls, xres: int, yres: int) -> "SaveData":
+        """An empty version-2 save of SimulationConfig::new(xres, yres)."""
+        c = SaveConfig()
+        lib().tpt_save_config_default(ctypes.byref(c), xres, yres)
+        h = ctypes.c_void_p()
+        check(lib().tpt_save_create(ctypes.byref(c), ctypes.byref(h)))
+        return cls(h)
+
+    def to_bytes(self) -> bytes:
+        p, n = ctypes.c_void_p(), ctypes.c_size_t()
+        check(lib().tpt_save_encode(self._h, ctypes.byref(p), ctypes.byref(n)))
+        return ctypes.string_at(p, n.value)
+
+    def info(self) -> SaveInfo:
+        out = SaveInfo()
+        check(lib().tpt_save_get_info(self._h, ctypes.byref(out)))
+        return out
+
+    @property
+    def version(self) -> int:
+        return int(self.info().version)
+
+    @version.setter
+    def version(self, v: int) -> None:
+        check(lib().tpt_save_set_version(self._h, int(v)))
+
+    @property
+    def config(self) -> SaveConfig:
+        c = SaveConfig()
+        check(lib().tpt_save_get_config(self._h, ctypes.byref(c)))
+        return c
+
+    @config.setter
+    def config(self, c: SaveConfig) -> None:
+        check(lib().tpt_save_set_config(self._h, ctypes.byref(c)))
+
+    def grid(self, name: str) -> np.ndarray:
+        g = SAVE_GRIDS.index(name)
+        out = np.empty(int(self.info().grid_len[g]), np.uint32 if name.startswith("wall") else np.float32)
+        check(lib().tpt_save_grid_read(self._h, g, _ptr(out), out.nbytes))
+        return out
+
+    def set_grid(self, name: str, values) -> None:
+        a = np.ascontiguousarray(values, np.uint32 if name.startswith("wall") else np.float32)
+        check(lib().tpt_save_grid_write(self._h, SAVE_GRIDS.index(name), _ptr(a), a.nbytes))
+
+    def restore_grid(self, name: str) -> np.ndarray:
+        d = self.instance_desc()
+        out = np.empty(d.air.xcells * d.air.ycells, np.uint32 if name.startswith("wall") else np.float32)
+        check(lib().tpt_save_grid_restore(self._h, SAVE_GRIDS.index(name), _ptr(out), out.size))
+        return out
+
+    def particles(self) -> np.ndarray:
+        n = int(self.info().n_particles)
+        out = np.empty((n, 16), np.uint32)
+        check(lib().tpt_save_particles_read(self._h, _ptr(out), out.nbytes))
+        return out
+
+    def set_particles(self, records) -> None:
+        a = np.ascontiguousarray(records, np.uint32).reshape(-1, 16)
+        check(lib().tpt_save_particles_write(self._h, _ptr(a), a.nbytes))
+
+    def retain_air_pressure(self, include: bool) -> "SaveData":
+        check(lib().tpt_save_retain_air_pressure(self._h, int(bool(include))))
+        return self
+
+    def instance_desc(self) -> InstanceDesc:
+        d = InstanceDesc()
+        check(lib().tpt_save_instance_desc(self._h, ctypes.byref(d)))
+        return d
+
+    def to_instance(self):
+        """The field-step state SaveData::restore_into gives the engine
+        (lib.rs:262-345), as a workloads.Instance for SimBuffers.from_instance
+        or Batch: the restored configuration, the eight grids fitted to the
+        canvas, the wall masks rebuilt from the walls (rebuild_spatial_maps)
+        and the gravity mask flood-filled from them; no element stamps and no
+        mass (particles are outside the field step)."""
+        import workloads as W
+
+        d = self.instance_desc()
+        a = d.air
+        cfg = W.AirConfig(air_mode=a.air_mode, aheat_enable=a.aheat_enable, convection_mode=a.convection_mode,
+                          gravity_mode=a.gravity_mode, edge_pressure=a.edge_pressure, edge_vx=a.edge_vx,
+                          edge_vy=a.edge_vy, ambient_air_temp=a.ambient_air_temp,
+                          vorticity_coeff=a.vorticity_coeff, custom_gx=a.custom_gx, custom_gy=a.custom_gy,
+                          newton_grav=d.newton_grav)
+        g = {n: self.restore_grid(n) for n in SAVE_GRIDS}
+        X, Y = int(a.xcells), int(a.ycells)
+        bair, bairh = W.wall_masks(g["wall_bmap"], g["wall_emap"])
+        zero = np.zeros(X * Y, np.uint32)
+        return W.Instance(X, Y, cfg, pv=g["air_pv"], vx=g["air_vx"], vy=g["air_vy"], hv=g["air_hv"],
+                          wall=g["wall_bmap"], emap=g["wall_emap"], bair=bair, bairh=bairh, eair=zero,
+                          eairh=zero.copy(), fan_vx=g["fan_vx"], fan_vy=g["fan_vy"],
+                          mass_fx=np.zeros(X * Y, np.int32), gmask=W.grav_mask(g["wall_bmap"], X, Y))
+
+    def set_field_state(self, state: dict) -> None:
+        """Writes air state back into the save's grids: `state` maps pv, vx,
+        vy, hv (and optionally wall, emap) to dense cell arrays, as
+        SimBuffers.air_state() or Batch.state() return them."""
+        names = {"pv": "air_pv", "vx": "air_vx", "vy": "air_vy", "hv": "air_hv", "wall": "wall_bmap",
+                 "emap": "wall_emap", "fan_vx": "fan_vx", "fan_vy": "fan_vy"}
+        for k, v in state.items():
+            if k in names:
+                self.set_grid(names[k], v)
+
+    def close(self) -> None:
+        if self._h:
+            lib().tpt_save_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):
