@@ -576,6 +576,73 @@ int tpt_save_retain_air_pressure(tpt_save *s, int include);
  * the other air fields and newton_grav at their defaults. */
 int tpt_save_instance_desc(const tpt_save *s, tpt_instance_desc *out);
 
+/* ---- 3-D save files (crates/tpt-save/src/voxel3d.rs) -------------------
+ *
+ * A `.tpt3` file is the magic "TPT3RS01" followed by
+ * zlib(bincode(Voxel3dSaveData)) (voxel3d.rs:1-15, 216-276), the same
+ * bincode 1.3.3 encoding as `.tptrs`. Voxel3dSaveData (voxel3d.rs:63-90) is
+ * version 4: the Voxel3dConfig, the voxel words, the four per-voxel
+ * auxiliary arrays (each empty or TPT_VOX_VOXELS long), the coarse air grid
+ * (empty or a multiple of TPT_VOX_CELLS floats: vx | vy | vz | pv | t |
+ * solid, pv in pressure units) and the rigid bodies (kept as read).
+ */
+typedef struct tpt_vox_save tpt_vox_save;
+
+/* Voxel3dConfig (crates/tpt-core/src/voxel3d/mod.rs:96-122), serialised
+ * fields in order. */
+typedef struct tpt_vox_save_config {
+    uint32_t dim;
+    uint8_t paused, _pad0[3];
+    float ambient_temp_k;
+    float gravity[3];
+    uint32_t edge_mode;      /* EdgeMode: 0 void, 1 solid, 2 loop */
+    uint8_t air_enabled, _pad1[3];
+    uint32_t air_iterations;
+    float sun_dir[3];
+    float exposure, render_scale;
+    uint32_t ao_rays;
+    uint8_t shadows, _pad2[3];
+} tpt_vox_save_config;
+
+/* The arrays of a 3-D save, in Voxel3dSaveData order. */
+enum {
+    TPT_VOX_SAVE_VOXELS = 0, TPT_VOX_SAVE_CTYPE, TPT_VOX_SAVE_TMP, TPT_VOX_SAVE_TMP2,
+    TPT_VOX_SAVE_TMP3, TPT_VOX_SAVE_AIR, TPT_VOX_SAVE_ARRAYS
+};
+enum { TPT_VOX_SAVE_VERSION = 4, TPT_VOX_MAX_BODIES = 64, TPT_VOX_BODY_VOXELS = 32768 };
+
+typedef struct tpt_vox_save_info {
+    uint32_t version;
+    uint64_t len[TPT_VOX_SAVE_ARRAYS]; /* elements of each array        */
+    uint64_t n_bodies;
+} tpt_vox_save_info;
+
+/* Voxel3dConfig::default (mod.rs:124-141). */
+void tpt_vox_save_config_default(tpt_vox_save_config *c);
+/* Voxel3dSaveData::empty (voxel3d.rs:147-152): zeroed voxels, no air,
+ * no auxiliary arrays, no bodies. */
+int tpt_vox_save_create(const tpt_vox_save_config *config, tpt_vox_save **out);
+/* Voxel3dSaveData::from_bytes (voxel3d.rs:234-253) and its layout checks
+ * (validate, :155-214); every malformed input is TPT_ERR_INVALID_ARG. */
+int tpt_vox_save_decode(const void *bytes, size_t len, tpt_vox_save **out);
+/* Voxel3dSaveData::to_bytes (voxel3d.rs:216-231): the layout is checked
+ * first. `*bytes` belongs to the save until the next encode or destroy. */
+int tpt_vox_save_encode(tpt_vox_save *s, const void **bytes, size_t *len);
+int tpt_vox_save_destroy(tpt_vox_save *s);
+int tpt_vox_save_get_info(const tpt_vox_save *s, tpt_vox_save_info *out);
+int tpt_vox_save_get_config(const tpt_vox_save *s, tpt_vox_save_config *out);
+int tpt_vox_save_set_config(tpt_vox_save *s, const tpt_vox_save_config *config);
+/* An array as stored (`bytes` = len * 4) / replaced (any multiple of 4). */
+int tpt_vox_save_array_read(const tpt_vox_save *s, int array, void *host, size_t bytes);
+int tpt_vox_save_array_write(tpt_vox_save *s, int array, const void *host, size_t bytes);
+/* The air state Voxel3dEngine::load_world gives the AirState
+ * (crates/tpt-sim/src/voxel3d/engine.rs:546-581): from the first six air
+ * slots, pv converted to 1/1024 fixed point ((value * 1024) as i32); with no
+ * air in the save, the cleared state (zero velocity, pv and solid, 293.15 K).
+ * Host arrays of TPT_VOX_CELLS elements each. */
+int tpt_vox_save_restore_air(const tpt_vox_save *s, float *vx, float *vy, float *vz, int32_t *pv, float *temp,
+                             float *solid);
+
 /* ---- diagnostics ------------------------------------------------------- */
 
 /*

@@ -2,7 +2,7 @@
 crates/tpt-save/src/lib.rs) decoded, restored the way SaveData::restore_into
 restores it (lib.rs:262-345), stepped on the GPU as one grid and inside a
 batch, bit-exact against the FP32 oracle from the same restored state, and
-written back into the save."""
+written back into the save; and a `.tpt3` file seeding the 3-D field step."""
 import numpy as np
 import pytest
 
@@ -57,3 +57,34 @@ def test_saves_seed_a_batch_and_are_written_back(cuda, tf, oracle):
         np.testing.assert_array_equal(back.grid("air_pv").view(np.uint32), got["pv"].view(np.uint32))
         np.testing.assert_array_equal(back.grid("wall_emap"), got["emap"])
     batch.close()
+
+
+def test_tpt3_save_seeds_the_3d_field_step(cuda, tf, oracle):
+    """A `.tpt3` world (crates/tpt-save/src/voxel3d.rs) written the way the
+    engine saves it (read_air_fields, engine.rs:391-430: pv in pressure
+    units), decoded, restored as load_world restores it and stepped one
+    tick, bit-exact against the oracle from the same restored state."""
+    import voxel3d as V
+    import workloads as W
+
+    w = W.voxel_world(0x3D33, active=0.5)
+    s = tf.VoxSave.new()
+    s.set_array("voxels", w["voxel"])
+    s.set_array("aux_tmp", w["aux_tmp"])
+    s.set_array("air", np.concatenate([w["vx"], w["vy"], w["vz"], w["pv"].astype(np.float32) / np.float32(1024.0),
+                                       w["temp"], w["solid"]]))
+    d = tf.VoxSave.from_bytes(s.to_bytes()).to_world()
+    np.testing.assert_array_equal(d["pv"], w["pv"])  # the fixed-point round trip is exact
+    assert d["sim_count"][0] > 0
+    bufs, air = V.upload(d)
+    plan = V.Plan()
+    V.field_step(plan, [(bufs, air)], 12)
+    V.gravity_gather(plan, bufs)
+    cuda.cuda.synchronize()
+    want = {k: v.copy() for k, v in d.items()}
+    oracle.vox_field_step(want, 12)
+    oracle.vox_grav_gather(want)
+    got = V.download(bufs, air)
+    for k in ("pv", "p", "p_tmp", "vx", "vy", "vz", "solid", "temp", "grav_mass", "grav_potential", "grav_force_z"):
+        assert np.array_equal(np.ascontiguousarray(got[k]).view(np.uint32),
+                              np.ascontiguousarray(want[k]).view(np.uint32)), k

@@ -310,6 +310,46 @@ bool get_raw_vec(Reader &r, std::vector<uint8_t> &raw, uint64_t &count, size_t m
     return true;
 }
 
+// The zlib stream after an 8-byte magic, inflated to its end (a stream cut
+// short is an error; bytes after its end are ignored, as flate2 does).
+int inflate_after_magic(const void *bytes, size_t len, const char *magic, const char *what,
+                        std::vector<uint8_t> &payload) {
+    const uint8_t *b = (const uint8_t *)bytes;
+    if (len <= 8) TPT_FAIL(TPT_ERR_INVALID_ARG, "%s is too short to contain a header", what);
+    if (memcmp(b, magic, 8) != 0) TPT_FAIL(TPT_ERR_INVALID_ARG, "not a %s: bad magic header", what);
+    z_stream zs{};
+    if (inflateInit(&zs) != Z_OK) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "zlib inflateInit failed");
+    zs.next_in = const_cast<Bytef *>(b + 8);
+    zs.avail_in = (uInt)(len - 8 > 0xFFFFFFFFu ? 0xFFFFFFFFu : len - 8);
+    int zr = Z_OK;
+    std::vector<uint8_t> chunk(1 << 20);
+    while (zr == Z_OK) {
+        zs.next_out = chunk.data();
+        zs.avail_out = (uInt)chunk.size();
+        zr = inflate(&zs, Z_NO_FLUSH);
+        if (zr != Z_OK && zr != Z_STREAM_END) break;
+        payload.insert(payload.end(), chunk.data(), chunk.data() + (chunk.size() - zs.avail_out));
+        if (zr == Z_OK && zs.avail_in == 0 && zs.avail_out != 0) {
+            zr = Z_BUF_ERROR;  // input ended inside the stream
+            break;
+        }
+    }
+    inflateEnd(&zs);
+    if (zr != Z_STREAM_END) TPT_FAIL(TPT_ERR_INVALID_ARG, "failed to decompress %s (zlib %d)", what, zr);
+    return TPT_OK;
+}
+
+// magic + zlib(payload) at the default level into `out`.
+int deflate_with_magic(const std::vector<uint8_t> &payload, const char *magic, std::vector<uint8_t> &out) {
+    uLongf cap = compressBound((uLong)payload.size());
+    out.resize(8 + (size_t)cap);
+    memcpy(out.data(), magic, 8);
+    if (compress2(out.data() + 8, &cap, payload.data(), (uLong)payload.size(), Z_DEFAULT_COMPRESSION) != Z_OK)
+        TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "failed to compress save data");
+    out.resize(8 + (size_t)cap);
+    return TPT_OK;
+}
+
 int decode_payload(const uint8_t *p, size_t n, tpt_save &s) {
     Reader r{p, n};
     r.u32(s.version);  // the version probe (SaveDataVersion, lib.rs:124-128)
@@ -390,34 +430,12 @@ int tpt_save_decode(const void *bytes, size_t len, tpt_save **out) {
     if (!out) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_save_decode: out is NULL");
     *out = nullptr;
     if (!bytes && len) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_save_decode: bytes is NULL");
-    const uint8_t *b = (const uint8_t *)bytes;
-    if (len <= 8) TPT_FAIL(TPT_ERR_INVALID_ARG, "save data is too short to contain a header");
-    if (memcmp(b, "TPTRS001", 8) != 0)
-        TPT_FAIL(TPT_ERR_INVALID_ARG, "not a Powder Toy (Rust) save file: bad magic header");
-    // zlib stream to its end
     std::vector<uint8_t> payload;
-    z_stream zs{};
-    if (inflateInit(&zs) != Z_OK) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "zlib inflateInit failed");
-    zs.next_in = const_cast<Bytef *>(b + 8);
-    zs.avail_in = (uInt)(len - 8 > 0xFFFFFFFFu ? 0xFFFFFFFFu : len - 8);
-    int zr = Z_OK;
-    uint8_t chunk[1 << 16];
-    while (zr == Z_OK) {
-        zs.next_out = chunk;
-        zs.avail_out = sizeof(chunk);
-        zr = inflate(&zs, Z_NO_FLUSH);
-        if (zr != Z_OK && zr != Z_STREAM_END) break;
-        payload.insert(payload.end(), chunk, chunk + (sizeof(chunk) - zs.avail_out));
-        if (zr == Z_OK && zs.avail_in == 0 && zs.avail_out != 0) {
-            zr = Z_BUF_ERROR;  // input ended inside the stream
-            break;
-        }
-    }
-    inflateEnd(&zs);
-    if (zr != Z_STREAM_END) TPT_FAIL(TPT_ERR_INVALID_ARG, "failed to decompress save data (zlib %d)", zr);
+    int rc = inflate_after_magic(bytes, len, "TPTRS001", "Powder Toy (Rust) save file", payload);
+    if (rc) return rc;
     tpt_save *s = new (std::nothrow) tpt_save();
     if (!s) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "host allocation failed");
-    const int rc = decode_payload(payload.data(), payload.size(), *s);
+    rc = decode_payload(payload.data(), payload.size(), *s);
     if (rc) {
         delete s;
         return rc;
@@ -441,12 +459,8 @@ int tpt_save_encode(tpt_save *s, const void **bytes, size_t *len) {
     w.bytes(s->rigid.data(), s->rigid.size());
     w.u64(s->n_signs);
     w.bytes(s->signs.data(), s->signs.size());
-    uLongf cap = compressBound((uLong)w.b.size());
-    s->encoded.resize(8 + (size_t)cap);
-    memcpy(s->encoded.data(), "TPTRS001", 8);
-    if (compress2(s->encoded.data() + 8, &cap, w.b.data(), (uLong)w.b.size(), Z_DEFAULT_COMPRESSION) != Z_OK)
-        TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "failed to compress save data");
-    s->encoded.resize(8 + (size_t)cap);
+    const int rc = deflate_with_magic(w.b, "TPTRS001", s->encoded);
+    if (rc) return rc;
     *bytes = s->encoded.data();
     *len = s->encoded.size();
     return TPT_OK;
@@ -565,6 +579,264 @@ int tpt_save_instance_desc(const tpt_save *s, tpt_instance_desc *out) {
     a.custom_gx = c.custom_gravity_x;
     a.custom_gy = c.custom_gravity_y;
     out->newton_grav = c.newton_grav;
+    return TPT_OK;
+}
+
+}  // extern "C"
+
+// ============================================================ .tpt3 ====
+// The 3-D sandbox's saves (crates/tpt-save/src/voxel3d.rs): "TPT3RS01" +
+// zlib(bincode(Voxel3dSaveData)), version 4 only.
+
+struct tpt_vox_save {
+    uint32_t version = TPT_VOX_SAVE_VERSION;
+    tpt_vox_save_config config{};
+    std::vector<uint32_t> arr[TPT_VOX_SAVE_ARRAYS];  // voxels, ctype, tmp, tmp2, tmp3 (words), air (f32 bits)
+    std::vector<uint8_t> bodies;                      // the encoded Voxel3dBodySave elements, kept as read
+    uint64_t n_bodies = 0;
+    std::vector<uint8_t> encoded;
+};
+
+namespace {
+
+// Voxel3dConfig (crates/tpt-core/src/voxel3d/mod.rs:96-122); fixed-size
+// arrays are their elements in order.
+void put_vox_config(Writer &w, const tpt_vox_save_config &c) {
+    w.u32(c.dim);
+    w.boolean(c.paused);
+    w.f32(c.ambient_temp_k);
+    for (float g : c.gravity) w.f32(g);
+    w.u32(c.edge_mode);
+    w.boolean(c.air_enabled);
+    w.u32(c.air_iterations);
+    for (float d : c.sun_dir) w.f32(d);
+    w.f32(c.exposure);
+    w.f32(c.render_scale);
+    w.u32(c.ao_rays);
+    w.boolean(c.shadows);
+}
+
+bool get_vox_config(Reader &r, tpt_vox_save_config &c) {
+    c = tpt_vox_save_config{};
+    r.u32(c.dim);
+    r.boolean(c.paused);
+    r.f32(c.ambient_temp_k);
+    for (float &g : c.gravity) r.f32(g);
+    r.variant(c.edge_mode, 3);
+    r.boolean(c.air_enabled);
+    r.u32(c.air_iterations);
+    for (float &d : c.sun_dir) r.f32(d);
+    r.f32(c.exposure);
+    r.f32(c.render_scale);
+    r.u32(c.ao_rays);
+    r.boolean(c.shadows);
+    return !r.err;
+}
+
+// One Voxel3dBodySave (voxel3d.rs:42-57): 16 floats, ty, Vec<u32>.
+bool skip_body(Reader &r) {
+    uint32_t u;
+    for (int k = 0; k < 17; ++k) r.u32(u);
+    uint64_t n;
+    if (!r.count(n, 4)) return false;
+    for (uint64_t k = 0; k < n; ++k) r.u32(u);
+    return !r.err;
+}
+
+// Voxel3dSaveData::validate (voxel3d.rs:155-214), the reference's messages.
+int vox_validate(const tpt_vox_save &s) {
+    if (s.version != TPT_VOX_SAVE_VERSION)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "unsupported voxel save version %u (this build supports %u)", s.version,
+                 (unsigned)TPT_VOX_SAVE_VERSION);
+    if (s.arr[TPT_VOX_SAVE_VOXELS].size() != (size_t)TPT_VOX_VOXELS)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "voxel save holds %zu voxels, expected %u", s.arr[TPT_VOX_SAVE_VOXELS].size(),
+                 (unsigned)TPT_VOX_VOXELS);
+    const char *names[] = {"ctype", "tmp", "tmp2", "tmp3"};
+    for (int a = TPT_VOX_SAVE_CTYPE; a <= TPT_VOX_SAVE_TMP3; ++a) {
+        const size_t n = s.arr[a].size();
+        if (n != 0 && n != (size_t)TPT_VOX_VOXELS)
+            TPT_FAIL(TPT_ERR_INVALID_ARG, "voxel save holds %zu %s words, expected 0 or %u", n, names[a - 1],
+                     (unsigned)TPT_VOX_VOXELS);
+    }
+    if (s.arr[TPT_VOX_SAVE_AIR].size() % (size_t)TPT_VOX_CELLS)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "voxel save air grid has %zu cells, expected a multiple of %u",
+                 s.arr[TPT_VOX_SAVE_AIR].size(), (unsigned)TPT_VOX_CELLS);
+    if (s.n_bodies > (uint64_t)TPT_VOX_MAX_BODIES)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "voxel save holds %llu rigid bodies, at most %u are supported",
+                 (unsigned long long)s.n_bodies, (unsigned)TPT_VOX_MAX_BODIES);
+    Reader r{s.bodies.data(), s.bodies.size()};
+    for (uint64_t b = 0; b < s.n_bodies; ++b) {
+        uint32_t u;
+        for (int k = 0; k < 17; ++k) r.u32(u);
+        uint64_t n = 0;
+        r.u64(n);
+        if (n > (uint64_t)TPT_VOX_BODY_VOXELS)
+            TPT_FAIL(TPT_ERR_INVALID_ARG, "rigid body %llu local grid holds %llu voxels, at most %u are supported",
+                     (unsigned long long)b, (unsigned long long)n, (unsigned)TPT_VOX_BODY_VOXELS);
+        r.i += (size_t)n * 4;
+    }
+    return TPT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void tpt_vox_save_config_default(tpt_vox_save_config *c) {
+    if (!c) return;
+    *c = tpt_vox_save_config{};
+    c->dim = 256;  // VOXEL_DIM
+    c->ambient_temp_k = 293.15f;
+    c->gravity[1] = -9.81f;
+    c->air_enabled = 1;
+    c->air_iterations = 12;
+    c->sun_dir[0] = 0.5f;
+    c->sun_dir[1] = 0.70710677f;
+    c->sun_dir[2] = 0.5f;
+    c->exposure = 1.0f;
+    c->render_scale = 1.0f;
+    c->ao_rays = 2;
+    c->shadows = 1;
+}
+
+int tpt_vox_save_create(const tpt_vox_save_config *config, tpt_vox_save **out) {
+    if (!config || !out) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_create: NULL argument");
+    *out = nullptr;
+    if (config->edge_mode > 2u) TPT_FAIL(TPT_ERR_INVALID_ARG, "tpt_vox_save_create: edge_mode out of range");
+    tpt_vox_save *s = new (std::nothrow) tpt_vox_save();
+    if (!s) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "host allocation failed");
+    s->config = *config;
+    s->arr[TPT_VOX_SAVE_VOXELS].assign((size_t)TPT_VOX_VOXELS, 0u);
+    *out = s;
+    return TPT_OK;
+}
+
+int tpt_vox_save_decode(const void *bytes, size_t len, tpt_vox_save **out) {
+    if (!out) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_decode: out is NULL");
+    *out = nullptr;
+    if (!bytes && len) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_decode: bytes is NULL");
+    std::vector<uint8_t> payload;
+    int rc = inflate_after_magic(bytes, len, "TPT3RS01", "Powder Toy 3D voxel save", payload);
+    if (rc) return rc;
+    tpt_vox_save *s = new (std::nothrow) tpt_vox_save();
+    if (!s) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "host allocation failed");
+    Reader r{payload.data(), payload.size()};
+    r.u32(s->version);
+    get_vox_config(r, s->config);
+    for (auto &a : s->arr) get_words(r, a);
+    if (!r.err) get_raw_vec(r, s->bodies, s->n_bodies, 76, skip_body);
+    if (r.err) {
+        delete s;
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "failed to deserialize voxel save data: %s", r.err);
+    }
+    rc = vox_validate(*s);
+    if (rc) {
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return TPT_OK;
+}
+
+int tpt_vox_save_encode(tpt_vox_save *s, const void **bytes, size_t *len) {
+    if (!s || !bytes || !len) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_encode: NULL argument");
+    int rc = vox_validate(*s);
+    if (rc) return rc;
+    Writer w;
+    w.u32(s->version);
+    put_vox_config(w, s->config);
+    for (const auto &a : s->arr) {
+        w.u64(a.size());
+        w.bytes(a.data(), a.size() * 4);  // little-endian words, the host's order
+    }
+    w.u64(s->n_bodies);
+    w.bytes(s->bodies.data(), s->bodies.size());
+    rc = deflate_with_magic(w.b, "TPT3RS01", s->encoded);
+    if (rc) return rc;
+    *bytes = s->encoded.data();
+    *len = s->encoded.size();
+    return TPT_OK;
+}
+
+int tpt_vox_save_destroy(tpt_vox_save *s) {
+    delete s;
+    return TPT_OK;
+}
+
+int tpt_vox_save_get_info(const tpt_vox_save *s, tpt_vox_save_info *out) {
+    if (!s || !out) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_get_info: NULL argument");
+    *out = tpt_vox_save_info{};
+    out->version = s->version;
+    for (int a = 0; a < TPT_VOX_SAVE_ARRAYS; ++a) out->len[a] = s->arr[a].size();
+    out->n_bodies = s->n_bodies;
+    return TPT_OK;
+}
+
+int tpt_vox_save_get_config(const tpt_vox_save *s, tpt_vox_save_config *out) {
+    if (!s || !out) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_get_config: NULL argument");
+    *out = s->config;
+    return TPT_OK;
+}
+
+int tpt_vox_save_set_config(tpt_vox_save *s, const tpt_vox_save_config *c) {
+    if (!s || !c) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_set_config: NULL argument");
+    if (c->edge_mode > 2u) TPT_FAIL(TPT_ERR_INVALID_ARG, "tpt_vox_save_set_config: edge_mode out of range");
+    s->config = *c;
+    return TPT_OK;
+}
+
+int tpt_vox_save_array_read(const tpt_vox_save *s, int array, void *host, size_t bytes) {
+    if (!s) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_array_read: save is NULL");
+    if (array < 0 || array >= TPT_VOX_SAVE_ARRAYS) TPT_FAIL(TPT_ERR_INVALID_ARG, "unknown voxel save array %d", array);
+    const auto &a = s->arr[array];
+    if (bytes != a.size() * 4)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "array %d holds %zu bytes, not %zu", array, a.size() * 4, bytes);
+    if (bytes && !host) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_array_read: host is NULL");
+    if (bytes) memcpy(host, a.data(), bytes);
+    return TPT_OK;
+}
+
+int tpt_vox_save_array_write(tpt_vox_save *s, int array, const void *host, size_t bytes) {
+    if (!s) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_array_write: save is NULL");
+    if (array < 0 || array >= TPT_VOX_SAVE_ARRAYS) TPT_FAIL(TPT_ERR_INVALID_ARG, "unknown voxel save array %d", array);
+    if (bytes % 4) TPT_FAIL(TPT_ERR_INVALID_ARG, "array bytes %zu is not a multiple of 4", bytes);
+    if (bytes && !host) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_array_write: host is NULL");
+    auto &a = s->arr[array];
+    a.resize(bytes / 4);
+    if (bytes) memcpy(a.data(), host, bytes);
+    return TPT_OK;
+}
+
+int tpt_vox_save_restore_air(const tpt_vox_save *s, float *vx, float *vy, float *vz, int32_t *pv, float *temp,
+                             float *solid) {
+    if (!s || !vx || !vy || !vz || !pv || !temp || !solid)
+        TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_vox_save_restore_air: NULL argument");
+    const size_t c = (size_t)TPT_VOX_CELLS;
+    const auto &air = s->arr[TPT_VOX_SAVE_AIR];
+    if (air.empty()) {  // AirState::new (air.rs:93-123)
+        for (size_t i = 0; i < c; ++i) {
+            vx[i] = vy[i] = vz[i] = solid[i] = 0.0f;
+            pv[i] = 0;
+            temp[i] = 293.15f;
+        }
+        return TPT_OK;
+    }
+    if (air.size() != 6 * c)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "voxel3d: expected 0 or %zu air floats, got %zu", 6 * c, air.size());
+    float *dst[6] = {vx, vy, vz, nullptr, temp, solid};
+    for (int f = 0; f < 6; ++f) {
+        const uint32_t *src = air.data() + (size_t)f * c;
+        if (f != 3) {
+            memcpy(dst[f], src, c * 4);
+            continue;
+        }
+        for (size_t i = 0; i < c; ++i) {  // (value * PV_SCALE) as i32, saturating, NaN -> 0
+            float v;
+            memcpy(&v, &src[i], 4);
+            const float q = v * 1024.0f;
+            pv[i] = q != q ? 0 : q >= 2147483648.0f ? INT32_MAX : q < -2147483648.0f ? INT32_MIN : (int32_t)q;
+        }
+    }
     return TPT_OK;
 }
 

@@ -53,10 +53,14 @@ EXPORTS = [
     "tpt_save_create", "tpt_save_decode", "tpt_save_encode", "tpt_save_destroy", "tpt_save_get_info",
     "tpt_save_get_config", "tpt_save_set_config", "tpt_save_set_version", "tpt_save_grid_read",
     "tpt_save_grid_write", "tpt_save_grid_restore", "tpt_save_particles_read", "tpt_save_particles_write",
-    "tpt_save_retain_air_pressure", "tpt_save_instance_desc", "tpt_check_device_errors",
+    "tpt_save_retain_air_pressure", "tpt_save_instance_desc", "tpt_vox_save_config_default", "tpt_vox_save_create",
+    "tpt_vox_save_decode", "tpt_vox_save_encode", "tpt_vox_save_destroy", "tpt_vox_save_get_info",
+    "tpt_vox_save_get_config", "tpt_vox_save_set_config", "tpt_vox_save_array_read", "tpt_vox_save_array_write",
+    "tpt_vox_save_restore_air", "tpt_check_device_errors",
     "tpt_last_error_string", "tpt_kernel_launch_count", "tpt_version",
 ]
 SAVE_GRIDS = ("air_vx", "air_vy", "air_pv", "air_hv", "fan_vx", "fan_vy", "wall_bmap", "wall_emap")
+VOX_SAVE_ARRAYS = ("voxels", "aux_ctype", "aux_tmp", "aux_tmp2", "aux_tmp3", "air")
 VOX_AUTO, VOX_CLUSTER, VOX_PER_SWEEP, VOX_BATCHED = 0, 1, 2, 3
 
 
@@ -156,6 +160,20 @@ class SaveConfig(ctypes.Structure):
     ]
 
 
+class VoxSaveConfig(ctypes.Structure):
+    """tpt_vox_save_config: Voxel3dConfig's serialised fields, in order."""
+
+    u8, u32, f32 = ctypes.c_uint8, ctypes.c_uint32, ctypes.c_float
+    _fields_ = [("dim", u32), ("paused", u8), ("_pad0", u8 * 3), ("ambient_temp_k", f32), ("gravity", f32 * 3),
+                ("edge_mode", u32), ("air_enabled", u8), ("_pad1", u8 * 3), ("air_iterations", u32),
+                ("sun_dir", f32 * 3), ("exposure", f32), ("render_scale", f32), ("ao_rays", u32), ("shadows", u8),
+                ("_pad2", u8 * 3)]
+
+
+class VoxSaveInfo(ctypes.Structure):
+    _fields_ = [("version", ctypes.c_uint32), ("len", ctypes.c_uint64 * 6), ("n_bodies", ctypes.c_uint64)]
+
+
 class SaveInfo(ctypes.Structure):
     _fields_ = [("version", ctypes.c_uint32), ("xcells", ctypes.c_uint32), ("ycells", ctypes.c_uint32),
                 ("n_particles", ctypes.c_uint64), ("n_rigid_bodies", ctypes.c_uint64), ("n_signs", ctypes.c_uint64),
@@ -228,6 +246,19 @@ def lib() -> ctypes.CDLL:
         L.tpt_save_particles_write.argtypes = [S, P, ctypes.c_size_t]
         L.tpt_save_retain_air_pressure.argtypes = [S, i32]
         L.tpt_save_instance_desc.argtypes = [S, ctypes.POINTER(InstanceDesc)]
+        VC = ctypes.POINTER(VoxSaveConfig)
+        L.tpt_vox_save_config_default.argtypes = [VC]
+        L.tpt_vox_save_config_default.restype = None
+        L.tpt_vox_save_create.argtypes = [VC, ctypes.POINTER(P)]
+        L.tpt_vox_save_decode.argtypes = [P, ctypes.c_size_t, ctypes.POINTER(P)]
+        L.tpt_vox_save_encode.argtypes = [P, ctypes.POINTER(P), ctypes.POINTER(ctypes.c_size_t)]
+        L.tpt_vox_save_destroy.argtypes = [P]
+        L.tpt_vox_save_get_info.argtypes = [P, ctypes.POINTER(VoxSaveInfo)]
+        L.tpt_vox_save_get_config.argtypes = [P, VC]
+        L.tpt_vox_save_set_config.argtypes = [P, VC]
+        L.tpt_vox_save_array_read.argtypes = [P, i32, P, ctypes.c_size_t]
+        L.tpt_vox_save_array_write.argtypes = [P, i32, P, ctypes.c_size_t]
+        L.tpt_vox_save_restore_air.argtypes = [P] * 7
         L.tpt_last_error_string.restype = ctypes.c_char_p
         L.tpt_kernel_launch_count.restype = ctypes.c_uint64
         L.tpt_version.restype = ctypes.c_char_p
@@ -720,6 +751,107 @@ class SaveData:
     def close(self) -> None:
         if self._h:
             lib().tpt_save_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class VoxSave:
+    """A `.tpt3` 3-D save (crates/tpt-save/src/voxel3d.rs:63-90), decoded and
+    encoded by the library on the host. `array(name)` / `set_array(name, a)`
+    for the names in VOX_SAVE_ARRAYS (voxels and ctype as uint32, the tmp
+    arrays as int32, air as float32); `restore_air()` the AirState fields
+    Voxel3dEngine::load_world restores; `to_world()` a world dict (the keys
+    of workloads.voxel_world) for voxel3d.upload."""
+
+    _DT = {"voxels": np.uint32, "aux_ctype": np.uint32, "aux_tmp": np.int32, "aux_tmp2": np.int32,
+           "aux_tmp3": np.int32, "air": np.float32}
+
+    def __init__(self, handle: ctypes.c_void_p):
+        self._h = handle
+
+    @classmethod
+    def from_bytes(cls, data: bytes) -> "VoxSave":
+        h = ctypes.c_void_p()
+        buf = ctypes.create_string_buffer(bytes(data), len(data))
+        check(lib().tpt_vox_save_decode(buf, len(data), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def new(cls, config: VoxSaveConfig | None = None) -> "VoxSave":
+        """Voxel3dSaveData::empty of `config` (Voxel3dConfig::default if None)."""
+        if config is None:
+            config = VoxSaveConfig()
+            lib().tpt_vox_save_config_default(ctypes.byref(config))
+        h = ctypes.c_void_p()
+        check(lib().tpt_vox_save_create(ctypes.byref(config), ctypes.byref(h)))
+        return cls(h)
+
+    def to_bytes(self) -> bytes:
+        p, n = ctypes.c_void_p(), ctypes.c_size_t()
+        check(lib().tpt_vox_save_encode(self._h, ctypes.byref(p), ctypes.byref(n)))
+        return ctypes.string_at(p, n.value)
+
+    def info(self) -> VoxSaveInfo:
+        out = VoxSaveInfo()
+        check(lib().tpt_vox_save_get_info(self._h, ctypes.byref(out)))
+        return out
+
+    @property
+    def config(self) -> VoxSaveConfig:
+        c = VoxSaveConfig()
+        check(lib().tpt_vox_save_get_config(self._h, ctypes.byref(c)))
+        return c
+
+    @config.setter
+    def config(self, c: VoxSaveConfig) -> None:
+        check(lib().tpt_vox_save_set_config(self._h, ctypes.byref(c)))
+
+    def array(self, name: str) -> np.ndarray:
+        a = VOX_SAVE_ARRAYS.index(name)
+        out = np.empty(int(self.info().len[a]), self._DT[name])
+        check(lib().tpt_vox_save_array_read(self._h, a, _ptr(out), out.nbytes))
+        return out
+
+    def set_array(self, name: str, values) -> None:
+        a = np.ascontiguousarray(values, self._DT[name])
+        check(lib().tpt_vox_save_array_write(self._h, VOX_SAVE_ARRAYS.index(name), _ptr(a), a.nbytes))
+
+    def restore_air(self) -> dict:
+        n = 64 ** 3
+        out = {k: np.empty(n, np.float32) for k in ("vx", "vy", "vz", "temp", "solid")}
+        out["pv"] = np.empty(n, np.int32)
+        check(lib().tpt_vox_save_restore_air(self._h, *[_ptr(out[k]) for k in ("vx", "vy", "vz", "pv", "temp",
+                                                                              "solid")]))
+        return out
+
+    def to_world(self) -> dict:
+        """The field-step state of the loaded world: the voxels, aux_tmp (zeros
+        when absent), the restored air, a zero Jacobi pair and zero gravity
+        fields (load_world resets them), and as the brick list every brick
+        holding a non-empty voxel, in id order."""
+        n = 64 ** 3
+        vox = self.array("voxels")
+        tmp = self.array("aux_tmp")
+        if tmp.size == 0:
+            tmp = np.zeros(vox.size, np.int32)
+        occupied = ((vox & 0xFF) != 0).reshape(32, 8, 32, 8, 32, 8).any(axis=(1, 3, 5)).reshape(-1)
+        bricks = np.flatnonzero(occupied).astype(np.uint32)
+        w = {"voxel": vox, "aux_tmp": tmp, "sim_list": bricks,
+             "sim_count": np.array([bricks.size, 1, 1], np.uint32),
+             "p": np.zeros(n, np.float32), "p_tmp": np.zeros(n, np.float32), "grav_mass": np.zeros(n, np.int32)}
+        w.update(self.restore_air())
+        for k in ("grav_potential", "grav_potential_tmp", "grav_force_x", "grav_force_y", "grav_force_z"):
+            w[k] = np.zeros(n, np.float32)
+        return w
+
+    def close(self) -> None:
+        if self._h:
+            lib().tpt_vox_save_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):
