@@ -646,15 +646,13 @@ int launch_air_clear(const World &w, cudaStream_t st) {
     return TPT_OK;
 }
 
-// Persistent gather grid: 256-thread blocks, `per_sm` per SM.
+// Persistent gather grid: 256-thread blocks, `per_sm` per SM of the current
+// device (an attribute query, cheap next to the launch).
 static int gather_blocks(int per_sm) {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        if (cudaGetDevice(&dev) != cudaSuccess ||
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-            sms = 148;
-    }
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                  cudaSuccess || sms <= 0)
+        sms = 148;
     return sms * per_sm;
 }
 
