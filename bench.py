@@ -273,32 +273,27 @@ def run_ours(args, rank, world, local):
     ms = max_over_ranks(e0.elapsed_time(e1), world)
     value = job_cells * ticks * args.steps / (ms / 1e3)
 
-    # end to end through the C ABI with pinned host buffers
-    names = [n for n, _ in tf.Batch.GRIDS]
-    host_in = []
-    for inst in insts:
-        d = {}
-        for n, fid in tf.Batch.GRIDS:
-            a = getattr(inst, n)
-            t = torch.empty(a.size, dtype=torch.int32, pin_memory=True)
-            t.numpy().view(a.dtype)[:] = a
-            d[fid] = t.numpy().view(a.dtype)
-        host_in.append(d)
-    out_fields = [(tf.FIELD_PV, np.float32), (tf.FIELD_VX, np.float32), (tf.FIELD_VY, np.float32),
-                  (tf.FIELD_HV, np.float32), (tf.FIELD_GX, np.float32), (tf.FIELD_GY, np.float32)]
-    host_out = [{fid: torch.empty(i.cells, dtype=torch.float32, pin_memory=True).numpy() for fid, _ in out_fields}
-                for i in insts]
-    h2d = sum(a.nbytes for d in host_in for a in d.values())
-    d2h = sum(a.nbytes for d in host_out for a in d.values())
+    # end to end through the C ABI with pinned host buffers: each grid kind of
+    # every instance in one dense buffer (tpt_batch_write_field /
+    # tpt_batch_read_field)
+    total = batch.total_cells
+    host_in = {}
+    for n, fid in tf.Batch.GRIDS:
+        dt = getattr(insts[0], n).dtype
+        t = torch.empty(total, dtype=torch.int32, pin_memory=True)
+        t.numpy().view(dt)[:] = np.concatenate([getattr(inst, n).ravel() for inst in insts])
+        host_in[fid] = t.numpy().view(dt)
+    out_fields = (tf.FIELD_PV, tf.FIELD_VX, tf.FIELD_VY, tf.FIELD_HV, tf.FIELD_GX, tf.FIELD_GY)
+    host_out = {fid: torch.empty(total, dtype=torch.float32, pin_memory=True).numpy() for fid in out_fields}
+    h2d = sum(a.nbytes for a in host_in.values())
+    d2h = sum(a.nbytes for a in host_out.values())
 
     def e2e_step():
-        for i, d in enumerate(host_in):
-            for fid, a in d.items():
-                tf.check(tf.lib().tpt_batch_write(batch._h, i, fid, tf._ptr(a), a.nbytes, tf._stream(stream)))
+        for fid, a in host_in.items():
+            tf.check(tf.lib().tpt_batch_write_field(batch._h, fid, tf._ptr(a), a.nbytes, tf._stream(stream)))
         batch.step(ticks, stream)
-        for i, d in enumerate(host_out):
-            for fid, a in d.items():
-                tf.check(tf.lib().tpt_batch_read(batch._h, i, fid, tf._ptr(a), a.nbytes, tf._stream(stream)))
+        for fid, a in host_out.items():
+            tf.check(tf.lib().tpt_batch_read_field(batch._h, fid, tf._ptr(a), a.nbytes, tf._stream(stream)))
 
     e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
     e2e_value = None
@@ -363,7 +358,9 @@ def run_ours(args, rank, world, local):
                        "ticks_per_step": ticks, "l2": "working set > 126 MB L2, no flush",
                        "tuning": {"ctas_per_sm": batch.tuning().ctas_per_sm}},
             "e2e": {"value": e2e_value, "unit": "cell-ticks/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "steps": e2e_steps},
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                    "calls": f"tpt_batch_write_field x{len(host_in)}, tpt_batch_step, "
+                             f"tpt_batch_read_field x{len(host_out)} from/to pinned host buffers"},
             "gpu_launches": launches,
             "roofline": dominant,
             "roofline_phases": {"air": roof_air, "gravity": roof_grav, **phases},

@@ -321,6 +321,25 @@ int tpt_batch_write(tpt_batch *batch, uint32_t instance, int field,
 int tpt_batch_read(tpt_batch *batch, uint32_t instance, int field,
                    void *host, size_t bytes, tpt_stream_t stream);
 
+/*
+ * Host <-> device copy of one grid of EVERY instance at once: `host` holds
+ * the instances' dense grids back to back in instance order, and `bytes`
+ * must equal 4 * (sum of xcells*ycells). This is the bulk form of calling
+ * tpt_batch_write / tpt_batch_read for each instance (the reference's
+ * per-simulation `client.write` / `client.read`,
+ * crates/tpt-sim/src/buffers/gpu_sync.rs:186-197, 375-396); it makes one
+ * host copy and one device scatter or gather instead of one strided copy
+ * per instance. The first call allocates a device staging buffer of one grid
+ * of every instance, which later calls reuse: calls on one batch must be
+ * ordered (one stream, or the caller's events), as its steps are. Stream
+ * ordered; use pinned host memory for an asynchronous copy and synchronise
+ * the stream before touching `host` again.
+ */
+int tpt_batch_write_field(tpt_batch *batch, int field, const void *host,
+                          size_t bytes, tpt_stream_t stream);
+int tpt_batch_read_field(tpt_batch *batch, int field, void *host,
+                         size_t bytes, tpt_stream_t stream);
+
 /* Tuning knobs the autotuner picks (and a caller may pin). */
 typedef struct tpt_batch_tuning {
     uint32_t tile_x, tile_y;  /* air tile shape in cells                  */

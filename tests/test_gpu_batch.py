@@ -98,3 +98,48 @@ def test_batch_field_io_round_trip(cuda, tf):
     with pytest.raises(tf.TptError):
         b.write(0, 99, insts[0].pv)
     b.close()
+
+
+def test_batch_whole_field_io_matches_per_instance(cuda, tf):
+    """tpt_batch_write_field / tpt_batch_read_field against the per-instance
+    calls, on uneven grids (row lengths off the 32-element pitch)."""
+    insts = mixed_instances()
+    b = tf.Batch(insts)  # written through tpt_batch_write_field
+    for i, inst in enumerate(insts):
+        assert np.array_equal(b.read(i, tf.FIELD_PV, np.float32), inst.pv)
+        assert np.array_equal(b.read(i, tf.FIELD_WALL_EMAP, np.uint32), inst.emap)
+        assert np.array_equal(b.read(i, tf.FIELD_GRAV_MASS, np.int32), inst.mass_fx)
+    total = sum(i.cells for i in insts)
+    assert b.total_cells == total
+    rng = np.random.default_rng(5)
+    vals = rng.standard_normal(total).astype(np.float32)
+    b.write_field(tf.FIELD_VY, vals)
+    got = b.read_field(tf.FIELD_VY, np.float32)
+    assert np.array_equal(got, vals)
+    off = 0
+    for i, inst in enumerate(insts):
+        assert np.array_equal(b.read(i, tf.FIELD_VY, np.float32), vals[off:off + inst.cells])
+        off += inst.cells
+    for bad in (vals[:-1], np.zeros(total + 1, np.float32)):
+        with pytest.raises(tf.TptError, match="cells"):
+            b.write_field(tf.FIELD_VY, bad)
+    with pytest.raises(tf.TptError, match="field id"):
+        b.write_field(99, vals)
+    with pytest.raises(tf.TptError):
+        b.read_field(tf.FIELD_PV, np.float32, out=np.zeros(3, np.float32))
+    b.close()
+
+
+def test_batch_whole_field_io_then_step(cuda, tf, oracle):
+    """Seeding a batch with the whole-field calls and reading it back with
+    them gives what the oracle gives per instance."""
+    insts = mixed_instances()
+    b = tf.Batch(insts)
+    b.step(3)
+    pv = b.read_field(tf.FIELD_PV, np.float32)
+    off = 0
+    for inst in insts:
+        want = oracle.air_steps(inst, 3)
+        assert np.array_equal(pv[off:off + inst.cells].view(np.uint32), want["pv"].view(np.uint32))
+        off += inst.cells
+    b.close()

@@ -35,6 +35,31 @@ enum F32 { F_PV, F_VX, F_VY, F_HV, F_HV2, F_OPV, F_OVX, F_OVY, F_FVX, F_FVY, F_G
 enum U32 { U_BA, U_BH, U_BA2, U_BH2, U_WALL, U_EMAP, U_EA, U_EH, U_GMASK, U_NU32 };
 
 size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
+
+// Where one instance's grid sits in the dense staging buffer (the
+// reference's `cy * xcells + cx` layout, instances back to back) and in a
+// pitched arena slot.
+struct IoInst {
+    size_t dense, arena;  // element offsets
+    uint32_t xcells, ycells, pitch;
+};
+
+// Dense <-> pitched copy of one grid kind for instances base .. base +
+// gridDim.y - 1: block (bx, k) copies rows bx, bx + gridDim.x, ... of
+// instance base + k, the threads walking a row so both sides coalesce.
+__global__ void k_batch_io(const IoInst *io, uint32_t base, uint32_t *arena, uint32_t *dense, int to_arena) {
+    const IoInst I = io[base + blockIdx.y];
+    for (uint32_t r = blockIdx.x; r < I.ycells; r += gridDim.x) {
+        uint32_t *a = arena + I.arena + (size_t)r * I.pitch;
+        uint32_t *d = dense + I.dense + (size_t)r * I.xcells;
+        for (uint32_t c = threadIdx.x; c < I.xcells; c += blockDim.x) {
+            if (to_arena)
+                a[c] = d[c];
+            else
+                d[c] = a[c];
+        }
+    }
+}
 }  // namespace
 
 struct tpt_batch {
@@ -61,6 +86,12 @@ struct tpt_batch {
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
     std::map<uint32_t, cudaGraphExec_t> graphs;
+    // whole-batch grid I/O (tpt_batch_write_field / tpt_batch_read_field),
+    // allocated by the first such call: the dense staging grid of every
+    // instance back to back, and the per-instance placement table
+    uint32_t *stage = nullptr;
+    IoInst *io = nullptr;
+    size_t dense_total = 0;  // cells of all instances
 
     float *f(int field, uint32_t i) const { return f32 + (size_t)field * stride + off[i]; }
     uint32_t *u(int field, uint32_t i) const { return u32 + (size_t)field * stride + off[i]; }
@@ -84,6 +115,8 @@ struct tpt_batch {
         cudaFree(u32);
         cudaFree(i32);
         cudaFree(insts);
+        cudaFree(stage);
+        cudaFree(io);
         cudaFree(tmaps);
         cudaFree(tiles);
         if (side) cudaStreamDestroy(side);
@@ -415,6 +448,66 @@ int tpt_batch_write(tpt_batch *b, uint32_t i, int field, const void *host, size_
 
 int tpt_batch_read(tpt_batch *b, uint32_t i, int field, void *host, size_t bytes, tpt_stream_t stream) {
     return batch_copy(b, i, field, host, bytes, false, stream);
+}
+
+// The staging buffer and placement table of the whole-batch calls.
+static int ensure_io(tpt_batch *b) {
+    if (b->stage) return TPT_OK;
+    std::vector<IoInst> io(b->n);
+    size_t dense = 0;
+    for (uint32_t i = 0; i < b->n; ++i) {
+        io[i] = {dense, b->off[i], b->descs[i].air.xcells, b->descs[i].air.ycells, b->pitch[i]};
+        dense += (size_t)io[i].xcells * io[i].ycells;
+    }
+    cudaError_t e = cudaMalloc(&b->io, io.size() * sizeof(IoInst));
+    if (e == cudaSuccess) e = cudaMemcpy(b->io, io.data(), io.size() * sizeof(IoInst), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&b->stage, dense * sizeof(uint32_t));
+    if (e != cudaSuccess) {
+        cudaFree(b->io);
+        cudaFree(b->stage);
+        b->io = nullptr;
+        b->stage = nullptr;
+        set_error("staging buffer of %zu cells: %s", dense, cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? TPT_ERR_OUT_OF_MEMORY : TPT_ERR_CUDA;
+    }
+    b->dense_total = dense;
+    return TPT_OK;
+}
+
+// One grid kind of every instance between a dense host buffer and the arena:
+// one host copy of the whole buffer plus one scatter or gather launch.
+static int batch_copy_field(tpt_batch *b, int field, void *host, size_t bytes, bool to_device,
+                            tpt_stream_t stream) {
+    const char *name = to_device ? "tpt_batch_write_field" : "tpt_batch_read_field";
+    if (!b || !host) TPT_FAIL(TPT_ERR_NULL_POINTER, "%s: NULL pointer", name);
+    void *base;
+    int rc = field_ptr(b, 0, field, &base);  // instance 0 starts its arena slot
+    if (rc) return rc;
+    rc = ensure_io(b);
+    if (rc) return rc;
+    if (bytes != b->dense_total * 4)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "%s: bytes %zu != %zu cells * 4", name, bytes, b->dense_total);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (to_device) TPT_CUDA(cudaMemcpyAsync(b->stage, host, bytes, cudaMemcpyHostToDevice, st));
+    uint32_t maxy = 1;
+    for (const auto &d : b->descs) maxy = std::max(maxy, d.air.ycells);
+    for (uint32_t first = 0; first < b->n; first += 65535u) {
+        const uint32_t k = std::min<uint32_t>(b->n - first, 65535u);
+        const uint32_t bx = std::min<uint32_t>(maxy, std::max<uint32_t>(1u, (uint32_t)b->sms * 8u / k));
+        k_batch_io<<<dim3(bx, k), 128, 0, st>>>(b->io, first, (uint32_t *)base, b->stage, to_device ? 1 : 0);
+        TPT_CUDA(cudaGetLastError());
+        TPT_LAUNCHED();
+    }
+    if (!to_device) TPT_CUDA(cudaMemcpyAsync(host, b->stage, bytes, cudaMemcpyDeviceToHost, st));
+    return TPT_OK;
+}
+
+int tpt_batch_write_field(tpt_batch *b, int field, const void *host, size_t bytes, tpt_stream_t stream) {
+    return batch_copy_field(b, field, const_cast<void *>(host), bytes, true, stream);
+}
+
+int tpt_batch_read_field(tpt_batch *b, int field, void *host, size_t bytes, tpt_stream_t stream) {
+    return batch_copy_field(b, field, host, bytes, false, stream);
 }
 
 int tpt_batch_step(tpt_batch *b, uint32_t ticks, tpt_stream_t stream) {

@@ -46,7 +46,7 @@ EXPORTS = [
     "tpt_air_params_default", "tpt_air_step", "tpt_air_step_static_scratch", "tpt_wall_masks_host", "tpt_grav_plan_create",
     "tpt_grav_plan_destroy", "tpt_grav_plan_dims", "tpt_grav_solve", "tpt_grav_solve_f32",
     "tpt_grav_mask_rebuild", "tpt_mass_to_fixed", "tpt_grav_step", "tpt_batch_create", "tpt_batch_destroy", "tpt_batch_fields",
-    "tpt_batch_write", "tpt_batch_read", "tpt_batch_step", "tpt_batch_tune", "tpt_batch_get_tuning",
+    "tpt_batch_write", "tpt_batch_read", "tpt_batch_write_field", "tpt_batch_read_field", "tpt_batch_step", "tpt_batch_tune", "tpt_batch_get_tuning",
     "tpt_batch_set_tuning", "tpt_batch_profile_phases", "tpt_vox_plan_create", "tpt_vox_plan_destroy",
     "tpt_vox_plan_form", "tpt_vox_air_clear", "tpt_vox_air_gather", "tpt_vox_air_solve", "tpt_vox_grav_solve",
     "tpt_vox_grav_clear_mass", "tpt_vox_grav_gather", "tpt_vox_field_step", "tpt_save_config_default",
@@ -212,6 +212,8 @@ def lib() -> ctypes.CDLL:
         L.tpt_batch_fields.argtypes = [P, u32, ctypes.POINTER(InstanceFields)]
         L.tpt_batch_write.argtypes = [P, u32, i32, P, ctypes.c_size_t, P]
         L.tpt_batch_read.argtypes = [P, u32, i32, P, ctypes.c_size_t, P]
+        L.tpt_batch_write_field.argtypes = [P, i32, P, ctypes.c_size_t, P]
+        L.tpt_batch_read_field.argtypes = [P, i32, P, ctypes.c_size_t, P]
         L.tpt_batch_step.argtypes = [P, u32, P]
         L.tpt_batch_tune.argtypes = [P, P]
         L.tpt_batch_get_tuning.argtypes = [P, ctypes.POINTER(BatchTuning)]
@@ -562,12 +564,27 @@ class Batch:
         check(lib().tpt_batch_read(self._h, i, field, _ptr(a), a.nbytes, _stream(stream)))
         return a
 
+    @property
+    def total_cells(self) -> int:
+        return sum(X * Y for X, Y in self.shapes)
+
+    def write_field(self, field: int, arr: np.ndarray, stream=None):
+        """One grid of every instance, dense and back to back in instance order."""
+        a = np.ascontiguousarray(arr)
+        assert a.itemsize == 4
+        check(lib().tpt_batch_write_field(self._h, field, _ptr(a), a.nbytes, _stream(stream)))
+
+    def read_field(self, field: int, dtype, out: np.ndarray | None = None, stream=None) -> np.ndarray:
+        a = np.empty(self.total_cells, dtype) if out is None else out
+        check(lib().tpt_batch_read_field(self._h, field, _ptr(a), a.nbytes, _stream(stream)))
+        return a
+
     def write_all(self, instances, stream=None):
         import torch
 
-        for i, inst in enumerate(instances):
-            for name, fid in self.GRIDS:
-                self.write(i, fid, getattr(inst, name), stream)
+        for name, fid in self.GRIDS:
+            self.write_field(fid, np.concatenate([np.ascontiguousarray(getattr(inst, name)).ravel()
+                                                  for inst in instances]), stream)
         torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
 
     def step(self, ticks: int, stream=None):
