@@ -356,7 +356,8 @@ def run_ours(args, rank, world, local):
             "data": "synthetic (seeded sandboxes, workloads.py)",
             "config": {"workload": WORKLOAD_NAMES[cid], "instances": len(insts), "cells": cells,
                        "ticks_per_step": ticks, "l2": "working set > 126 MB L2, no flush",
-                       "tuning": {"ctas_per_sm": batch.tuning().ctas_per_sm}},
+                       "tuning": {"ctas_per_sm": batch.tuning().ctas_per_sm,
+                                  "grav_side_ctas": batch.tuning().grav_side_ctas}},
             "e2e": {"value": e2e_value, "unit": "cell-ticks/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps,
                     "calls": f"tpt_batch_write_field x{len(host_in)}, tpt_batch_step, "

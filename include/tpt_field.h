@@ -345,6 +345,14 @@ typedef struct tpt_batch_tuning {
     uint32_t tile_x, tile_y;  /* air tile shape in cells                  */
     uint32_t temporal_depth;  /* ticks per air launch (1 = no blocking)   */
     uint32_t ctas_per_sm;     /* persistent grid size multiplier          */
+    /* Split-BF16 gravity of a batch holding both kinds of y stage (groups of
+     * many equal-shape instances take the Toeplitz GEMM, the others the y
+     * DFT pair): CTAs per launch of the DFT-pair groups' chain, which then
+     * runs on a second stream beside the Toeplitz groups' chain (on the
+     * remaining SMs). 0 runs the stages one after another on one stream.
+     * Must be 0 for other batches; at most half the SMs. Results are the same
+     * for every value. */
+    uint32_t grav_side_ctas;
 } tpt_batch_tuning;
 
 /*
@@ -454,7 +462,8 @@ typedef struct tpt_vox_plan tpt_vox_plan;
  * with TPT_ERR_UNSUPPORTED where the device cannot hold a 16-CTA cluster of
  * its kernel. The plan owns the forms' scratch (the reference's velocity
  * snapshot, air.rs:78-79, and the batched form's per-world source fields,
- * about 5 MiB per world for 16 worlds); no entry point below allocates.
+ * about 5 MiB per world for 16 worlds) and the gravity gather's table of
+ * per-brick list counts (128 KiB); no entry point below allocates.
  */
 int tpt_vox_plan_create(int form, tpt_vox_plan **out);
 int tpt_vox_plan_destroy(tpt_vox_plan *plan);

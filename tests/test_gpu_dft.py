@@ -148,3 +148,61 @@ def test_split_bf16_batch_mixed_y_forms(cuda, tf, oracle, monkeypatch, ymode):
         # gravity reads the previous tick's mass, which the air step leaves alone
         assert np.array_equal(st["gx"], first[i]["gx"]) and np.array_equal(st["gy"], first[i]["gy"])
     b.close()
+
+
+def test_split_bf16_concurrent_y_branches(cuda, tf, oracle, monkeypatch):
+    """grav_side_ctas > 0 runs the DFT-pair groups' chain (R, C, C^-1, R^-1)
+    on a second stream beside the Toeplitz groups' chain (R, T, R^-1): every
+    tile still runs the same code, so the fields are bit-identical to the
+    one-stream order for every CTA split, and the autotuner's choice keeps
+    them. A batch with one kind of y stage rejects a split."""
+    import workloads as W
+
+    monkeypatch.setenv("TPT_SPLIT_BF16_Y_STAGE", "toeplitz:2")
+    insts = W.config_instances(5, limit=2)  # two 400x225: Toeplitz
+    insts += [W.make_instance(57, 36, 5, mass_density=0.02), W.make_instance(33, 151, 6, mass_density=0.02),
+              W.make_instance(57, 36, 7, mass_density=0.02), W.make_instance(200, 40, 8, mass_density=0.02)]
+    b = tf.Batch(insts, tf.PRECISION_SPLIT_BF16)
+    sms = cuda.cuda.get_device_properties(0).multi_processor_count
+    assert b.tuning().grav_side_ctas == 0
+    assert b.profile_phases(2).grav_launches_per_tick == 6  # prep, R, C, C^-1, T, R^-1
+    b.step(2)
+    cuda.cuda.synchronize()
+    ref = [(b.state(i)["gx"], b.state(i)["gy"]) for i in range(len(insts))]
+    for side in (1, 8, 30, sms // 2):
+        t = b.tuning()
+        t.grav_side_ctas = side
+        b.set_tuning(t)
+        # Toeplitz branch R, T, R^-1; DFT-pair branch R, C, C^-1, R^-1; prep
+        assert b.profile_phases(2).grav_launches_per_tick == 8
+        b.step(3)
+        cuda.cuda.synchronize()
+        check_clean(tf)
+        for i in range(len(insts)):
+            st = b.state(i)
+            assert np.array_equal(st["gx"], ref[i][0]) and np.array_equal(st["gy"], ref[i][1]), (side, i)
+    t = b.tuning()
+    t.grav_side_ctas = sms // 2 + 1
+    with pytest.raises(tf.TptError, match="grav_side_ctas"):
+        b.set_tuning(t)
+    b.tune()
+    assert b.tuning().grav_side_ctas <= sms // 2
+    b.step(2)
+    cuda.cuda.synchronize()
+    check_clean(tf)
+    for i, inst in enumerate(insts):
+        st = b.state(i)
+        assert np.array_equal(st["gx"], ref[i][0]) and np.array_equal(st["gy"], ref[i][1]), ("tuned", i)
+        dx, dy = oracle.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx, dtype=np.float64)
+        for g, d in ((st["gx"], dx), (st["gy"], dy)):
+            emax, el2 = errors(g, d)
+            assert emax <= TOL and el2 <= TOL, (i, emax, el2)
+    b.close()
+    # one kind of y stage (and the FP32 solve) takes no split
+    for prec in (tf.PRECISION_SPLIT_BF16, tf.PRECISION_FP32):
+        b = tf.Batch(insts[2:4], prec)
+        t = b.tuning()
+        t.grav_side_ctas = 4
+        with pytest.raises(tf.TptError, match="grav_side_ctas"):
+            b.set_tuning(t)
+        b.close()

@@ -79,7 +79,7 @@ struct tpt_batch {
     uint32_t ntiles = 0;
     bool any_noupdate_heat = false;
     bool any_grav = false;
-    tpt_batch_tuning tuning{AIR_TX, AIR_TY, 1, 4};
+    tpt_batch_tuning tuning{AIR_TX, AIR_TY, 1, 4, 0};
     int sms = 148;
     gfft::FftSet fft;
     dft::DftSet dft;
@@ -495,7 +495,6 @@ static int batch_copy_field(tpt_batch *b, int field, void *host, size_t bytes, b
         const uint32_t k = std::min<uint32_t>(b->n - first, 65535u);
         const uint32_t bx = std::min<uint32_t>(maxy, std::max<uint32_t>(1u, (uint32_t)b->sms * 8u / k));
         k_batch_io<<<dim3(bx, k), 128, 0, st>>>(b->io, first, (uint32_t *)base, b->stage, to_device ? 1 : 0);
-        TPT_CUDA(cudaGetLastError());
         TPT_LAUNCHED();
     }
     if (!to_device) TPT_CUDA(cudaMemcpyAsync(host, b->stage, bytes, cudaMemcpyDeviceToHost, st));
@@ -544,7 +543,14 @@ int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
         TPT_FAIL(TPT_ERR_UNSUPPORTED, "tile %ux%u not built (only %dx%d)", t->tile_x, t->tile_y, AIR_TX, AIR_TY);
     if (t->temporal_depth != 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "temporal depth %u not built", t->temporal_depth);
     if (t->ctas_per_sm < 1 || t->ctas_per_sm > 32) TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm must be 1..32");
-    if (t->ctas_per_sm != b->tuning.ctas_per_sm) b->drop_graphs();
+    const bool split = b->any_grav && b->precision == TPT_PRECISION_SPLIT_BF16 && b->dft.can_split();
+    if (t->grav_side_ctas && !split)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "grav_side_ctas must be 0: the batch's gravity has one kind of y stage");
+    if (split) {
+        int rc = b->dft.set_side_ctas(t->grav_side_ctas);
+        if (rc) return rc;
+    }
+    if (t->ctas_per_sm != b->tuning.ctas_per_sm || t->grav_side_ctas != b->tuning.grav_side_ctas) b->drop_graphs();
     b->tuning = *t;
     return TPT_OK;
 }
@@ -620,6 +626,43 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
             best_ms = ms;
             best = t;
         }
+    }
+    // Then, with that air grid, the gravity split: the graph a step replays
+    // (air and gravity chains together) per candidate CTA count of the
+    // DFT-pair groups' branch, 0 (one stream) included.
+    if (rc == TPT_OK && b->any_grav && b->precision == TPT_PRECISION_SPLIT_BF16 && b->dft.can_split()) {
+        rc = tpt_batch_set_tuning(b, &best);
+        const uint32_t cap = b->dft.max_side_ctas();
+        const uint32_t pcts[] = {0, 10, 15, 20, 25, 33, 40, 50};  // side CTAs, percent of the SMs (0: no split)
+        float split_best = 1e30f;
+        tpt_batch_tuning chosen = best;
+        for (uint32_t pct : pcts) {
+            if (rc) break;
+            tpt_batch_tuning t = best;
+            t.grav_side_ctas = pct ? std::min<uint32_t>(cap, std::max<uint32_t>(1u, (uint32_t)b->sms * pct / 100u)) : 0u;
+            rc = tpt_batch_set_tuning(b, &t);
+            cudaGraphExec_t ex = nullptr;
+            if (rc == TPT_OK) rc = graph_for(b, CHUNK, &ex);
+            float ms = 1e30f;
+            for (int rep = 0; rep < 3 && rc == TPT_OK; ++rep) {  // warm-up, then the faster of two
+                cudaEventRecord(e0, st);
+                if (cudaGraphLaunch(ex, st) != cudaSuccess) {
+                    set_error("graph launch failed while tuning");
+                    rc = TPT_ERR_CUDA;
+                }
+                cudaEventRecord(e1, st);
+                cudaEventSynchronize(e1);
+                float r = 0;
+                cudaEventElapsedTime(&r, e0, e1);
+                if (rep > 0 && r < ms) ms = r;
+            }
+            if (rc) break;
+            if (ms < split_best) {
+                split_best = ms;
+                chosen = t;
+            }
+        }
+        best = chosen;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);

@@ -794,10 +794,25 @@ struct DftImpl {
     PrepRef *prep = nullptr;
     uint32_t nprep = 0;
     uint32_t grid[NSTAGES] = {};
+    // The same tiles split by the form of the group's y stage: branch 0 the
+    // Toeplitz groups (R, T, R^-1), branch 1 the DFT-pair groups (R, C,
+    // C^-1, R^-1). With side_ctas > 0 and both branches non-empty, branch 1
+    // runs on `side` with side_ctas CTAs per launch, concurrently with branch
+    // 0 on the caller's stream with the remaining SMs.
+    Tile *btiles[2][NSTAGES] = {};
+    uint32_t bntiles[2][NSTAGES] = {};
+    bool split_ok = false;
+    uint32_t side_ctas = 0;
+    uint32_t sms = 148;
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     double flops = 0;
     uint32_t *err = nullptr;  // device address of g_dft_err
     ~DftImpl() {
         for (void *p : allocs) cudaFree(p);
+        if (side) cudaStreamDestroy(side);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
     }
     template <typename T> int alloc(T **p, size_t n) {
         void *q = nullptr;
@@ -1015,6 +1030,7 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
     std::vector<Problem> pr;
     if ((rc = I->alloc(&I->tmaps, tm.size()))) return rc;
     std::vector<Tile> tl[NSTAGES];
+    std::vector<Tile> btl[2][NSTAGES];  // per y-stage form: 0 Toeplitz, 1 DFT pair
     std::vector<PrepRef> pref;
     // Consecutive CTAs share the data operand's tile (L2 reuse): in C and
     // C^-1 the data is B (M tiles fastest), in R and R^-1 it is A (N tiles
@@ -1023,12 +1039,17 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
         const Problem &P = pr[prob];
         const Group &gq = I->hg[P.group].g;
         const uint32_t nts = st == ST_R ? gq.wR : st == ST_RI ? gq.wRI : NT;
+        std::vector<Tile> &bl = btl[gq.toe ? 0 : 1][st];
+        auto push = [&](uint32_t mt, uint32_t nt) {
+            tl[st].push_back({prob, (uint16_t)mt, (uint16_t)nt, 0});
+            bl.push_back({prob, (uint16_t)mt, (uint16_t)nt, 0});
+        };
         if (m_fastest) {
             for (uint32_t nt = 0; nt * nts < P.N; ++nt)
-                for (uint32_t mt = 0; mt * MT < P.M; ++mt) tl[st].push_back({prob, (uint16_t)mt, (uint16_t)nt, 0});
+                for (uint32_t mt = 0; mt * MT < P.M; ++mt) push(mt, nt);
         } else {
             for (uint32_t mt = 0; mt * MT < P.M; ++mt)
-                for (uint32_t nt = 0; nt * nts < P.N; ++nt) tl[st].push_back({prob, (uint16_t)mt, (uint16_t)nt, 0});
+                for (uint32_t nt = 0; nt * nts < P.N; ++nt) push(mt, nt);
         }
     };
     for (size_t gi = 0; gi < ng; ++gi) {
@@ -1055,8 +1076,10 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
             // share the A slice while it is in L2
             for (uint32_t kx = 0; kx < g.N1h; ++kx)
                 for (uint32_t f = 0; f < 2; ++f)
-                    for (uint32_t mt = 0; mt * MT < 2 * g.G; ++mt)
+                    for (uint32_t mt = 0; mt * MT < 2 * g.G; ++mt) {
                         tl[ST_T].push_back({pt, (uint16_t)mt, 0, f * g.N1h + kx});
+                        btl[0][ST_T].push_back({pt, (uint16_t)mt, 0, f * g.N1h + kx});
+                    }
             for (uint32_t f = 0; f < 2; ++f) {
                 pr.push_back({tmd + 6, tmd + 7, gi32, g.G * g.Yp, g.X, 2 * g.kpRi / KT, g.kpRi, g.X, f + 1});
                 add_tiles(ST_RI, (uint32_t)pr.size() - 1, false);
@@ -1085,15 +1108,32 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
     int sms = 148, dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    for (int st = 0; st < NSTAGES; ++st) {
-        // Longest K loops first: CTA b takes tiles b, b + grid, ..., so a
-        // long tile placed late would start late and stretch the launch.
-        std::stable_sort(tl[st].begin(), tl[st].end(),
+    // Longest K loops first: CTA b takes tiles b, b + grid, ..., so a long
+    // tile placed late would start late and stretch the launch.
+    auto upload = [&](std::vector<Tile> &v, Tile **dst, uint32_t *n) -> int {
+        std::stable_sort(v.begin(), v.end(),
                          [&](const Tile &a, const Tile &b) { return pr[a.problem].ktiles > pr[b.problem].ktiles; });
-        if ((rc = I->alloc(&I->tiles[st], tl[st].size()))) return rc;
-        TPT_CUDA(cudaMemcpy(I->tiles[st], tl[st].data(), tl[st].size() * sizeof(Tile), cudaMemcpyHostToDevice));
-        I->ntiles[st] = (uint32_t)tl[st].size();
+        int r = I->alloc(dst, v.size());
+        if (r) return r;
+        TPT_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+        *n = (uint32_t)v.size();
+        return TPT_OK;
+    };
+    I->sms = (uint32_t)sms;
+    size_t in_branch[2] = {0, 0};
+    for (int st = 0; st < NSTAGES; ++st) {
+        if ((rc = upload(tl[st], &I->tiles[st], &I->ntiles[st]))) return rc;
         I->grid[st] = std::min<uint32_t>(I->ntiles[st], (uint32_t)sms);
+        for (int b = 0; b < 2; ++b) {
+            if ((rc = upload(btl[b][st], &I->btiles[b][st], &I->bntiles[b][st]))) return rc;
+            in_branch[b] += btl[b][st].size();
+        }
+    }
+    I->split_ok = in_branch[0] > 0 && in_branch[1] > 0 && sms > 1;
+    if (I->split_ok) {
+        TPT_CUDA(cudaStreamCreateWithFlags(&I->side, cudaStreamNonBlocking));
+        TPT_CUDA(cudaEventCreateWithFlags(&I->fork, cudaEventDisableTiming));
+        TPT_CUDA(cudaEventCreateWithFlags(&I->join, cudaEventDisableTiming));
     }
     if ((rc = I->alloc(&I->prep, pref.size()))) return rc;
     TPT_CUDA(cudaMemcpy(I->prep, pref.data(), pref.size() * sizeof(PrepRef), cudaMemcpyHostToDevice));
@@ -1117,6 +1157,17 @@ int DftSet::set_io(size_t j, const SolveIO &io) {
     return TPT_OK;
 }
 
+// One stage's GEMM launch over a tile list, `ctas` persistent CTAs at most.
+template <int S>
+static int stage_launch(const DftImpl *I, const Tile *tiles, uint32_t n, uint32_t ctas, cudaStream_t st,
+                        const InstIO &io0, int act) {
+    if (n == 0) return TPT_OK;
+    dft_gemm<S><<<std::min(n, ctas), THREADS, SMEM_BYTES, st>>>(I->probs, tiles, n, I->groups, I->ios, io0, act,
+                                                                  I->err);
+    TPT_LAUNCHED();
+    return TPT_OK;
+}
+
 int DftSet::launch(cudaStream_t st, const SolveIO *io) const {
     const DftImpl *I = impl;
     InstIO io0{};
@@ -1125,29 +1176,61 @@ int DftSet::launch(cudaStream_t st, const SolveIO *io) const {
         io0 = InstIO{io->mass_i, io->mass_f, io->mask, io->gx, io->gy, io->mass_scale_inv, io->pitch};
         act = 1;
     }
-    uint32_t *err = I->err;
     prep_mass<<<I->nprep, 64, 0, st>>>(I->groups, I->prep, I->ios, io0, act);
     TPT_LAUNCHED();
-#define TPT_DFT_STAGE(S)                                                                                      \
-    if (I->ntiles[S]) {                                                                                      \
-        dft_gemm<S><<<I->grid[S], THREADS, SMEM_BYTES, st>>>(I->probs, I->tiles[S], I->ntiles[S], I->groups, \
-                                                             I->ios, io0, act, err);                         \
-        TPT_LAUNCHED();                                                                                      \
+    int rc;
+    if (!split_active()) {
+        // R, then the y stage of each group (DFT pair or Toeplitz), then R^-1
+        if ((rc = stage_launch<ST_R>(I, I->tiles[ST_R], I->ntiles[ST_R], I->grid[ST_R], st, io0, act))) return rc;
+        if ((rc = stage_launch<ST_C>(I, I->tiles[ST_C], I->ntiles[ST_C], I->grid[ST_C], st, io0, act))) return rc;
+        if ((rc = stage_launch<ST_CI>(I, I->tiles[ST_CI], I->ntiles[ST_CI], I->grid[ST_CI], st, io0, act))) return rc;
+        if ((rc = stage_launch<ST_T>(I, I->tiles[ST_T], I->ntiles[ST_T], I->grid[ST_T], st, io0, act))) return rc;
+        return stage_launch<ST_RI>(I, I->tiles[ST_RI], I->ntiles[ST_RI], I->grid[ST_RI], st, io0, act);
     }
-    // R, then the y stage of each group (DFT pair or Toeplitz), then R^-1
-    TPT_DFT_STAGE(ST_R)
-    TPT_DFT_STAGE(ST_C)
-    TPT_DFT_STAGE(ST_CI)
-    TPT_DFT_STAGE(ST_T)
-    TPT_DFT_STAGE(ST_RI)
-#undef TPT_DFT_STAGE
+    // The two forms of y stage touch disjoint groups: fork the DFT-pair
+    // groups' chain onto the side stream with side_ctas CTAs per launch and
+    // run the Toeplitz groups' chain beside it on the remaining SMs.
+    const uint32_t cs = I->side_ctas, cm = I->sms - I->side_ctas;
+    TPT_CUDA(cudaEventRecord(I->fork, st));
+    TPT_CUDA(cudaStreamWaitEvent(I->side, I->fork, 0));
+    Tile *const *b1 = I->btiles[1];
+    const uint32_t *n1 = I->bntiles[1];
+    if ((rc = stage_launch<ST_R>(I, b1[ST_R], n1[ST_R], cs, I->side, io0, act))) return rc;
+    if ((rc = stage_launch<ST_C>(I, b1[ST_C], n1[ST_C], cs, I->side, io0, act))) return rc;
+    if ((rc = stage_launch<ST_CI>(I, b1[ST_CI], n1[ST_CI], cs, I->side, io0, act))) return rc;
+    if ((rc = stage_launch<ST_RI>(I, b1[ST_RI], n1[ST_RI], cs, I->side, io0, act))) return rc;
+    Tile *const *b0 = I->btiles[0];
+    const uint32_t *n0 = I->bntiles[0];
+    if ((rc = stage_launch<ST_R>(I, b0[ST_R], n0[ST_R], cm, st, io0, act))) return rc;
+    if ((rc = stage_launch<ST_T>(I, b0[ST_T], n0[ST_T], cm, st, io0, act))) return rc;
+    if ((rc = stage_launch<ST_RI>(I, b0[ST_RI], n0[ST_RI], cm, st, io0, act))) return rc;
+    TPT_CUDA(cudaEventRecord(I->join, I->side));
+    TPT_CUDA(cudaStreamWaitEvent(st, I->join, 0));
+    return TPT_OK;
+}
+
+bool DftSet::can_split() const { return impl && impl->split_ok; }
+
+bool DftSet::split_active() const { return impl && impl->split_ok && impl->side_ctas > 0; }
+
+uint32_t DftSet::max_side_ctas() const { return impl && impl->split_ok ? impl->sms / 2 : 0u; }
+
+int DftSet::set_side_ctas(uint32_t ctas) {
+    if (ctas > max_side_ctas())
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "grav_side_ctas %u above %u", ctas, max_side_ctas());
+    impl->side_ctas = ctas;
     return TPT_OK;
 }
 
 uint32_t DftSet::launches() const {
     uint32_t n = 1;  // prep_mass
-    if (impl)
+    if (!impl) return n;
+    if (split_active()) {
+        for (int b = 0; b < 2; ++b)
+            for (int s = 0; s < NSTAGES; ++s) n += impl->bntiles[b][s] ? 1u : 0u;
+    } else {
         for (int s = 0; s < NSTAGES; ++s) n += impl->ntiles[s] ? 1u : 0u;
+    }
     return n;
 }
 double DftSet::flops() const { return impl ? impl->flops : 0.0; }

@@ -30,6 +30,13 @@ struct DftSet {
     // Binds job j to fixed inputs/outputs (a batch's arenas).
     int set_io(size_t j, const SolveIO &io);
     int launch(cudaStream_t st, const SolveIO *io = nullptr) const;
+    // Concurrent y stages: true when the set holds both Toeplitz and
+    // DFT-pair groups; set_side_ctas(c > 0) then runs the DFT-pair groups'
+    // chain on a second stream with c CTAs per launch (0: one stream).
+    bool can_split() const;
+    bool split_active() const;
+    uint32_t max_side_ctas() const;
+    int set_side_ctas(uint32_t ctas);
     // kernel launches and executed tensor flops of one launch() of the set
     uint32_t launches() const;
     double flops() const;
