@@ -84,6 +84,27 @@ def test_grav_gather(cuda, oracle, plans, world, active):
     _same(V.download(bufs, air), d, ("grav_mass",))
 
 
+def test_grav_gather_repeated_bricks(cuda, oracle, plans, world):
+    """A brick listed k times adds its mass k times, as the reference's
+    per-listed-brick atomics do (the device sums cells in memory order)."""
+    import voxel3d as V
+    import workloads as W
+
+    d = _copy(world)
+    uniq = np.random.default_rng(8).permutation(W.VOX_BRICKS)[:3000].astype(np.uint32)
+    lst = np.concatenate([uniq, uniq[:1000], uniq[:10]])
+    np.random.default_rng(9).shuffle(lst)
+    d["sim_list"] = np.zeros(W.VOX_BRICKS, np.uint32)
+    d["sim_list"][:lst.size] = lst
+    d["sim_count"] = np.array([lst.size, 1, 1], np.uint32)
+    bufs, air = V.upload(d)
+    V.gravity_gather(plans["batched"], bufs)
+    V.gravity_gather(plans["batched"], bufs)  # twice in a row: the brick table is rebuilt per call
+    oracle.vox_grav_gather(d)
+    oracle.vox_grav_gather(d)
+    _same(V.download(bufs, air), d, ("grav_mass",))
+
+
 @pytest.mark.parametrize("form", sorted(FORMS))
 @pytest.mark.parametrize("iterations", [0, 1, 2, 3, 12])
 def test_air_solve(cuda, oracle, plans, world, form, iterations):

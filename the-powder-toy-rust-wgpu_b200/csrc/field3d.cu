@@ -111,71 +111,69 @@ __global__ void __launch_bounds__(256) k_air_gather(const uint32_t *__restrict__
     }
 }
 
-// gravity_gather_kernel (gravity.rs:125-166). Only GRVT (39) .. GPMP (43)
-// carry mass, and only GRVT, NBHL and NWHL (39..41) read tmp: a tmp word
-// group is loaded only where its voxel group holds one of those, and each
-// lane runs the mass arithmetic for its gravity voxels only (a loop over a
-// bit mask of them). Integer sums wrap like the reference's i32 accumulator
-// and atomic add.
-__global__ void __launch_bounds__(256) k_grav_gather(const uint32_t *__restrict__ voxel,
-                                                     const int32_t *__restrict__ aux,
-                                                     const uint32_t *__restrict__ list,
-                                                     const uint32_t *__restrict__ count, int32_t *__restrict__ mass) {
+// Per-brick multiplicity of the active list: how many times each brick id
+// is listed (a compaction lists each active brick once). `mult` is cleared
+// before the launch; ids are taken modulo the brick count, as the gathers do.
+__global__ void k_brick_mult(const uint32_t *__restrict__ list, const uint32_t *__restrict__ count,
+                             uint32_t *__restrict__ mult) {
     const uint32_t n = min(__ldg(count), (uint32_t)TPT_VOX_BRICKS);
-    const int lane = threadIdx.x & 31;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-    for (uint32_t b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < n; b += nwarps) {
-        const uint32_t brick = __ldg(list + b) & (TPT_VOX_BRICKS - 1u);
-        const uint32_t base = brick_base(brick);
-        uint32_t ws[16];
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x)
+        atomicAdd(mult + (__ldg(list + b) & (TPT_VOX_BRICKS - 1u)), 1u);
+}
+
+// gravity_gather_kernel (gravity.rs:125-166) in memory order. The reference
+// adds each voxel's fixed-point mass to its cell with one atomic per voxel of
+// every listed brick; in wrapping i32 arithmetic the result is each cell's
+// voxel sum times the number of times its brick is listed, in any order.
+// Block (zc, yc) owns the 64 cells of one cell row. Its 16 voxel rows
+// (y = 4 yc + r / 4, z = 4 zc + r % 4) are read as 256-byte runs: warp w
+// holds rows 2w and 2w + 1, one per half-warp, and lane l of a half the word
+// quads of cells xc = 16 j + l, j = 0..3. A cell of an unlisted brick is
+// neither read nor written; aux_tmp is read only for the quads holding GRVT,
+// NBHL or NWHL.
+__global__ void __launch_bounds__(256) k_grav_gather_rows(const uint32_t *__restrict__ voxel,
+                                                          const int32_t *__restrict__ aux,
+                                                          const uint32_t *__restrict__ mult,
+                                                          int32_t *__restrict__ mass) {
+    __shared__ uint32_t part[8][N];
+    const uint32_t zc = blockIdx.x, yc = blockIdx.y;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t l = (uint32_t)lane & 15u, r = 2u * (uint32_t)warp + ((uint32_t)lane >> 4);
+    const uint32_t row = ((4u * yc + (r >> 2)) << 16) | ((4u * zc + (r & 3u)) << 8);
+    const uint32_t bbase = ((yc >> 1) << 10) | ((zc >> 1) << 5);
+    uint32_t s[4];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const uint4 w = __ldg(reinterpret_cast<const uint4 *>(voxel + base + lane_offset(lane, j)));
-            ws[4 * j] = w.x;
-            ws[4 * j + 1] = w.y;
-            ws[4 * j + 2] = w.z;
-            ws[4 * j + 3] = w.w;
-        }
-        uint32_t gmask = 0u, tmask = 0u;  // gravity voxels; groups whose tmp is read
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t xc = 16u * (uint32_t)j + l;
+        s[j] = 0u;
+        if (__ldg(mult + (bbase | (xc >> 1))) == 0u) continue;
+        const uint32_t o = row | (4u * xc);
+        const uint4 w = __ldg(reinterpret_cast<const uint4 *>(voxel + o));
+        const uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+        bool need = false;
 #pragma unroll
-        for (int v = 0; v < 16; ++v) {
-            const uint32_t e = (ws[v] & 0xFFu) - 39u;
-            gmask |= (uint32_t)(e < 5u) << v;
-            tmask |= (uint32_t)(e < 3u) << (v >> 2);
-        }
-        int32_t ts[16];
+        for (int k = 0; k < 4; ++k) need |= ((ws[k] & 0xFFu) - 39u) < 3u;
+        int4 t = make_int4(0, 0, 0, 0);
+        if (need) t = __ldg(reinterpret_cast<const int4 *>(aux + o));
+        const int32_t ts[4] = {t.x, t.y, t.z, t.w};
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            int4 t = make_int4(0, 0, 0, 0);
-            if ((tmask >> j) & 1u) t = __ldg(reinterpret_cast<const int4 *>(aux + base + lane_offset(lane, j)));
-            ts[4 * j] = t.x;
-            ts[4 * j + 1] = t.y;
-            ts[4 * j + 2] = t.z;
-            ts[4 * j + 3] = t.w;
-        }
-        uint32_t acc[2] = {0u, 0u};
-        while (gmask) {
-            const int v = __ffs(gmask) - 1;
-            gmask &= gmask - 1u;
-            uint32_t word = 0u;
-            int32_t tmp = 0;
+        for (int k = 0; k < 4; ++k)
+            s[j] += (uint32_t)voxel_mass(ws[k] & 0xFFu, (ws[k] >> 24) & 0xFFu, ts[k], (ws[k] >> 8) & 0xFFFFu);
+    }
 #pragma unroll
-            for (int u = 0; u < 16; ++u)
-                if (u == v) {
-                    word = ws[u];
-                    tmp = ts[u];
-                }
-            acc[v >> 3] += (uint32_t)voxel_mass(word & 0xFFu, (word >> 24) & 0xFFu, tmp,
-                                                (float)((word >> 8) & 0xFFFFu) * 0.125f);
-        }
+    for (int j = 0; j < 4; ++j) {
+        s[j] += __shfl_xor_sync(0xFFFFFFFFu, s[j], 16);
+        if (lane < 16) part[warp][16 * j + (int)l] = s[j];
+    }
+    __syncthreads();
+    if (threadIdx.x < (unsigned)N) {
+        const uint32_t xc = threadIdx.x, m = __ldg(mult + (bbase | (xc >> 1)));
+        if (m != 0u) {
+            uint32_t tot = 0u;
 #pragma unroll
-        for (int cy = 0; cy < 2; ++cy) acc[cy] = cell_sum(acc[cy]);
-        if ((lane & 0x16) == 0) {
-#pragma unroll
-            for (int cy = 0; cy < 2; ++cy)
-                if (acc[cy] != 0u)
-                    atomicAdd(reinterpret_cast<unsigned int *>(mass) + brick_cell(brick, lane & 1, cy, (lane >> 3) & 1),
-                              acc[cy]);
+            for (int w = 0; w < 8; ++w) tot += part[w][xc];
+            uint32_t *c = reinterpret_cast<uint32_t *>(mass) + ((yc << 12) | (zc << 6) | xc);
+            *c += m * tot;
         }
     }
 }
@@ -662,8 +660,11 @@ int launch_air_gather(const World &w, cudaStream_t st) {
     return TPT_OK;
 }
 
-int launch_grav_gather(const World &w, cudaStream_t st) {
-    k_grav_gather<<<gather_blocks(4), 256, 0, st>>>(w.voxel, w.aux_tmp, w.sim_list, w.sim_count, w.grav_mass);
+int launch_grav_gather(const World &w, uint32_t *brick_mult, cudaStream_t st) {
+    TPT_CUDA(cudaMemsetAsync(brick_mult, 0, TPT_VOX_BRICKS * sizeof(uint32_t), st));
+    k_brick_mult<<<TPT_VOX_BRICKS / 256, 256, 0, st>>>(w.sim_list, w.sim_count, brick_mult);
+    TPT_LAUNCHED();
+    k_grav_gather_rows<<<dim3(N, N), 256, 0, st>>>(w.voxel, w.aux_tmp, brick_mult, w.grav_mass);
     TPT_LAUNCHED();
     return TPT_OK;
 }

@@ -77,7 +77,8 @@ int launch_batch(Batch &b, cudaStream_t st);
 
 int launch_air_clear(const World &w, cudaStream_t st);
 int launch_air_gather(const World &w, cudaStream_t st);
-int launch_grav_gather(const World &w, cudaStream_t st);
+// gravity::gather; brick_mult is TPT_VOX_BRICKS words of scratch.
+int launch_grav_gather(const World &w, uint32_t *brick_mult, cudaStream_t st);
 int launch_grav_clear(const World &w, cudaStream_t st);
 // Whether the device can hold one cluster of the cluster kernel.
 int cluster_supported(bool *ok);

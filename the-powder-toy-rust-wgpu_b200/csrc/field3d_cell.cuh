@@ -133,22 +133,29 @@ __device__ __forceinline__ float pressure_grad(float lo, float hi, float self, i
     return (h - l) * 0.5f;
 }
 
-// Fixed-point mass of one voxel (gravity.rs:74-109), every element's case
-// evaluated and the voxel's selected, so a warp does not diverge on the
-// element mix. `temp_k` is a 16-bit count times 0.125 and always finite, so
-// seed_f32(temp_k, 0.1) is 0.1.
-__device__ __forceinline__ int32_t voxel_mass(uint32_t ty, uint32_t life, int32_t tmp, float temp_k) {
-    const float tf = (float)tmp;
-    // clamp((float)tmp, -100, 100) truncated is the integer clamp of tmp: the
-    // f32 rounding of an integer beyond +-100 stays beyond it.
-    const int32_t t = min(max(tmp, -100), 100);
-    const int32_t grvt = __float2int_rz(0.2f * (float)t * 1024.0f);                    // GRVT
+// Fixed-point mass of one voxel (gravity.rs:74-109), branch-free so a warp
+// does not diverge on the element mix. Each element's case converts one
+// integer to f32 and truncates one f32 product, so the integer the voxel's
+// case needs (GRVT the clamped tmp, NBHL/NWHL tmp, GPMP the 16-bit
+// temperature count) is picked first and converted once, the three f32
+// expressions are evaluated from it, and the voxel's one is truncated once:
+// two conversions per voxel instead of one per case. GRVT: clamp((float)tmp,
+// -100, 100) truncated is the integer clamp of tmp (the f32 rounding of an
+// integer beyond +-100 stays beyond it). NBHL/NWHL: the reference's seed
+// value of `add` is 0.1 (the temperature is always finite). GPMP: temp_k is
+// the count times 0.125.
+__device__ __forceinline__ int32_t voxel_mass(uint32_t ty, uint32_t life, int32_t tmp, uint32_t temp_q) {
+    const bool grvt = ty == 39u, hole = ty == 40u || ty == 41u;
+    const int32_t src = grvt ? min(max(tmp, -100), 100) : hole ? tmp : (int32_t)temp_q;
+    const float x = (float)src;
+    const float fg = 0.2f * x * 1024.0f;  // GRVT
     float add = 0.1f;
-    if (tmp != 0) add = clampf(0.001f * tf, 0.1f, 51.2f);
-    const int32_t hole = __float2int_rz((ty == 41u ? -add : add) * 1024.0f);           // NBHL, NWHL
-    const int32_t gbmb = life > 20u ? 20480 : (life >= 1u ? -81920 : 0);               // GBMB
-    const int32_t gpmp = life == 10u ? __float2int_rz(0.2f * (temp_k - 273.15f) * 1024.0f) : 0;  // GPMP
-    return ty == 39u ? grvt : (ty == 40u || ty == 41u) ? hole : ty == 42u ? gbmb : ty == 43u ? gpmp : 0;
+    if (tmp != 0) add = clampf(0.001f * x, 0.1f, 51.2f);
+    const float fh = (ty == 41u ? -add : add) * 1024.0f;  // NBHL, NWHL
+    const float fp = 0.2f * (x * 0.125f - 273.15f) * 1024.0f;  // GPMP
+    const int32_t r = __float2int_rz(grvt ? fg : hole ? fh : fp);
+    const int32_t gbmb = life > 20u ? 20480 : (life >= 1u ? -81920 : 0);  // GBMB
+    return (grvt || hole || (ty == 43u && life == 10u)) ? r : ty == 42u ? gbmb : 0;
 }
 
 __device__ __forceinline__ float f4(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }

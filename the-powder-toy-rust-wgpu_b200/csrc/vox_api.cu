@@ -12,6 +12,7 @@ struct tpt_vox_plan {
     // Cluster form: one AirScratch (4 fields) per world of a launch.
     // Batched form: BATCH_SCRATCH_BYTES per world of a launch.
     float *scratch = nullptr;
+    uint32_t *brick_mult = nullptr;  // the gravity gather's per-brick list multiplicity
     tpt::vox::AirScratch slot(uint32_t i) const {
         float *b = scratch + (size_t)i * tpt::vox::AIR_SCRATCH_FLOATS;
         return {b, b + TPT_VOX_CELLS};
@@ -146,7 +147,9 @@ int tpt_vox_plan_create(int form, tpt_vox_plan **out) {
     if (p->form == TPT_VOX_CLUSTER) bytes = (size_t)(vox::MAX_JOBS / 2) * vox::AIR_SCRATCH_FLOATS * sizeof(float);
     if (p->form == TPT_VOX_BATCHED) bytes = (size_t)vox::MAX_BWORLDS * vox::BATCH_SCRATCH_BYTES;
     cudaError_t e = cudaMalloc(&p->scratch, bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&p->brick_mult, TPT_VOX_BRICKS * sizeof(uint32_t));
     if (e != cudaSuccess) {
+        cudaFree(p->scratch);
         delete p;
         TPT_FAIL(e == cudaErrorMemoryAllocation ? TPT_ERR_OUT_OF_MEMORY : TPT_ERR_CUDA,
                  "tpt_vox_plan_create: scratch allocation failed: %s", cudaGetErrorString(e));
@@ -158,6 +161,7 @@ int tpt_vox_plan_create(int form, tpt_vox_plan **out) {
 int tpt_vox_plan_destroy(tpt_vox_plan *plan) {
     if (!plan) return TPT_OK;
     if (plan->scratch) cudaFree(plan->scratch);
+    if (plan->brick_mult) cudaFree(plan->brick_mult);
     delete plan;
     return TPT_OK;
 }
@@ -218,7 +222,7 @@ int tpt_vox_grav_gather(tpt_vox_plan *plan, const tpt_vox_world *w, tpt_stream_t
     int rc = check_gather(w);
     if (!rc) rc = check_ptrs("gravity gather", {w->aux_tmp, w->grav_mass});
     if (rc) return rc;
-    return vox::launch_grav_gather(world_of(*w), (cudaStream_t)stream);
+    return vox::launch_grav_gather(world_of(*w), plan->brick_mult, (cudaStream_t)stream);
 }
 
 int tpt_vox_field_step(tpt_vox_plan *plan, const tpt_vox_world *worlds, uint32_t n, uint32_t air_iterations,
