@@ -206,3 +206,37 @@ def test_split_bf16_concurrent_y_branches(cuda, tf, oracle, monkeypatch):
         with pytest.raises(tf.TptError, match="grav_side_ctas"):
             b.set_tuning(t)
         b.close()
+
+
+def test_c5_batch_concurrent_branches_full_size(cuda, tf, oracle):
+    """The full C5 batch (128 instances, 6.1M cells) in the configuration the
+    bench times: autotuned, then with the gravity branches concurrent. gx/gy
+    stay bit-identical to the one-stream order on instances of both y forms
+    and meet the 1e-4 bar against FP64; the air fields after 5 ticks are
+    bit-exact against the oracle."""
+    import workloads as W
+    from test_gpu_air import assert_bit_exact
+
+    insts = W.config_instances(5)
+    b = tf.Batch(insts, tf.PRECISION_SPLIT_BF16)
+    sample = (0, 63, 64, 70, 100, 127)
+    b.step(2)
+    cuda.cuda.synchronize()
+    ref = {i: (b.state(i)["gx"], b.state(i)["gy"]) for i in sample}
+    b.tune()
+    t = b.tuning()
+    t.grav_side_ctas = max(1, cuda.cuda.get_device_properties(0).multi_processor_count * 2 // 5)
+    b.set_tuning(t)
+    b.step(3)
+    cuda.cuda.synchronize()
+    check_clean(tf)
+    for i in sample:
+        inst = insts[i]
+        st = b.state(i)
+        assert np.array_equal(st["gx"], ref[i][0]) and np.array_equal(st["gy"], ref[i][1]), i
+        dx, dy = oracle.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx, dtype=np.float64)
+        for g, d in ((st["gx"], dx), (st["gy"], dy)):
+            emax, el2 = errors(g, d)
+            assert emax <= TOL and el2 <= TOL, (i, emax, el2)
+        assert_bit_exact(st, oracle.air_steps(inst, 5), f"C5 instance {i}")
+    b.close()
