@@ -2,7 +2,7 @@
 """Benchmark of the coarse-grid field step (air + Newtonian gravity) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload c1|c2|c4|c5] [--ticks T]
+                    [--workload 1|2|4|5] [--ticks T]   (workloads C1, C2, C4, C5)
     python bench.py --voxel3d [--worlds W] ...   (the 3-D sandbox's field step)
     python bench.py --save-io                    (the .tptrs save codec, host only)
 
