@@ -1,0 +1,40 @@
+"""CPU test of bench.py's reference arm, the line the driver compares the
+GPU line against: under two ranks (RANK / WORLD_SIZE as torchrun sets them)
+rank 0 prints exactly one JSON line with the contract's keys and rank 1 exits
+0 without output. The arm times the oracle's port of the reference kernels
+on host cores on a bounded sample of the C5 workload."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _run(rank, world):
+    env = dict(os.environ, RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                           "--warmup", "3", "--cpu-seconds", "1"], cwd=ROOT, env=env, capture_output=True, text=True,
+                          timeout=600)
+
+
+def test_reference_arm_other_rank_exits_quietly():
+    p = _run(1, 2)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert p.stdout.strip() == ""
+
+
+def test_reference_arm_rank0_prints_one_contract_line():
+    p = _run(0, 2)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [ln for ln in p.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["metric"] == "cell-ticks/s" and d["unit"] == "cell-ticks/s"
+    assert d["n_gpus"] == 2 and d["steps"] == 1 and d["warmup"] >= 3 and d["higher_is_better"] is True
+    assert d["value"] > 0 and d["config"]["workload"].startswith("C5")
+    cb = d["cpu_baseline"]
+    assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
+    e2e = d["e2e"]
+    assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
+    assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
