@@ -162,38 +162,77 @@ def max_over_ranks(v: float, world: int) -> float:
 
 # ----------------------------------------------------------- CPU baseline --
 
+def _strata(insts):
+    """Instances grouped by shape class: equal-shape groups of eight or more
+    (C5's 64 x 400x225) and the rest (the heavy tail, or all of C4)."""
+    shapes = {}
+    for i, inst in enumerate(insts):
+        shapes.setdefault((inst.xcells, inst.ycells), []).append(i)
+    groups = [v for v in shapes.values() if len(v) >= 8]
+    rest = sorted(i for v in shapes.values() if len(v) < 8 for i in v)
+    out = [g for g in groups]
+    if rest:
+        out.append(rest)
+    return out
+
+
 def cpu_rate(insts, target_s: float, threads: int | None = None):
-    """Oracle FP32 air + gravity on a bounded sample of `insts` (all host
-    threads); returns (cell-ticks/s, cores, sample description)."""
+    """The oracle's FP32 air + gravity (all host threads) on a stratified
+    sample of `insts`: from each shape stratum (equal-shape groups, and the
+    heavy tail) a few evenly spaced instances run the same number of ticks;
+    each stratum's time per cell-tick is scaled by that stratum's share of the
+    workload's cells, so the result estimates the whole workload's
+    cell-ticks/s. Ticks are chosen so the timed sample takes about `target_s`.
+    Returns (cell-ticks/s, cores, sample description)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
     if threads:
         O.set_threads(threads)
     cores = O.num_threads()
-    sample = insts[: max(1, min(len(insts), 8))]
+    strata = []
+    for idx in _strata(insts):
+        k = min(len(idx), 4)
+        pick = [idx[(j * len(idx)) // k] for j in range(k)]
+        strata.append((idx, pick))
 
-    def one_tick():
-        t0 = time.perf_counter()
-        for inst in sample:
-            O.air_steps(inst, 1)
+    def run(cur, ticks):
+        for inst in cur:
+            O.air_steps(inst, ticks)
             if inst.config.newton_grav:
-                O.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx)
-        return time.perf_counter() - t0
+                for _ in range(ticks):
+                    O.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx)
 
-    t1 = one_tick()
-    ticks = max(1, min(200, int(target_s / max(t1, 1e-6))))
-    cur = [i.copy() for i in sample]
     t0 = time.perf_counter()
-    for inst in cur:
-        st = O.air_steps(inst, ticks)
-        if inst.config.newton_grav:
-            for _ in range(ticks):
-                O.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx)
-    dt = time.perf_counter() - t0
-    cells = sum(i.cells for i in sample)
-    desc = f"{len(sample)} of {len(insts)} instances ({cells} cells) x {ticks} ticks, air + gravity solve per tick"
-    return cells * ticks / dt, cores, desc
+    run([insts[i] for _, pick in strata for i in pick], 1)
+    t1 = time.perf_counter() - t0
+    ticks = max(2, int(target_s / max(t1, 1e-6)))
+    est_s_per_tick = 0.0
+    parts = []
+    for idx, pick in strata:
+        cur = [insts[i].copy() for i in pick]
+        t0 = time.perf_counter()
+        run(cur, ticks)
+        dt = time.perf_counter() - t0
+        cells_s = sum(insts[i].cells for i in pick)
+        cells_all = sum(insts[i].cells for i in idx)
+        est_s_per_tick += dt / ticks / cells_s * cells_all
+        parts.append(f"{len(pick)} of {len(idx)} instances ({cells_s} of {cells_all} cells)")
+    total = sum(i.cells for i in insts)
+    desc = (f"stratified sample, {ticks} ticks each: " + "; ".join(parts) +
+            "; air + gravity solve per tick; each stratum's time scaled by its share of the cells")
+    return total / est_s_per_tick, cores, desc
+
+
+def ticks_of(cid: int) -> int:
+    """Ticks of one bench step: the configs' stated horizon (C2 states 10000)."""
+    return 10000 if cid == 2 else 1000
+
+
+def config_of(cid: int, insts, ticks: int | None = None) -> dict:
+    """The workload as both arms print it (the whole workload, all instances)."""
+    return {"workload": WORKLOAD_NAMES[cid], "instances": len(insts), "cells": sum(i.cells for i in insts),
+            "ticks_per_step": ticks or ticks_of(cid)}
 
 
 # ------------------------------------------------------------------ ours --
@@ -242,9 +281,10 @@ def run_ours(args, rank, world, local):
     cid = args.workload
     insts = workload(cid)
     total_cells = sum(i.cells for i in insts)
+    cfg = config_of(cid, insts, args.ticks or None)
     if args.scaling == "strong" and world > 1:  # this rank's share, no exchange between ranks
         insts = [insts[i] for i in sharding.shard_of([(i.xcells, i.ycells) for i in insts], rank, world)]
-    ticks = args.ticks or (1000 if cid in (4, 5) else (1000 if cid == 1 else 10000))
+    ticks = args.ticks or ticks_of(cid)
     precision = tf.PRECISION_SPLIT_BF16 if cid == 5 else tf.PRECISION_FP32
     stream = torch.cuda.current_stream()
     batch = tf.Batch(insts, precision)
@@ -354,10 +394,9 @@ def run_ours(args, rank, world, local):
             "higher_is_better": True, "scaling": args.scaling, "vs_baseline": None,
             "dtype": "f32" if precision == tf.PRECISION_FP32 else "f32 air + bf16x3 gravity (f32 accumulate)",
             "data": "synthetic (seeded sandboxes, workloads.py)",
-            "config": {"workload": WORKLOAD_NAMES[cid], "instances": len(insts), "cells": cells,
-                       "ticks_per_step": ticks, "l2": "working set > 126 MB L2, no flush",
-                       "tuning": {"ctas_per_sm": batch.tuning().ctas_per_sm,
-                                  "grav_side_ctas": batch.tuning().grav_side_ctas}},
+            "config": cfg,
+            "l2": "working set > 126 MB L2, no flush",
+            "tuning": batch.tuning_dict(),
             "e2e": {"value": e2e_value, "unit": "cell-ticks/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps,
                     "calls": f"tpt_batch_write_field x{len(host_in)}, tpt_batch_step, "
@@ -585,8 +624,10 @@ def run_reference(args, rank, world):
     insts = workload(cid)
     rate_samples = []
     cores = desc = None
+    # each step: a stratified sample of the workload, sized to about
+    # --ref-step-seconds of host work
     for _ in range(args.warmup + args.steps):
-        rate, cores, desc = cpu_rate(insts, args.cpu_seconds / max(args.steps, 1))
+        rate, cores, desc = cpu_rate(insts, args.ref_step_seconds)
         rate_samples.append(rate)
     rates = rate_samples[args.warmup:]
     value = statistics.median(rates)
@@ -594,7 +635,8 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": "cell-ticks/s", "value": value, "unit": "cell-ticks/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded sandboxes, workloads.py)",
-        "config": {"workload": WORKLOAD_NAMES[cid], "instances": len(insts)},
+        "config": config_of(cid, insts, args.ticks or None),
+        "spread": {"min": min(rates), "max": max(rates)},
         "cpu_baseline": {"value": value, "unit": "cell-ticks/s", "cores": cores, "kind": "port", "sample": desc},
         "e2e": {"value": value, "unit": "cell-ticks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -686,7 +728,9 @@ def main():
     ap.add_argument("--plain-ticks", type=int, default=500, help="ticks of the plain FP32 comparison (0 = skip)")
     ap.add_argument("--scaling", choices=("weak", "strong"), default="weak",
                     help="weak: every rank steps a full copy; strong: ranks split one copy's instances")
-    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="host work of the GPU arm's cpu_baseline leg")
+    ap.add_argument("--ref-step-seconds", type=float, default=2.0,
+                    help="host work of one --impl reference step (a stratified sample of the workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer run (profiling captures)")
     ap.add_argument("--phase-ticks", type=int, default=200, help="even tick count of the per-phase timing")

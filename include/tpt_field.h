@@ -161,9 +161,11 @@ int tpt_air_step(const tpt_air_params *params, const tpt_air_bufs *bufs,
  * process exits. Grids larger than TPT_STATIC_SCRATCH_MAX_CELLS cells are
  * rejected with TPT_ERR_INVALID_DIMS.
  *
- * The first call on a device looks the array up for that device (with the
- * device current); make that first call outside any stream capture. All
- * calls share the one array: calls whose work can overlap on the GPU (other
+ * Every call looks up the array's address in the current device's context
+ * (cudaGetSymbolAddress, which allocates nothing), so the address stays
+ * valid across a cudaDeviceReset. The first call on a device may load the
+ * library's device code into that context: make it outside any stream
+ * capture. All calls share the one array: calls whose work can overlap on the GPU (other
  * streams, other host threads) race on it and must be serialised by the
  * caller. Nothing needs clearing between calls -- each step writes every
  * scratch cell it reads.

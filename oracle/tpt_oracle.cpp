@@ -193,6 +193,17 @@ static inline R vorticity_bmap(const R *vx, const R *vy, const uint32_t *b, cons
     return out;
 }
 
+// f32 -> i32 as the kernels' `as i32` (WGSL `i32(f32)`): round toward zero
+// and saturate to the i32 range; NaN gives 0, as CUDA's cvt.rzi does (WGSL
+// leaves NaN to the implementation). A plain C++ cast of an out-of-range or
+// NaN float is undefined behaviour, so every such conversion goes through here.
+template <typename R> static inline int32_t to_i32(R v) {
+    if (v != v) return 0;
+    if (v >= R(2147483648.0)) return INT32_MAX;
+    if (v <= R(-2147483648.0)) return INT32_MIN;
+    return (int32_t)v;
+}
+
 // advect.rs:46-52
 static inline uint32_t advect_blocked(const uint32_t *b, size_t idx, bool heat) {
     return heat ? (b[idx] & 0x8u) : b[idx];
@@ -218,11 +229,11 @@ static inline void far_advect_target(uint32_t x, uint32_t y, R dx, R dy, const u
         if (abs_dx > abs_dy) {
             step_x = dx < R(0) ? R(1) : R(-1);
             step_y = R(0) - dy / abs_dx;
-            step_limit = (int32_t)adx;
+            step_limit = to_i32(adx);
         } else {
             step_x = R(0) - dx / abs_dy;
             step_y = dy < R(0) ? R(1) : R(-1);
-            step_limit = (int32_t)ady;
+            step_limit = to_i32(ady);
         }
         tx = R(x);
         ty = R(y);
@@ -230,8 +241,8 @@ static inline void far_advect_target(uint32_t x, uint32_t y, R dx, R dy, const u
         for (int32_t step = 0; step < step_limit; ++step) {
             tx += step_x;
             ty += step_y;
-            int32_t cx = (int32_t)(tx + R(0.5f));
-            int32_t cy = (int32_t)(ty + R(0.5f));
+            int32_t cx = to_i32(tx + R(0.5f));
+            int32_t cy = to_i32(ty + R(0.5f));
             bool hit = true;
             if (cx >= 0 && cy >= 0 && cx < (int32_t)g.X && cy < (int32_t)g.Y)
                 hit = advect_blocked(b, (size_t)cy * g.X + (size_t)cx, heat) != 0;
@@ -298,7 +309,7 @@ static void smooth_advect_pass(const Grid &g, const tpt_air_params &p, const R *
 
             R tx0, ty0;
             far_advect_target<R>(x, y, nvx, nvy, b, g, false, tx0, ty0);
-            int32_t i0 = (int32_t)tx0, j0 = (int32_t)ty0;
+            int32_t i0 = to_i32(tx0), j0 = to_i32(ty0);
             R fx = tx0 - R(i0), fy = ty0 - R(j0);
             if (b[idx] == 0 && i0 >= 2 && i0 < (int32_t)g.X - 3 && j0 >= 2 && j0 < (int32_t)g.Y - 3 && fx >= R(0) &&
                 fy >= R(0)) {
@@ -393,7 +404,7 @@ static void heat_convect_pass(const Grid &g, const tpt_air_params &p, const R *h
 
             R tx, ty;
             far_advect_target<R>(x, y, svx, svy, bh, g, true, tx, ty);
-            int32_t i0 = (int32_t)tx, j0 = (int32_t)ty;
+            int32_t i0 = to_i32(tx), j0 = to_i32(ty);
             R fx = tx - R(i0), fy = ty - R(j0);
             if ((bh[idx] & 0x8u) == 0 && i0 >= 0 && i0 < (int32_t)g.X - 1 && j0 >= 0 && j0 < (int32_t)g.Y - 1 &&
                 fx >= R(0) && fy >= R(0)) {
@@ -852,7 +863,7 @@ int32_t ora_mass_to_fixed(float m) {
     float scaled = m * 65536.0f;
     if (scaled >= 0.0f) scaled += 0.5f;
     else scaled -= 0.5f;
-    return (int32_t)scaled;
+    return to_i32(scaled);
 }
 
 // ---- gravity tick around the solve (host pointers in the ABI structs) ------

@@ -14,7 +14,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def _run(rank, world):
     env = dict(os.environ, RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
     return subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                           "--warmup", "3", "--cpu-seconds", "1"], cwd=ROOT, env=env, capture_output=True, text=True,
+                           "--warmup", "3", "--ref-step-seconds", "0.3"], cwd=ROOT, env=env, capture_output=True, text=True,
                           timeout=600)
 
 
@@ -33,6 +33,11 @@ def test_reference_arm_rank0_prints_one_contract_line():
     assert d["impl"] == "reference" and d["metric"] == "cell-ticks/s" and d["unit"] == "cell-ticks/s"
     assert d["n_gpus"] == 2 and d["steps"] == 1 and d["warmup"] >= 3 and d["higher_is_better"] is True
     assert d["value"] > 0 and d["config"]["workload"].startswith("C5")
+    # the same config keys and values the GPU arm prints for the workload
+    assert d["config"]["instances"] == 128 and d["config"]["cells"] == 6121601
+    assert d["config"]["ticks_per_step"] == 1000
+    # the sample covers both strata of C5: the 400x225 group and the heavy tail
+    assert "of 64 instances" in d["cpu_baseline"]["sample"] and d["cpu_baseline"]["sample"].count("instances (") == 2
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] == "port" and cb["cores"] >= 1 and cb["sample"]
     e2e = d["e2e"]

@@ -109,3 +109,33 @@ def test_gravity_error_c5_batch_both_y_forms(cuda, tf, oracle):
     _dump()
     b.close()
     assert worst <= 1e-4
+
+
+def test_c5_every_instance_air_and_gravity(cuda, tf, oracle):
+    """The whole C5 batch as benchmarked (64 x 400x225 + 64 heavy-tailed,
+    split-BF16 gravity) after 20 ticks: every instance's air bit-exact
+    against the oracle, and every instance's gx/gy within 1e-4 (rel-max and
+    rel-L2, normalised by max|g64|) of FP64."""
+    import workloads as W
+
+    from test_gpu_air import assert_bit_exact
+
+    insts = W.config_instances(5)
+    assert len(insts) == 128
+    b = tf.Batch(insts, tf.PRECISION_SPLIT_BF16)
+    b.step(20)
+    cuda.cuda.synchronize()
+    assert tf.lib().tpt_check_device_errors() == 0
+    worst = (0.0, -1)
+    for i, inst in enumerate(insts):
+        st = b.state(i)
+        assert_bit_exact(st, oracle.air_steps(inst, 20), f"C5 instance {i} ({inst.xcells}x{inst.ycells})")
+        dx, dy = oracle.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx, dtype=np.float64)
+        e = max(*_err(st["gx"], dx), *_err(st["gy"], dy))
+        worst = max(worst, (e, i))
+    REPORT["gravity/split_bf16/C5 batch, all 128 instances, worst"] = {
+        "rel_err": worst[0], "instance": worst[1],
+        "shape": f"{insts[worst[1]].xcells}x{insts[worst[1]].ycells}"}
+    _dump()
+    b.close()
+    assert worst[0] <= 1e-4

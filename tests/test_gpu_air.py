@@ -22,11 +22,17 @@ def run_gpu(tf, torch, inst, ticks, pmap=None, props=None):
     return b.air_state()
 
 
-def assert_bit_exact(got, want, ctx=""):
+def assert_bit_exact(got, want, ctx="", nan_equal=False):
+    """Every bit of pv/vx/vy/hv equal (with nan_equal, a NaN matches any NaN:
+    NaN payloads are not part of the reference's results); masks and emap
+    identical."""
     for k in ("pv", "vx", "vy", "hv"):
         g = np.ascontiguousarray(got[k], np.float32)
         w = np.ascontiguousarray(want[k], np.float32)
-        bad = np.flatnonzero(g.view(np.uint32) != w.view(np.uint32))
+        diff = g.view(np.uint32) != w.view(np.uint32)
+        if nan_equal:
+            diff &= ~(np.isnan(g) & np.isnan(w))
+        bad = np.flatnonzero(diff)
         if bad.size:
             i = bad[0]
             raise AssertionError(f"{ctx} {k}: {bad.size} cells differ, first {i}: gpu {g[i]!r} oracle {w[i]!r}, "
@@ -35,7 +41,7 @@ def assert_bit_exact(got, want, ctx=""):
         assert np.array_equal(got[k], want[k]), f"{ctx} {k}"
 
 
-@pytest.mark.parametrize("ticks", [1, 100])
+@pytest.mark.parametrize("ticks", [1, 100, 1000])
 def test_c1_default_canvas(cuda, tf, oracle, ticks):
     import workloads as W
 
@@ -59,6 +65,48 @@ def test_c2_large_canvas(cuda, tf, oracle):
         done = t
         cuda.cuda.synchronize()
         assert_bit_exact(b.air_state(), s, f"C2 tick {t}")
+
+
+def test_c2_every_tick_to_1000(cuda, tf, oracle):
+    """C2 (400x225) compared against the oracle after every one of its first
+    1000 ticks, GPU and oracle stepping in lock step."""
+    import workloads as W
+
+    inst = W.config_instances(2)[0]
+    b = tf.SimBuffers.from_instance(inst)
+    cur = inst.copy()
+    for t in range(1, 1001):
+        tf.step_air_gpu(b)
+        s = oracle.air_steps(cur, 1)
+        for k in ("pv", "vx", "vy", "hv", "emap", "bair", "bairh"):
+            setattr(cur, k, s[k])
+        cuda.cuda.synchronize()
+        assert_bit_exact(b.air_state(), s, f"C2 tick {t}")
+
+
+def test_c2_10000_ticks(cuda, tf, oracle):
+    """C2's stated horizon: 10000 ticks, compared at the end point."""
+    import workloads as W
+
+    inst = W.config_instances(2)[0]
+    b = tf.SimBuffers.from_instance(inst)
+    for _ in range(10000):
+        tf.step_air_gpu(b)
+    cuda.cuda.synchronize()
+    assert_bit_exact(b.air_state(), oracle.air_steps(inst, 10000), "C2 10000 ticks")
+
+
+def test_nonfinite_and_clamp_inputs(cuda, tf, oracle):
+    """NaN and +-Inf in every state grid, velocities at and far beyond the
+    +-256 clamp: the f32 -> i32 conversions of the walks and samples see NaN
+    and out-of-range values, which round toward zero, saturate, and give 0
+    for NaN on the GPU as in the oracle."""
+    from test_oracle_air_numpy import nonfinite_instance
+
+    inst = nonfinite_instance()
+    for ticks in (1, 3):
+        assert_bit_exact(run_gpu(tf, cuda, inst, ticks), oracle.air_steps(inst, ticks), f"non-finite t{ticks}",
+                         nan_equal=True)
 
 
 MODES = [

@@ -82,6 +82,22 @@ def test_batch_measured_config_subset(cuda, tf, oracle):
     b.close()
 
 
+def test_c4_every_instance_20_ticks(cuda, tf, oracle):
+    """The whole C4 batch (256 instances, W, H log-uniform 32..512, FP32
+    gravity) after 20 ticks: every instance's air bit-exact against the
+    oracle and its gx/gy within 1e-5 of max|g| against FP64."""
+    import workloads as W
+
+    insts = W.config_instances(4)
+    assert len(insts) == 256
+    b = tf.Batch(insts)
+    b.step(20)
+    cuda.cuda.synchronize()
+    assert tf.lib().tpt_check_device_errors() == 0
+    check_against_oracle(tf, oracle, b, insts, 20, "C4")
+    b.close()
+
+
 def test_batch_field_io_round_trip(cuda, tf):
     import workloads as W
 

@@ -73,3 +73,27 @@ def test_partition_balance_and_determinism():
             assert sharding.imbalance(costs, shards) < 1.25
     with pytest.raises(ValueError):
         sharding.partition([1.0], 0)
+
+
+def test_instance_cost_matches_its_flop_formula():
+    """The split-BF16 cost is 3 * (12 X^2 Y + 48 X Y^2) flops (half of the
+    full-spectrum F = 24 X^2 Y + 96 X Y^2, times the three split products)
+    at 2000 flops per air cell-tick, plus the cells."""
+    import sharding
+
+    for x, y in ((400, 225), (32, 36), (512, 41), (153, 96)):
+        flops = 3.0 * (12.0 * x * x * y + 48.0 * x * y * y)
+        assert sharding.instance_cost(x, y) == pytest.approx(x * y + flops / 2000.0, rel=1e-12)
+        assert flops == pytest.approx(1.5 * (24.0 * x * x * y + 96.0 * x * y * y), rel=1e-12)
+        assert sharding.instance_cost(x, y, newton_grav=False) == x * y
+
+
+def test_partition_imbalance_every_world_size():
+    """C5 and C4 shapes split over 2..8 ranks stay within 6% of perfect balance."""
+    import sharding
+    import workloads as W
+
+    for cid in (4, 5):
+        costs = [sharding.instance_cost(x, y) for x, y in W.config_shapes(cid)]
+        for world in range(2, 9):
+            assert sharding.imbalance(costs, sharding.partition(costs, world)) < 1.06

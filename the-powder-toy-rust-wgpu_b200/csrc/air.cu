@@ -1,7 +1,6 @@
 // air.cu -- the one-grid air step (tpt_air_step and its static-scratch
 // variant). Compiled with -fmad=false: see air.cuh.
 #include <algorithm>
-#include <mutex>
 
 #include "air.cuh"
 #include "air_launch.hpp"
@@ -113,25 +112,22 @@ int launch_single(const AirInst &I, const uint32_t *pmap, const uint32_t *props,
 // holds the array (4 MiB) until the process exits.
 static __device__ __align__(256) float g_static_scratch[4 * (size_t)TPT_STATIC_SCRATCH_MAX_CELLS];
 
-// Device address of g_static_scratch on the current device. The name is a
-// host-side stand-in in host code, so the address is looked up once per
-// device with that device current, and cached.
+// Device address of g_static_scratch in the current device's context. The
+// name is a host-side stand-in in host code, so the address is looked up
+// with the device current. It is looked up on every call rather than cached:
+// the lookup allocates nothing, and a cached address would go stale when the
+// context is torn down and recreated (cudaDeviceReset, or a primary-context
+// reset through the driver API), leaving kernels to write through a pointer
+// of the old context.
 static int static_scratch(float **out) {
-    static std::mutex mu;
-    static float *cache[128] = {};
     int dev = 0;
     TPT_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 128) TPT_FAIL(TPT_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
-    std::lock_guard<std::mutex> lock(mu);
-    if (!cache[dev]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            TPT_FAIL(TPT_ERR_CUDA, "cudaGetSymbolAddress(static scratch) failed on device %d: %s", dev,
-                     cudaGetErrorString(e));
-        cache[dev] = static_cast<float *>(p);
-    }
-    *out = cache[dev];
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || p == nullptr)
+        TPT_FAIL(TPT_ERR_CUDA, "cudaGetSymbolAddress(static scratch) failed on device %d: %s", dev,
+                 cudaGetErrorString(e));
+    *out = static_cast<float *>(p);
     return TPT_OK;
 }
 

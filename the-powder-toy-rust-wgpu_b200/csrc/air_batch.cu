@@ -29,6 +29,21 @@ __device__ __forceinline__ void load_box(void *dst, const CUtensorMap *m, int x0
 
 constexpr uint32_t BOX_BYTES = Box::N * 4;
 
+// Error exit of a CTA whose wait on full[k] timed out. Thread 0 may still have
+// bulk copies in flight that write this CTA's shared memory and complete on
+// its mbarriers: the one the failed wait was for, and the prefetch of the next
+// tile into the other buffer (issued before the wait). A CTA must not exit
+// with those outstanding, so thread 0 waits for both phases again (each wait
+// bounded, recording ERR_WAIT_TIMEOUT if it gives up) before every thread
+// returns. `uses` is the phase word after the failed wait was accounted for.
+__device__ __forceinline__ void drain_on_timeout(uint64_t *full, int k, uint32_t uses, bool next_issued) {
+    if (threadIdx.x == 0) {
+        tc::mbar_wait(&full[k], ((uses >> k) & 1u) ^ 1u, &g_air_err);
+        if (next_issued) tc::mbar_wait(&full[k ^ 1], (uses >> (k ^ 1)) & 1u, &g_air_err);
+    }
+    __syncthreads();
+}
+
 // ---- pass A --------------------------------------------------------------------
 // Which grids pass A stages for an instance (0 = none: NoUpdate).
 __device__ __forceinline__ uint32_t a_loads(const AirInst &I) { return I.air_mode == 4u ? 0u : 4u; }
@@ -56,12 +71,14 @@ __global__ void __launch_bounds__(NT) kb_pressure_velocity(const AirInst *__rest
     }
     __syncthreads();
     uint32_t uses = 0;  // bit k: phase parity of full[k] (a register, not an indexed array)
-    auto issue = [&](uint32_t t, int k) {
+    auto issue = [&](uint32_t t, int k) -> bool {
         uint32_t i;
         int x0, y0;
         tile_of(tiles, t, i, x0, y0);
         const AirInst &I = insts[2 * i + parity];
-        if (a_loads(I)) issue_a(I, tmaps + (size_t)i * TM_COUNT, parity, x0, y0, &buf[k], &full[k]);
+        if (!a_loads(I)) return false;
+        issue_a(I, tmaps + (size_t)i * TM_COUNT, parity, x0, y0, &buf[k], &full[k]);
+        return true;
     };
     if (threadIdx.x == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
     int k = 0;
@@ -71,14 +88,18 @@ __global__ void __launch_bounds__(NT) kb_pressure_velocity(const AirInst *__rest
         tile_of(tiles, t, i, x0, y0);
         const AirInst I = insts[2 * i + parity];
         const uint32_t tn = t + gridDim.x;
+        bool next_issued = false;  // thread 0: a bulk copy into buf[k ^ 1] is in flight
         if (threadIdx.x == 0 && tn < ntiles) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            issue(tn, k ^ 1);
+            next_issued = issue(tn, k ^ 1);
         }
         if (!a_loads(I)) continue;
         bool ok = tc::mbar_wait(&full[k], (uses >> k) & 1u, &g_air_err);
         uses ^= 1u << k;
-        if (!__syncthreads_and(ok)) return;
+        if (!__syncthreads_and(ok)) {
+            drain_on_timeout(full, k, uses, next_issued);
+            return;
+        }
         LayoutA2 S{&buf[k], opv};
         pass_a(I, x0, y0, S);
         __syncthreads();
@@ -131,12 +152,14 @@ __global__ void __launch_bounds__(NT, 6) kb_advect_heat(const AirInst *__restric
     }
     __syncthreads();
     uint32_t uses = 0;  // bit k: phase parity of full[k] (a register, not an indexed array)
-    auto issue = [&](uint32_t t, int k) {
+    auto issue = [&](uint32_t t, int k) -> bool {
         uint32_t i;
         int x0, y0;
         tile_of(tiles, t, i, x0, y0);
         const AirInst &I = insts[2 * i + parity];
-        if (b_loads(I)) issue_b(I, tmaps + (size_t)i * TM_COUNT, parity, x0, y0, &buf[k], &full[k]);
+        if (!b_loads(I)) return false;
+        issue_b(I, tmaps + (size_t)i * TM_COUNT, parity, x0, y0, &buf[k], &full[k]);
+        return true;
     };
     if (threadIdx.x == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
     int k = 0;
@@ -146,14 +169,18 @@ __global__ void __launch_bounds__(NT, 6) kb_advect_heat(const AirInst *__restric
         tile_of(tiles, t, i, x0, y0);
         const AirInst I = insts[2 * i + parity];
         const uint32_t tn = t + gridDim.x;
+        bool next_issued = false;  // thread 0: a bulk copy into buf[k ^ 1] is in flight
         if (threadIdx.x == 0 && tn < ntiles) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            issue(tn, k ^ 1);
+            next_issued = issue(tn, k ^ 1);
         }
         if (b_loads(I)) {
             bool ok = tc::mbar_wait(&full[k], (uses >> k) & 1u, &g_air_err);
             uses ^= 1u << k;
-            if (!__syncthreads_and(ok)) return;
+            if (!__syncthreads_and(ok)) {
+                drain_on_timeout(full, k, uses, next_issued);
+                return;
+            }
             LayoutB2 S{&buf[k], &work};
             if (I.air_mode == 4u) {  // stored velocity of the +1 ring for the heat pass
                 for_ring<1>(I, x0, y0, [&](int gx, int gy) {

@@ -13,14 +13,19 @@ from __future__ import annotations
 
 def instance_cost(xcells: int, ycells: int, newton_grav: bool = True) -> float:
     """Relative cost of one tick of one instance: the air step is linear in
-    the cells; the split-BF16 gravity solve is dominated by the y-stage
-    GEMMs, 24 * X * Y^2 * 3 flops on the Hermitian half-spectrum, expressed
-    in cell units at the measured ratio of air to gravity time per cell
-    (about one air cell-tick per 2000 gravity flops)."""
+    the cells; the split-BF16 gravity solve costs the executed flops of the
+    DFT-as-GEMM on the Hermitian half-spectrum, half of the full-spectrum
+    F = 24*X^2*Y + 96*X*Y^2 per solve, times the 3 split products:
+    3 * (12*X^2*Y + 48*X*Y^2), where the x-stage terms are
+    6*X*Y*(2X) = 12*X^2*Y and the y-stage terms 12*Y*(2X)*(2Y) = 48*X*Y^2.
+    Flops are expressed in cell units at the measured ratio of air to
+    gravity time per cell (about one air cell-tick per 2000 gravity flops)."""
     air = float(xcells * ycells)
     if not newton_grav:
         return air
-    grav_flops = 3.0 * (6.0 * xcells * ycells * 2 * xcells + 12.0 * ycells * 2 * xcells * 2 * ycells)
+    x_stage = 6.0 * xcells * ycells * (2 * xcells)            # = 12 X^2 Y
+    y_stage = 12.0 * ycells * (2 * xcells) * (2 * ycells)     # = 48 X Y^2
+    grav_flops = 3.0 * (x_stage + y_stage)
     return air + grav_flops / 2000.0
 
 

@@ -603,6 +603,10 @@ class Batch:
         check(lib().tpt_batch_get_tuning(self._h, ctypes.byref(t)))
         return t
 
+    def tuning_dict(self) -> dict:
+        t = self.tuning()
+        return {name: getattr(t, name) for name, _ in BatchTuning._fields_}
+
     def set_tuning(self, t: BatchTuning):
         check(lib().tpt_batch_set_tuning(self._h, ctypes.byref(t)))
 
