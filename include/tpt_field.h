@@ -342,11 +342,19 @@ int tpt_batch_write_field(tpt_batch *batch, int field, const void *host,
 int tpt_batch_read_field(tpt_batch *batch, int field, void *host,
                          size_t bytes, tpt_stream_t stream);
 
-/* Tuning knobs the autotuner picks (and a caller may pin). */
+/* Tuning knobs the autotuner picks (and a caller may pin). Results are the
+ * same for every value: they change how the work is laid out, not what is
+ * computed. */
 typedef struct tpt_batch_tuning {
-    uint32_t tile_x, tile_y;  /* air tile shape in cells                  */
+    /* The air tick's work unit: a CTA of tile_x lanes (a multiple of 32 in
+     * 64..256) sweeps down strips of about tile_y rows (8..2048). Each lane
+     * owns a column; a strip is at most tile_x - 12 columns wide (six halo
+     * columns on each side), and strips of narrow instances are packed side
+     * by side into one CTA. */
+    uint32_t tile_x, tile_y;
     uint32_t temporal_depth;  /* ticks per air launch (1 = no blocking)   */
-    uint32_t ctas_per_sm;     /* persistent grid size multiplier          */
+    /* Resident sweep CTAs per SM (0 = as many as fit). */
+    uint32_t ctas_per_sm;
     /* Split-BF16 gravity of a batch holding both kinds of y stage (groups of
      * many equal-shape instances take the Toeplitz GEMM, the others the y
      * DFT pair): CTAs per launch of the DFT-pair groups' chain, which then
@@ -374,7 +382,12 @@ int tpt_batch_fields(tpt_batch *batch, uint32_t instance,
  */
 int tpt_batch_step(tpt_batch *batch, uint32_t ticks, tpt_stream_t stream);
 /* Times candidate tunings on the batch's own data (state is saved and
- * restored) and keeps the fastest. Synchronous. */
+ * restored) and keeps the fastest: sweep shapes (tile_x x tile_y) with
+ * their CTAs per SM, then the gravity branch split. The choice is cached in
+ * the process per batch composition -- the instances' (xcells, ycells)
+ * buckets (powers of two) with their counts, and the gravity precision -- so
+ * tuning a batch of the same composition again only applies the cached
+ * settings. Synchronous. */
 int tpt_batch_tune(tpt_batch *batch, tpt_stream_t stream);
 int tpt_batch_get_tuning(const tpt_batch *batch, tpt_batch_tuning *out);
 int tpt_batch_set_tuning(tpt_batch *batch, const tpt_batch_tuning *tuning);

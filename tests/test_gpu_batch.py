@@ -64,10 +64,82 @@ def test_tune_keeps_state_and_results(cuda, tf, oracle):
     b = tf.Batch(insts)
     b.tune()
     t = b.tuning()
-    assert t.ctas_per_sm in (1, 2, 3, 4, 6, 8) and t.temporal_depth == 1
+    assert t.tile_x in (128, 160, 192, 224, 256) and t.tile_y in (32, 64, 128) and t.temporal_depth == 1
+    assert t.ctas_per_sm >= 1
     b.step(5)
     cuda.cuda.synchronize()
     check_against_oracle(tf, oracle, b, insts, 5, "tuned")
+    # a second batch of the same composition takes the cached choice
+    b2 = tf.Batch(insts)
+    b2.tune()
+    assert b2.tuning_dict() == b.tuning_dict()
+    b2.close()
+    b.close()
+
+
+@pytest.mark.parametrize("tile_x,tile_y,per_sm", [(64, 8, 0), (96, 16, 1), (128, 32, 0), (224, 64, 0),
+                                                  (256, 128, 2), (256, 2048, 0)])
+def test_every_sweep_shape_gives_the_same_fields(cuda, tf, oracle, tile_x, tile_y, per_sm):
+    """The sweep's tuning knobs change the work layout only: for every shape
+    (narrow CTAs that split a grid into many column strips, short strips,
+    whole-grid strips) the fields after 9 ticks are bit-exact."""
+    insts = mixed_instances()
+    b = tf.Batch(insts)
+    t = b.tuning()
+    t.tile_x, t.tile_y, t.ctas_per_sm = tile_x, tile_y, per_sm
+    b.set_tuning(t)
+    b.step(9)
+    cuda.cuda.synchronize()
+    assert tf.lib().tpt_check_device_errors() == 0
+    check_against_oracle(tf, oracle, b, insts, 9, f"sweep {tile_x}x{tile_y}")
+    b.close()
+
+
+def test_bad_tunings_are_rejected(cuda, tf):
+    b = tf.Batch(mixed_instances()[:2])
+    for kw in (dict(tile_x=100), dict(tile_x=32), dict(tile_x=288), dict(tile_y=4), dict(temporal_depth=2),
+               dict(ctas_per_sm=64)):
+        t = b.tuning()
+        for k, v in kw.items():
+            setattr(t, k, v)
+        with pytest.raises(tf.TptError):
+            b.set_tuning(t)
+    b.close()
+
+
+def test_packed_narrow_instances_and_modes(cuda, tf, oracle):
+    """Many narrow and short instances packed side by side into shared CTAs
+    (up to eight strips per CTA), in different air modes, next to one wide
+    instance; far-advection samples on every tick."""
+    import workloads as W
+
+    insts = []
+    for k, (X, Y) in enumerate([(3, 3), (5, 40), (9, 9), (17, 33), (31, 8), (32, 36), (40, 12), (12, 70),
+                                (23, 23), (60, 5), (7, 64), (44, 19)]):
+        cfg = W.AirConfig(**[dict(), dict(air_mode=4), dict(aheat_enable=0), dict(convection_mode=1),
+                             dict(vorticity_coeff=2.5), dict(air_mode=2)][k % 6])
+        insts.append(W.make_stress_instance(X, Y, 500 + k, config=cfg))
+    insts.append(W.make_stress_instance(300, 20, 599))
+    b = tf.Batch(insts)
+    for ticks in (1, 3):
+        b.step(ticks)
+    cuda.cuda.synchronize()
+    check_against_oracle(tf, oracle, b, insts, 4, "packed")
+    b.close()
+
+
+def test_nonfinite_inputs_in_a_batch(cuda, tf, oracle):
+    """NaN / Inf state and velocities past the clamp, through the batch's
+    sweep (pointwise and pre-pass far samples included)."""
+    from test_gpu_air import assert_bit_exact
+    from test_oracle_air_numpy import nonfinite_instance
+
+    insts = [nonfinite_instance(), nonfinite_instance(70, 50, 32)]
+    b = tf.Batch(insts)
+    b.step(3)
+    cuda.cuda.synchronize()
+    for i, inst in enumerate(insts):
+        assert_bit_exact(b.state(i), oracle.air_steps(inst, 3), f"non-finite {i}", nan_equal=True)
     b.close()
 
 

@@ -24,8 +24,9 @@
 //
 // The tile code is written once over a shared-memory layout policy `L`:
 // the single-grid kernels stage each array with its own halo (Reg<H>); the
-// batched kernels stage every array as one TMA box of the tile plus a
-// 4-cell (x) by 3-cell (y) halo.
+// batch's velocity pre-pass stages every array as one TMA box of the tile
+// plus a 4-cell (x) by 3-cell (y) halo. The batch's own tick is the row
+// sweep of air_sweep.cu, which reuses the per-cell helpers below.
 #pragma once
 
 #include "common.cuh"
@@ -144,39 +145,6 @@ struct LayoutB1 {
     __device__ __forceinline__ float &NVX(int x, int y, int x0, int y0) { return nvx[Reg<1>::at(x, y, x0, y0)]; }
     __device__ __forceinline__ float &NVY(int x, int y, int x0, int y0) { return nvy[Reg<1>::at(x, y, x0, y0)]; }
     __device__ __forceinline__ float &NPV(int x, int y, int x0, int y0) { return npv[Reg<1>::at(x, y, x0, y0)]; }
-};
-
-struct __align__(128) BoxB {  // batched: one TMA box per array
-    float ovx[Box::NP];  // ovx (or vx when the pressure/velocity pass is off)
-    float ovy[Box::NP];
-    float opv[Box::NP];
-    float hv[Box::NP];
-    uint32_t b[Box::NP];
-    uint32_t bh[Box::NP];
-};
-struct WorkB2 {
-    float vort[Box::N], nvx[Box::N], nvy[Box::N], npv[Box::N];
-};
-struct LayoutB2 {
-    BoxB *in;
-    WorkB2 *w;
-    // every staged grid covers the whole box
-    __device__ __forceinline__ static bool has3(int x, int y, int x0, int y0) {
-        return x >= x0 - Box::HX && x < x0 + TX + Box::HX && y >= y0 - Box::HY && y < y0 + TY + Box::HY;
-    }
-    __device__ __forceinline__ static bool hasH(int x, int y, int x0, int y0) { return has3(x, y, x0, y0); }
-    __device__ __forceinline__ bool blk(int x, int y, int x0, int y0) const { return in->b[Box::at(x, y, x0, y0)] != 0u; }
-    __device__ __forceinline__ bool hblk(int x, int y, int x0, int y0) const {
-        return (in->bh[Box::at(x, y, x0, y0)] & 0x8u) != 0u;
-    }
-    __device__ __forceinline__ float OVX(int x, int y, int x0, int y0) const { return in->ovx[Box::at(x, y, x0, y0)]; }
-    __device__ __forceinline__ float OVY(int x, int y, int x0, int y0) const { return in->ovy[Box::at(x, y, x0, y0)]; }
-    __device__ __forceinline__ float OPV(int x, int y, int x0, int y0) const { return in->opv[Box::at(x, y, x0, y0)]; }
-    __device__ __forceinline__ float HV(int x, int y, int x0, int y0) const { return in->hv[Box::at(x, y, x0, y0)]; }
-    __device__ __forceinline__ float &VORT(int x, int y, int x0, int y0) { return w->vort[Box::at(x, y, x0, y0)]; }
-    __device__ __forceinline__ float &NVX(int x, int y, int x0, int y0) { return w->nvx[Box::at(x, y, x0, y0)]; }
-    __device__ __forceinline__ float &NVY(int x, int y, int x0, int y0) { return w->nvy[Box::at(x, y, x0, y0)]; }
-    __device__ __forceinline__ float &NPV(int x, int y, int x0, int y0) { return w->npv[Box::at(x, y, x0, y0)]; }
 };
 
 // ---- staging by loads (single-grid path) -------------------------------------

@@ -8,27 +8,69 @@
 namespace tpt {
 namespace air {
 
-// One AIR_TX x AIR_TY tile of one batched instance.
+// One AIR_TX x AIR_TY tile of one batched instance (the pre-pass and the
+// copy-back walk these).
 struct TileRef {
     uint32_t inst;
     uint16_t tx, ty;
 };
 
-// Tensor maps of one batched instance: the grids pass A and pass B stage,
-// with the two halves of the heat and mask ping-pong.
-enum TensorMapSlot {
-    TM_PV, TM_VX, TM_VY, TM_OVX, TM_OVY, TM_OPV, TM_BA0, TM_BA1, TM_BH0, TM_BH1, TM_HV0, TM_HV1, TM_COUNT
+// Tensor maps of one batched instance: the grids the pre-pass stages, both
+// halves of each ping-pong pair.
+enum TensorMapSlot { TM_PV0, TM_PV1, TM_VX0, TM_VX1, TM_VY0, TM_VY1, TM_BA0, TM_BA1, TM_COUNT };
+
+// ---- row sweeps (air_sweep.cu) -------------------------------------------------
+// Lanes of halo on each side of a segment: the tick's stencil reaches six
+// columns (block_air of the effective velocity's wall clear, five more stages
+// of one column each).
+constexpr int SW_H = 6;
+constexpr int SW_MAXSEG = 8;          // segments packed into one work item
+constexpr int SWEEP_MAX_LANES = 256;  // lanes (threads) of a sweep CTA
+constexpr int SWEEP_RING_ROWS = 42;   // shared-memory rows of NL + 2 words each
+
+// A column strip of one instance inside a work item: lanes [lane0, lane0 +
+// lanes) hold columns x0 - SW_H .. x0 + nx + SW_H - 1; output columns x0 ..
+// x0 + nx - 1 and rows y0 .. y0 + ny - 1.
+struct SweepSeg {
+    uint32_t inst;
+    uint16_t lane0, lanes;
+    uint16_t x0, nx;
+    uint16_t y0, ny;
 };
+struct SweepItem {
+    uint32_t nseg;
+    uint32_t steps;  // max ny over the segments
+    SweepSeg seg[SW_MAXSEG];
+};
+
+// Everything one tick of the sweep form needs.
+struct SweepLaunch {
+    const AirInst *insts;       // two per instance (parity 0 and 1 of the ping-pong pairs)
+    const CUtensorMap *tmaps;   // TM_COUNT per instance
+    const TileRef *tiles;       // pre-pass tiles
+    uint32_t ntiles;
+    const SweepItem *items;
+    uint32_t nitems;
+    uint32_t ninst;
+    uint32_t lanes;             // threads per sweep CTA (multiple of 32, <= SWEEP_MAX_LANES)
+    uint32_t grid;              // sweep CTAs
+    uint32_t prepass_grid;      // pre-pass CTAs
+    uint32_t *ctl;              // [0]: the sweep's work-queue counter
+    uint32_t *want;             // [2][ninst]: pre-pass flags per tick parity
+};
+
+// One tick of every instance of a batch: the pre-pass of flagged instances,
+// then the sweep. `parity` selects the ping-pong halves read.
+int launch_sweep_tick(const SweepLaunch &s, uint32_t parity, cudaStream_t st);
+int launch_prepass(const SweepLaunch &s, uint32_t parity, cudaStream_t st);
+int sweep_max_ctas_per_sm(uint32_t lanes, int *out);
 
 // One tick of one grid: A (pressure+velocity), B (advection+heat), settle.
 int launch_single(const AirInst &I, const uint32_t *pmap, const uint32_t *props, uint32_t nprops, uint32_t xres,
                   uint32_t yres, cudaStream_t st);
 
-// One tick of every instance of a batch. `insts` holds two AirInst per
-// instance (parity 0 and 1 of the hv / mask ping-pong); `tmaps` TM_COUNT
-// tensor maps per instance.
-int launch_batch_tick(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles,
-                      uint32_t grid, uint32_t parity, bool any_noupdate_heat, cudaStream_t st);
+// Copies the ping-pong halves that hold the newest state back to the
+// instance's canonical buffers (after an odd number of ticks).
 int launch_copy_back(const AirInst *insts, const TileRef *tiles, uint32_t ntiles, uint32_t grid, cudaStream_t st);
 
 // Reads and clears the device error word of the batched air kernels.

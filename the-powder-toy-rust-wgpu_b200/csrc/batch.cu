@@ -4,13 +4,15 @@
 // arenas (f32, u32, i32). Instance i's grids are `ycells` rows of
 // `pitch_i` elements (pitch = xcells rounded up to 32, so rows start on
 // 128-byte boundaries as TMA needs); cell (cx, cy) is at cy * pitch + cx.
-// Ambient heat and the two wall masks have a second copy (ping-pong), so a
-// tick is two air launches over a tile list of all instances (no settle
-// pass); after an odd tick count one copy-back restores the canonical
-// buffers. Gravity (instances with newton_grav) is independent of air in
-// the field step (crates/tpt-sim/src/air_kernel/heat.rs:182-203 uses the
-// configured direction, not the Newtonian field), so it runs on a second
-// stream branch of the captured graph, concurrently with the air chain.
+// The air state (pv, vx, vy, hv and the two wall masks) has a second copy
+// (ping-pong): a tick reads one half and writes the other, so the whole air
+// tick is one sweep launch (air_sweep.cu) plus a velocity pre-pass that only
+// works for instances flagged by the previous tick; after an odd tick count
+// one copy-back restores the canonical buffers. Gravity (instances with
+// newton_grav) is independent of air in the field step
+// (crates/tpt-sim/src/air_kernel/heat.rs:182-203 uses the configured
+// direction, not the Newtonian field), so it runs on a second stream branch
+// of the captured graph, concurrently with the air chain.
 //
 // N ticks are captured once into a CUDA graph (in chunks of CHUNK ticks so
 // instantiation stays cheap) and replayed on later calls.
@@ -18,6 +20,7 @@
 
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <vector>
 
 #include "air_launch.hpp"
@@ -31,7 +34,7 @@ namespace {
 constexpr uint32_t CHUNK = 50;  // ticks per captured graph (even)
 constexpr size_t ALIGN = 64;    // elements (256 B) between instances
 
-enum F32 { F_PV, F_VX, F_VY, F_HV, F_HV2, F_OPV, F_OVX, F_OVY, F_FVX, F_FVY, F_GX, F_GY, F_N32 };
+enum F32 { F_PV, F_VX, F_VY, F_HV, F_PV2, F_VX2, F_VY2, F_HV2, F_OPV, F_OVX, F_OVY, F_FVX, F_FVY, F_GX, F_GY, F_N32 };
 enum U32 { U_BA, U_BH, U_BA2, U_BH2, U_WALL, U_EMAP, U_EA, U_EH, U_GMASK, U_NU32 };
 
 size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
@@ -62,6 +65,74 @@ __global__ void k_batch_io(const IoInst *io, uint32_t base, uint32_t *arena, uin
 }
 }  // namespace
 
+// Default sweep shape: 224 lanes (a 400-column grid in two 200-column strips
+// plus halos) by 64-row strips.
+constexpr uint32_t DEFAULT_LANES = 224, DEFAULT_ROWS = 64;
+
+// Splits every instance into column strips of at most lanes - 2 * SW_H
+// columns and row strips of about `rows` rows (sizes balanced within an
+// instance), then packs the strips side by side into work items of `lanes`
+// lanes: strips sorted by height, next fit, at most SW_MAXSEG per item. Items
+// are returned largest first (the work queue hands them out in this order).
+static std::vector<air::SweepItem> plan_sweep(const std::vector<tpt_instance_desc> &descs, uint32_t lanes,
+                                              uint32_t rows) {
+    struct Strip {
+        uint32_t inst;
+        uint16_t x0, nx, y0, ny;
+    };
+    std::vector<Strip> strips;
+    const uint32_t maxw = lanes - 2 * air::SW_H;
+    for (uint32_t i = 0; i < (uint32_t)descs.size(); ++i) {
+        const uint32_t X = descs[i].air.xcells, Y = descs[i].air.ycells;
+        const uint32_t nc = (X + maxw - 1) / maxw;
+        const uint32_t nr = std::max<uint32_t>(1u, (Y + rows / 2) / rows);
+        uint32_t x = 0;
+        for (uint32_t k = 0; k < nc; ++k) {
+            const uint32_t w = X / nc + (k < X % nc ? 1u : 0u);
+            uint32_t y = 0;
+            for (uint32_t j = 0; j < nr; ++j) {
+                const uint32_t h = Y / nr + (j < Y % nr ? 1u : 0u);
+                strips.push_back({i, (uint16_t)x, (uint16_t)w, (uint16_t)y, (uint16_t)h});
+                y += h;
+            }
+            x += w;
+        }
+    }
+    std::stable_sort(strips.begin(), strips.end(), [](const Strip &a, const Strip &b) {
+        return a.ny != b.ny ? a.ny > b.ny : a.nx > b.nx;
+    });
+    std::vector<air::SweepItem> items;
+    air::SweepItem cur{};
+    uint32_t used = 0;
+    for (const Strip &t : strips) {
+        const uint32_t need = t.nx + 2u * air::SW_H;
+        if (cur.nseg == (uint32_t)air::SW_MAXSEG || (cur.nseg && used + need > lanes)) {
+            items.push_back(cur);
+            cur = air::SweepItem{};
+            used = 0;
+        }
+        air::SweepSeg &g = cur.seg[cur.nseg++];
+        g.inst = t.inst;
+        g.lane0 = (uint16_t)used;
+        g.lanes = (uint16_t)need;
+        g.x0 = t.x0;
+        g.nx = t.nx;
+        g.y0 = t.y0;
+        g.ny = t.ny;
+        cur.steps = std::max<uint32_t>(cur.steps, t.ny);
+        used += need;
+    }
+    if (cur.nseg) items.push_back(cur);
+    auto work = [](const air::SweepItem &it) {
+        uint32_t lanes_used = 0;
+        for (uint32_t k = 0; k < it.nseg; ++k) lanes_used += it.seg[k].lanes;
+        return (uint64_t)(it.steps + 13u) * lanes_used;
+    };
+    std::stable_sort(items.begin(), items.end(),
+                     [&](const air::SweepItem &a, const air::SweepItem &b) { return work(a) > work(b); });
+    return items;
+}
+
 struct tpt_batch {
     uint32_t n = 0;
     int precision = TPT_PRECISION_FP32;
@@ -77,9 +148,15 @@ struct tpt_batch {
     CUtensorMap *tmaps = nullptr;
     air::TileRef *tiles = nullptr;
     uint32_t ntiles = 0;
-    bool any_noupdate_heat = false;
+    // the sweep form of the air tick: work items (device), the queue counter
+    // and the pre-pass flags ([2][n], zeroed at creation)
+    air::SweepItem *items = nullptr;
+    uint32_t nitems = 0;
+    uint32_t *ctl = nullptr;
+    uint32_t *want = nullptr;
     bool any_grav = false;
-    tpt_batch_tuning tuning{AIR_TX, AIR_TY, 1, 4, 0};
+    tpt_batch_tuning tuning{DEFAULT_LANES, DEFAULT_ROWS, 1, 0, 0};
+    int sweep_occupancy = 1;  // resident sweep CTAs per SM at tuning.tile_x lanes
     int sms = 148;
     gfft::FftSet fft;
     dft::DftSet dft;
@@ -95,12 +172,26 @@ struct tpt_batch {
 
     float *f(int field, uint32_t i) const { return f32 + (size_t)field * stride + off[i]; }
     uint32_t *u(int field, uint32_t i) const { return u32 + (size_t)field * stride + off[i]; }
-    uint32_t grid() const {
-        return std::min<uint32_t>(ntiles, (uint32_t)sms * std::max<uint32_t>(tuning.ctas_per_sm, 1));
+    // CTAs of the tile-walking launches (pre-pass, copy-back)
+    uint32_t grid() const { return std::min<uint32_t>(ntiles, (uint32_t)sms * 4u); }
+    air::SweepLaunch sweep() const {
+        air::SweepLaunch L{};
+        L.insts = insts;
+        L.tmaps = tmaps;
+        L.tiles = tiles;
+        L.ntiles = ntiles;
+        L.items = items;
+        L.nitems = nitems;
+        L.ninst = n;
+        L.lanes = tuning.tile_x;
+        const uint32_t per_sm = tuning.ctas_per_sm ? tuning.ctas_per_sm : (uint32_t)sweep_occupancy;
+        L.grid = std::max<uint32_t>(1u, std::min<uint32_t>(nitems, (uint32_t)sms * per_sm));
+        L.prepass_grid = grid();
+        L.ctl = ctl;
+        L.want = want;
+        return L;
     }
-    int air_tick(uint32_t parity, cudaStream_t st) const {
-        return air::launch_batch_tick(insts, tmaps, tiles, ntiles, grid(), parity, any_noupdate_heat, st);
-    }
+    int air_tick(uint32_t parity, cudaStream_t st) const { return air::launch_sweep_tick(sweep(), parity, st); }
     int grav_solve(cudaStream_t st) const {
         return precision == TPT_PRECISION_FP32 ? fft.launch(st) : dft.launch(st);
     }
@@ -119,6 +210,8 @@ struct tpt_batch {
         cudaFree(io);
         cudaFree(tmaps);
         cudaFree(tiles);
+        cudaFree(items);
+        cudaFree(ctl);
         if (side) cudaStreamDestroy(side);
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
@@ -235,6 +328,30 @@ struct StateCopy {
     }
 };
 
+// Plans the sweep's work items for `lanes` x `rows` and uploads them; reads
+// the sweep kernel's occupancy at that width.
+static int set_sweep_shape(tpt_batch *b, uint32_t lanes, uint32_t rows) {
+    std::vector<air::SweepItem> items = plan_sweep(b->descs, lanes, rows);
+    int occ = 0;
+    int rc = air::sweep_max_ctas_per_sm(lanes, &occ);
+    if (rc) return rc;
+    if (occ < 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "the sweep kernel does not fit an SM at %u lanes", lanes);
+    air::SweepItem *d = nullptr;
+    TPT_CUDA(cudaMalloc(&d, items.size() * sizeof(air::SweepItem)));
+    cudaError_t e = cudaMemcpy(d, items.data(), items.size() * sizeof(air::SweepItem), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        TPT_FAIL(TPT_ERR_CUDA, "sweep item upload failed: %s", cudaGetErrorString(e));
+    }
+    cudaFree(b->items);
+    b->items = d;
+    b->nitems = (uint32_t)items.size();
+    b->sweep_occupancy = occ;
+    b->tuning.tile_x = lanes;
+    b->tuning.tile_y = rows;
+    return TPT_OK;
+}
+
 extern "C" {
 
 int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, tpt_batch **out) {
@@ -298,9 +415,6 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
         const tpt_air_params &p = descs[i].air;
         AirInst I = make_air_inst(p);
         I.pitch = b->pitch[i];
-        I.pv = b->f(F_PV, i);
-        I.vx = b->f(F_VX, i);
-        I.vy = b->f(F_VY, i);
         I.opv = b->f(F_OPV, i);
         I.ovx = b->f(F_OVX, i);
         I.ovy = b->f(F_OVY, i);
@@ -313,6 +427,12 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
         I.fvy = b->f(F_FVY, i);
         for (int par = 0; par < 2; ++par) {
             AirInst J = I;
+            J.pv = b->f(par ? F_PV2 : F_PV, i);
+            J.vx = b->f(par ? F_VX2 : F_VX, i);
+            J.vy = b->f(par ? F_VY2 : F_VY, i);
+            J.pv_out = b->f(par ? F_PV : F_PV2, i);
+            J.vx_out = b->f(par ? F_VX : F_VX2, i);
+            J.vy_out = b->f(par ? F_VY : F_VY2, i);
             if (p.aheat_enable) {
                 J.hv = b->f(par ? F_HV2 : F_HV, i);
                 J.hv_out = b->f(par ? F_HV : F_HV2, i);
@@ -325,7 +445,7 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
             J.bairh_out = b->u(par ? U_BH : U_BH2, i);
             b->insts_host[2 * (size_t)i + par] = J;
         }
-        // tensor maps of the grids the two passes stage (box = tile + halo)
+        // tensor maps of the grids the velocity pre-pass stages (box = tile + halo)
         CUtensorMap *m = &tm[(size_t)i * air::TM_COUNT];
         const uint32_t X = p.xcells, Y = p.ycells, P = b->pitch[i];
         const uint32_t BW = AIR_TX + 8, BH = AIR_TY + 6;
@@ -334,19 +454,15 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
             const void *base;
             bool f;
         } slots[] = {
-            {air::TM_PV, b->f(F_PV, i), true},        {air::TM_VX, b->f(F_VX, i), true},
-            {air::TM_VY, b->f(F_VY, i), true},        {air::TM_OVX, b->f(F_OVX, i), true},
-            {air::TM_OVY, b->f(F_OVY, i), true},      {air::TM_OPV, b->f(F_OPV, i), true},
-            {air::TM_BA0, b->u(U_BA, i), false},      {air::TM_BA1, b->u(U_BA2, i), false},
-            {air::TM_BH0, b->u(U_BH, i), false},      {air::TM_BH1, b->u(U_BH2, i), false},
-            {air::TM_HV0, b->insts_host[2 * (size_t)i].hv, true},
-            {air::TM_HV1, b->insts_host[2 * (size_t)i + 1].hv, true},
+            {air::TM_PV0, b->f(F_PV, i), true},  {air::TM_PV1, b->f(F_PV2, i), true},
+            {air::TM_VX0, b->f(F_VX, i), true},  {air::TM_VX1, b->f(F_VX2, i), true},
+            {air::TM_VY0, b->f(F_VY, i), true},  {air::TM_VY1, b->f(F_VY2, i), true},
+            {air::TM_BA0, b->u(U_BA, i), false}, {air::TM_BA1, b->u(U_BA2, i), false},
         };
         for (const Slot &s : slots) {
             rc = make_grid_tmap(&m[s.slot], s.base, s.f, X, Y, P, BW, BH);
             if (rc) return bail(rc);
         }
-        if (p.air_mode == 4u && p.aheat_enable) b->any_noupdate_heat = true;
         for (uint32_t ty = 0; ty * AIR_TY < p.ycells; ++ty)
             for (uint32_t tx = 0; tx * AIR_TX < p.xcells; ++tx) tiles.push_back({i, (uint16_t)tx, (uint16_t)ty});
         if (descs[i].newton_grav) {
@@ -362,6 +478,8 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     if (e == cudaSuccess)
         e = cudaMemcpy(b->tiles, tiles.data(), tiles.size() * sizeof(air::TileRef), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(b->tmaps, tm.data(), tm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&b->ctl, (1 + 2 * (size_t)n) * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(b->ctl, 0, (1 + 2 * (size_t)n) * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
@@ -369,6 +487,9 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
         set_error("batch setup failed: %s", cudaGetErrorString(e));
         return bail(TPT_ERR_CUDA);
     }
+    b->want = b->ctl + 1;
+    rc = set_sweep_shape(b, b->tuning.tile_x, b->tuning.tile_y);
+    if (rc) return bail(rc);
     b->any_grav = !gshapes.empty();
     if (b->any_grav) {
         if (precision == TPT_PRECISION_FP32) {
@@ -539,10 +660,14 @@ int tpt_batch_get_tuning(const tpt_batch *b, tpt_batch_tuning *t) {
 
 int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
     if (!b || !t) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_set_tuning: NULL pointer");
-    if (t->tile_x != AIR_TX || t->tile_y != AIR_TY)
-        TPT_FAIL(TPT_ERR_UNSUPPORTED, "tile %ux%u not built (only %dx%d)", t->tile_x, t->tile_y, AIR_TX, AIR_TY);
+    if (t->tile_x < 64 || t->tile_x > (uint32_t)air::SWEEP_MAX_LANES || t->tile_x % 32u)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "tile_x (sweep lanes) %u must be a multiple of 32 in 64..%d", t->tile_x,
+                 air::SWEEP_MAX_LANES);
+    if (t->tile_y < 8 || t->tile_y > TPT_MAX_CELLS_PER_SIDE)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "tile_y (rows per strip) %u must be in 8..%u", t->tile_y,
+                 TPT_MAX_CELLS_PER_SIDE);
     if (t->temporal_depth != 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "temporal depth %u not built", t->temporal_depth);
-    if (t->ctas_per_sm < 1 || t->ctas_per_sm > 32) TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm must be 1..32");
+    if (t->ctas_per_sm > 32) TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm must be 0 (as many as fit) .. 32");
     const bool split = b->any_grav && b->precision == TPT_PRECISION_SPLIT_BF16 && b->dft.can_split();
     if (t->grav_side_ctas && !split)
         TPT_FAIL(TPT_ERR_INVALID_ARG, "grav_side_ctas must be 0: the batch's gravity has one kind of y stage");
@@ -550,7 +675,14 @@ int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
         int rc = b->dft.set_side_ctas(t->grav_side_ctas);
         if (rc) return rc;
     }
-    if (t->ctas_per_sm != b->tuning.ctas_per_sm || t->grav_side_ctas != b->tuning.grav_side_ctas) b->drop_graphs();
+    if (t->tile_x != b->tuning.tile_x || t->tile_y != b->tuning.tile_y) {
+        int rc = set_sweep_shape(b, t->tile_x, t->tile_y);
+        if (rc) return rc;
+    }
+    if (t->ctas_per_sm > (uint32_t)b->sweep_occupancy)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm %u exceeds the %d sweep CTAs of %u lanes that fit an SM",
+                 t->ctas_per_sm, b->sweep_occupancy, t->tile_x);
+    b->drop_graphs();
     b->tuning = *t;
     return TPT_OK;
 }
@@ -569,7 +701,7 @@ int tpt_batch_profile_phases(tpt_batch *b, uint32_t ticks, tpt_stream_t stream, 
         out->cells += c;
         if (b->descs[i].newton_grav) out->grav_cells += c;
     }
-    out->air_launches_per_tick = b->any_noupdate_heat ? 3 : 2;
+    out->air_launches_per_tick = 2;  // velocity pre-pass (flagged instances only) + sweep
     out->grav_launches_per_tick = b->any_grav ? (b->precision == TPT_PRECISION_FP32 ? 3 : b->dft.launches()) : 0;
     out->grav_flops_per_tick = b->any_grav && b->precision != TPT_PRECISION_FP32 ? b->dft.flops() : 0.0;
     cudaEvent_t e0, e1, e2;
@@ -594,8 +726,43 @@ int tpt_batch_profile_phases(tpt_batch *b, uint32_t ticks, tpt_stream_t stream, 
     return rc ? rc : rc2;
 }
 
+// Tuned settings per batch composition: the shapes' (W, H) buckets
+// (powers of two) with their counts, and the gravity precision. A batch whose
+// instances fall in the same buckets reuses the tuned settings without
+// timing.
+struct TuneKey {
+    int precision;
+    std::vector<std::pair<uint32_t, uint32_t>> buckets;  // (log2 W << 8 | log2 H, count), sorted
+    bool operator<(const TuneKey &o) const {
+        return precision != o.precision ? precision < o.precision : buckets < o.buckets;
+    }
+};
+static std::mutex g_tune_mu;
+static std::map<TuneKey, tpt_batch_tuning> g_tune_cache;
+
+static uint32_t log2_bucket(uint32_t v) {
+    uint32_t k = 0;
+    while ((2u << k) <= v) ++k;
+    return k;
+}
+
+static TuneKey tune_key(const tpt_batch *b) {
+    std::map<uint32_t, uint32_t> h;
+    for (const auto &d : b->descs) ++h[log2_bucket(d.air.xcells) << 8 | log2_bucket(d.air.ycells)];
+    TuneKey k;
+    k.precision = b->any_grav ? b->precision : -1;
+    k.buckets.assign(h.begin(), h.end());
+    return k;
+}
+
 int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
     if (!b) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_tune: batch is NULL");
+    const TuneKey key = tune_key(b);
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) return tpt_batch_set_tuning(b, &it->second);
+    }
     cudaStream_t st = (cudaStream_t)stream;
     StateCopy saved;
     int src = saved.save(b, st);
@@ -603,35 +770,50 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    const uint32_t cands[] = {1, 2, 3, 4, 6, 8};
+    // Phase 1: the sweep's shape (lanes per CTA x rows per strip) and its
+    // resident CTAs per SM, by timing 20 air ticks of each candidate.
+    const uint32_t lane_c[] = {128, 160, 192, 224, 256};
+    const uint32_t row_c[] = {32, 64, 128};
     tpt_batch_tuning best = b->tuning;
     float best_ms = 1e30f;
     int rc = TPT_OK;
-    for (uint32_t c : cands) {
-        tpt_batch_tuning t = b->tuning;
-        t.ctas_per_sm = c;
-        rc = tpt_batch_set_tuning(b, &t);
-        if (rc) break;
-        const uint32_t trial = 20;
-        for (int rep = 0; rep < 2 && rc == TPT_OK; ++rep) {  // warm-up, then timed
-            cudaEventRecord(e0, st);
-            for (uint32_t k = 0; k < trial && rc == TPT_OK; ++k) rc = b->air_tick(k & 1u, st);
-            cudaEventRecord(e1, st);
+    for (uint32_t lanes : lane_c) {
+        for (uint32_t rows : row_c) {
+            tpt_batch_tuning t = b->tuning;
+            t.tile_x = lanes;
+            t.tile_y = rows;
+            t.ctas_per_sm = 0;
+            rc = tpt_batch_set_tuning(b, &t);
+            if (rc) break;
+            const uint32_t occ = (uint32_t)b->sweep_occupancy;
+            for (uint32_t per_sm = occ; per_sm + 1 >= occ && per_sm >= 1 && rc == TPT_OK; --per_sm) {
+                t.ctas_per_sm = per_sm;
+                rc = tpt_batch_set_tuning(b, &t);
+                const uint32_t trial = 20;
+                for (int rep = 0; rep < 2 && rc == TPT_OK; ++rep) {  // warm-up, then timed
+                    cudaEventRecord(e0, st);
+                    for (uint32_t k = 0; k < trial && rc == TPT_OK; ++k) rc = b->air_tick(k & 1u, st);
+                    cudaEventRecord(e1, st);
+                }
+                if (rc) break;
+                cudaEventSynchronize(e1);
+                float ms = 0;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = t;
+                }
+                if (per_sm == 1) break;
+            }
+            if (rc) break;
         }
         if (rc) break;
-        cudaEventSynchronize(e1);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best_ms) {
-            best_ms = ms;
-            best = t;
-        }
     }
-    // Then, with that air grid, the gravity split: the graph a step replays
-    // (air and gravity chains together) per candidate CTA count of the
+    // Phase 2, with that air shape: the gravity split -- the graph a step
+    // replays (air and gravity chains together) per candidate CTA count of the
     // DFT-pair groups' branch, 0 (one stream) included.
+    if (rc == TPT_OK) rc = tpt_batch_set_tuning(b, &best);
     if (rc == TPT_OK && b->any_grav && b->precision == TPT_PRECISION_SPLIT_BF16 && b->dft.can_split()) {
-        rc = tpt_batch_set_tuning(b, &best);
         const uint32_t cap = b->dft.max_side_ctas();
         const uint32_t pcts[] = {0, 10, 15, 20, 25, 33, 40, 50};  // side CTAs, percent of the SMs (0: no split)
         float split_best = 1e30f;
@@ -669,7 +851,12 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
     int rrc = saved.restore(b, st);
     if (rc) return rc;
     if (rrc) return rrc;
-    return tpt_batch_set_tuning(b, &best);
+    rc = tpt_batch_set_tuning(b, &best);
+    if (rc == TPT_OK) {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_cache[key] = best;
+    }
+    return rc;
 }
 
 }  // extern "C"

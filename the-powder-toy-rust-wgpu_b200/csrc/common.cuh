@@ -66,6 +66,9 @@ struct AirInst {
     // for a batch they are the other half of a ping-pong pair.
     uint32_t *bair_out, *bairh_out;
     float *hv_out;
+    // the batch's sweep writes the new pv/vx/vy to the other half of their
+    // ping-pong pairs (the one-grid step updates pv/vx/vy in place: null)
+    float *pv_out, *vx_out, *vy_out;
 };
 
 // AirInst with the scalar fields of `p` set and every pointer null.
