@@ -34,8 +34,12 @@ def rel_max(a, b):
     return np.abs(a.astype(np.float64) - b).max() / max(np.abs(b).max(), 1e-30)
 
 
-@pytest.mark.parametrize("X,Y,seed", [(24, 24, 1), (64, 48, 2), (37, 29, 3), (153, 96, 4)])
+@pytest.mark.parametrize("X,Y,seed", [(24, 24, 1), (64, 48, 2), (37, 29, 3), (153, 96, 4), (5, 7, 5),
+                                      (16, 3, 6), (600, 40, 7), (40, 520, 8)])
 def test_fp32_plan_stress(cuda, tf, oracle, X, Y, seed):
+    """Shapes of both FFT forms: padded lengths 32..1024 (one warp per 1-D
+    transform; 5x7 and 16x3 are padded up to 32) and longer ones (600 and 520
+    cells: 2048-point transforms in shared memory)."""
     import workloads as W
 
     g = W.make_stress_instance(X, Y, seed)

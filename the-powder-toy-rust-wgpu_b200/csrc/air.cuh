@@ -22,11 +22,10 @@
 // The one global dependency of a tick is between A and B: the far-advection
 // sample can reach any cell of ovx/ovy (0.7*|v| <= 179 cells).
 //
-// The tile code is written once over a shared-memory layout policy `L`:
-// the single-grid kernels stage each array with its own halo (Reg<H>); the
-// batch's velocity pre-pass stages every array as one TMA box of the tile
-// plus a 4-cell (x) by 3-cell (y) halo. The batch's own tick is the row
-// sweep of air_sweep.cu, which reuses the per-cell helpers below.
+// The tile code is written over a shared-memory layout policy `L`: the
+// single-grid kernels and the batch's velocity pre-pass stage each array with
+// its own halo (Reg<H>). The batch's own tick is the row sweep of
+// air_sweep.cu, which reuses the per-cell helpers below.
 #pragma once
 
 #include "common.cuh"
@@ -44,16 +43,6 @@ template <int H> struct Reg {
     static constexpr int N = W * HGT;
     __device__ static __forceinline__ int at(int gx, int gy, int x0, int y0) {
         return (gy - y0 + H) * W + (gx - x0 + H);
-    }
-};
-
-// The TMA box of the batched kernels: x halo 4 (keeps the box start 16-byte
-// aligned), y halo 3.
-struct Box {
-    static constexpr int HX = 4, HY = 3, W = TX + 2 * HX, HGT = TY + 2 * HY, N = W * HGT;
-    static constexpr int NP = (N + 31) / 32 * 32;  // array stride: TMA destinations are 128-byte aligned
-    __device__ static __forceinline__ int at(int gx, int gy, int x0, int y0) {
-        return (gy - y0 + HY) * W + (gx - x0 + HX);
     }
 };
 
@@ -99,22 +88,6 @@ struct LayoutA1 {  // single grid: per-array halos, masks as flags
     __device__ __forceinline__ float &VY(int x, int y, int x0, int y0) { return vy[Reg<2>::at(x, y, x0, y0)]; }
     __device__ __forceinline__ float PV(int x, int y, int x0, int y0) const { return pv[Reg<1>::at(x, y, x0, y0)]; }
     __device__ __forceinline__ float &OPV(int x, int y, int x0, int y0) { return opv[Reg<1>::at(x, y, x0, y0)]; }
-};
-
-struct __align__(128) BoxA {  // batched: one TMA box per array
-    float pv[Box::NP];
-    float vx[Box::NP];
-    float vy[Box::NP];
-    uint32_t b[Box::NP];
-};
-struct LayoutA2 {
-    BoxA *in;
-    float *opv;  // Box::N
-    __device__ __forceinline__ bool blk(int x, int y, int x0, int y0) const { return in->b[Box::at(x, y, x0, y0)] != 0u; }
-    __device__ __forceinline__ float &VX(int x, int y, int x0, int y0) { return in->vx[Box::at(x, y, x0, y0)]; }
-    __device__ __forceinline__ float &VY(int x, int y, int x0, int y0) { return in->vy[Box::at(x, y, x0, y0)]; }
-    __device__ __forceinline__ float PV(int x, int y, int x0, int y0) const { return in->pv[Box::at(x, y, x0, y0)]; }
-    __device__ __forceinline__ float &OPV(int x, int y, int x0, int y0) { return opv[Box::at(x, y, x0, y0)]; }
 };
 
 // Pass B working set: staged ovx/ovy/opv/hv, the two masks, and the

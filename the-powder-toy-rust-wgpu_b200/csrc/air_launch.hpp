@@ -1,8 +1,6 @@
 // air_launch.hpp -- host entry points of the air kernels.
 #pragma once
 
-#include <cuda.h>
-
 #include "common.cuh"
 
 namespace tpt {
@@ -14,10 +12,6 @@ struct TileRef {
     uint32_t inst;
     uint16_t tx, ty;
 };
-
-// Tensor maps of one batched instance: the grids the pre-pass stages, both
-// halves of each ping-pong pair.
-enum TensorMapSlot { TM_PV0, TM_PV1, TM_VX0, TM_VX1, TM_VY0, TM_VY1, TM_BA0, TM_BA1, TM_COUNT };
 
 // ---- row sweeps (air_sweep.cu) -------------------------------------------------
 // Lanes of halo on each side of a segment: the tick's stencil reaches six
@@ -46,7 +40,6 @@ struct SweepItem {
 // Everything one tick of the sweep form needs.
 struct SweepLaunch {
     const AirInst *insts;       // two per instance (parity 0 and 1 of the ping-pong pairs)
-    const CUtensorMap *tmaps;   // TM_COUNT per instance
     const TileRef *tiles;       // pre-pass tiles
     uint32_t ntiles;
     const SweepItem *items;

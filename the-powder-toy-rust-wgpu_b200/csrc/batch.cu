@@ -26,7 +26,6 @@
 #include "air_launch.hpp"
 #include "grav_dft.hpp"
 #include "grav_plan.hpp"
-#include "tmap.hpp"
 
 using namespace tpt;
 
@@ -145,7 +144,6 @@ struct tpt_batch {
     int32_t *i32 = nullptr;
     std::vector<AirInst> insts_host;
     AirInst *insts = nullptr;
-    CUtensorMap *tmaps = nullptr;
     air::TileRef *tiles = nullptr;
     uint32_t ntiles = 0;
     // the sweep form of the air tick: work items (device), the queue counter
@@ -177,7 +175,6 @@ struct tpt_batch {
     air::SweepLaunch sweep() const {
         air::SweepLaunch L{};
         L.insts = insts;
-        L.tmaps = tmaps;
         L.tiles = tiles;
         L.ntiles = ntiles;
         L.items = items;
@@ -208,7 +205,6 @@ struct tpt_batch {
         cudaFree(insts);
         cudaFree(stage);
         cudaFree(io);
-        cudaFree(tmaps);
         cudaFree(tiles);
         cudaFree(items);
         cudaFree(ctl);
@@ -371,7 +367,6 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     }
     int rc = require_sm100();
     if (rc) return rc;
-    if (!tensor_map_encoder()) TPT_FAIL(TPT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available");
     tpt_batch *b = new (std::nothrow) tpt_batch();
     if (!b) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "host allocation failed");
     auto bail = [&](int code) {
@@ -399,7 +394,6 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     if (e == cudaSuccess) e = cudaMemset(b->f32, 0, total * F_N32 * sizeof(float));
     if (e == cudaSuccess) e = cudaMemset(b->u32, 0, total * U_NU32 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(b->i32, 0, total * sizeof(int32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&b->tmaps, (size_t)n * air::TM_COUNT * sizeof(CUtensorMap));
     if (e != cudaSuccess) {
         set_error("batch arena allocation (%zu cells) failed: %s", total, cudaGetErrorString(e));
         return bail(e == cudaErrorMemoryAllocation ? TPT_ERR_OUT_OF_MEMORY : TPT_ERR_CUDA);
@@ -407,7 +401,6 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     // two AirInst per instance: parity 0 reads canonical hv/masks and writes
     // the second copies; parity 1 the reverse.
     std::vector<air::TileRef> tiles;
-    std::vector<CUtensorMap> tm((size_t)n * air::TM_COUNT);
     b->insts_host.resize(2 * (size_t)n);
     std::vector<JobShape> gshapes;
     std::vector<uint32_t> gidx;
@@ -445,24 +438,6 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
             J.bairh_out = b->u(par ? U_BH : U_BH2, i);
             b->insts_host[2 * (size_t)i + par] = J;
         }
-        // tensor maps of the grids the velocity pre-pass stages (box = tile + halo)
-        CUtensorMap *m = &tm[(size_t)i * air::TM_COUNT];
-        const uint32_t X = p.xcells, Y = p.ycells, P = b->pitch[i];
-        const uint32_t BW = AIR_TX + 8, BH = AIR_TY + 6;
-        struct Slot {
-            int slot;
-            const void *base;
-            bool f;
-        } slots[] = {
-            {air::TM_PV0, b->f(F_PV, i), true},  {air::TM_PV1, b->f(F_PV2, i), true},
-            {air::TM_VX0, b->f(F_VX, i), true},  {air::TM_VX1, b->f(F_VX2, i), true},
-            {air::TM_VY0, b->f(F_VY, i), true},  {air::TM_VY1, b->f(F_VY2, i), true},
-            {air::TM_BA0, b->u(U_BA, i), false}, {air::TM_BA1, b->u(U_BA2, i), false},
-        };
-        for (const Slot &s : slots) {
-            rc = make_grid_tmap(&m[s.slot], s.base, s.f, X, Y, P, BW, BH);
-            if (rc) return bail(rc);
-        }
         for (uint32_t ty = 0; ty * AIR_TY < p.ycells; ++ty)
             for (uint32_t tx = 0; tx * AIR_TX < p.xcells; ++tx) tiles.push_back({i, (uint16_t)tx, (uint16_t)ty});
         if (descs[i].newton_grav) {
@@ -477,7 +452,6 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
         e = cudaMemcpy(b->insts, b->insts_host.data(), b->insts_host.size() * sizeof(AirInst), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(b->tiles, tiles.data(), tiles.size() * sizeof(air::TileRef), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(b->tmaps, tm.data(), tm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&b->ctl, (1 + 2 * (size_t)n) * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(b->ctl, 0, (1 + 2 * (size_t)n) * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);

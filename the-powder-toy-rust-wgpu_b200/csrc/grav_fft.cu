@@ -6,6 +6,7 @@
 #include <vector>
 
 #include "grav_fft.cuh"
+#include "grav_fft_warp.cuh"
 #include "grav_plan.hpp"
 
 namespace tpt {
@@ -85,6 +86,173 @@ __global__ void __launch_bounds__(NT) rows_inverse(const Job *__restrict__ jobs,
     }
 }
 
+// ---- the warp form: one warp per 1-D transform ---------------------------------
+constexpr int WARPS = NT / 32;
+
+// Forward transform of mass row y (real, zero beyond X and where the mask is
+// clear), stored in the warp FFT's permuted order.
+template <int M> __device__ __forceinline__ void row_fwd_warp(const Job &J, uint32_t y, int lane) {
+    float2 v[M];
+#pragma unroll
+    for (int j1 = 0; j1 < M; ++j1) {
+        const uint32_t x = 32u * j1 + lane;
+        float m = 0.0f;
+        if (x < J.X) {
+            const size_t c = (size_t)y * J.pitch + x;
+            if (__ldg(J.mask + c) != 0u) m = J.mass_f ? __ldg(J.mass_f + c) : (float)__ldg(J.mass_i + c) * J.mass_scale_inv;
+        }
+        v[j1] = make_float2(m, 0.0f);
+    }
+    WarpFft<M>::forward(v, J.tw1, lane);
+    float2 *dst = J.work + (size_t)y * J.n1;
+#pragma unroll
+    for (int k = 0; k < M; ++k) dst[32 * k + lane] = v[k];
+}
+
+__global__ void __launch_bounds__(NT) rows_forward_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
+                                                     uint32_t nrefs, const JobIO io) {
+    const uint32_t w = blockIdx.x * WARPS + threadIdx.x / 32;
+    if (w >= nrefs) return;
+    const int lane = threadIdx.x & 31;
+    const BlockRef r = refs[w];
+    const Job J = load_job(jobs, r.job, io);
+    switch (J.n1 >> 5) {
+        case 1: row_fwd_warp<1>(J, r.item, lane); break;
+        case 2: row_fwd_warp<2>(J, r.item, lane); break;
+        case 4: row_fwd_warp<4>(J, r.item, lane); break;
+        case 8: row_fwd_warp<8>(J, r.item, lane); break;
+        case 16: row_fwd_warp<16>(J, r.item, lane); break;
+        case 32: row_fwd_warp<32>(J, r.item, lane); break;
+        default: break;
+    }
+}
+
+// One column (storage column c of the row spectra): forward transform down
+// the column, product with each field's kernel spectrum, inverse transform;
+// the Y rows both fields need are left in tx / ty (shared memory). tx holds
+// the column's input before; fs (n2 entries, the same memory as ty) holds the
+// forward spectrum while the two products are taken, in the lane order the
+// registers use, so each lane reads back only what it wrote and the y field's
+// rows overwrite only entries their own lane has read.
+template <int M>
+__device__ __forceinline__ void col_warp(const Job &J, uint32_t c, float2 *tx, float2 *fs, int lane) {
+    float2 g[M];
+#pragma unroll
+    for (int j1 = 0; j1 < M; ++j1) {
+        const uint32_t j = 32u * j1 + lane;
+        g[j1] = j < J.Y ? tx[j] : make_float2(0.0f, 0.0f);
+    }
+    WarpFft<M>::forward(g, J.tw2, lane);
+#pragma unroll
+    for (int k = 0; k < M; ++k) fs[32 * k + lane] = g[k];
+    const float2 *kx = J.kx + (size_t)c * J.n2, *ky = J.ky + (size_t)c * J.n2;
+#pragma unroll
+    for (int k = 0; k < M; ++k) g[k] = cmulf(g[k], __ldg(kx + 32 * k + lane));
+    WarpFft<M>::inverse(g, J.tw2, lane);
+#pragma unroll
+    for (int j1 = 0; j1 < M; ++j1) {
+        const uint32_t j = 32u * j1 + lane;
+        if (j < J.Y) tx[j] = g[j1];
+    }
+#pragma unroll
+    for (int k = 0; k < M; ++k) g[k] = cmulf(fs[32 * k + lane], __ldg(ky + 32 * k + lane));
+    WarpFft<M>::inverse(g, J.tw2, lane);
+#pragma unroll
+    for (int j1 = 0; j1 < M; ++j1) {
+        const uint32_t j = 32u * j1 + lane;
+        if (j < J.Y) fs[j] = g[j1];
+    }
+}
+
+// A block takes WARPS consecutive storage columns of one job: the Y x WARPS
+// tile is staged through shared memory (row runs of WARPS columns are
+// contiguous), each warp transforms one column, and both fields' Y x WARPS
+// tiles go back the same way. Per warp: `ystride` entries of the x field
+// tile, `fstride` (>= n2) of the spectrum stash / y field tile.
+__global__ void __launch_bounds__(NT) cols_convolve_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
+                                                      uint32_t ystride, uint32_t fstride) {
+    extern __shared__ float2 sm2[];
+    const BlockRef r = refs[blockIdx.x];
+    const Job J = jobs[r.job];
+    const uint32_t c0 = r.item, n1 = J.n1, Y = J.Y;
+    float2 *TX = sm2, *TY = sm2 + (size_t)WARPS * ystride;
+    for (uint32_t i = threadIdx.x; i < Y * WARPS; i += NT) {
+        const uint32_t j = i / WARPS, col = i - j * WARPS;
+        TX[(size_t)col * ystride + j] = J.work[(size_t)j * n1 + c0 + col];
+    }
+    __syncthreads();
+    const int wi = threadIdx.x / 32, lane = threadIdx.x & 31;
+    float2 *tx = TX + (size_t)wi * ystride, *ty = TY + (size_t)wi * fstride;
+    switch (J.n2 >> 5) {
+        case 1: col_warp<1>(J, c0 + wi, tx, ty, lane); break;
+        case 2: col_warp<2>(J, c0 + wi, tx, ty, lane); break;
+        case 4: col_warp<4>(J, c0 + wi, tx, ty, lane); break;
+        case 8: col_warp<8>(J, c0 + wi, tx, ty, lane); break;
+        case 16: col_warp<16>(J, c0 + wi, tx, ty, lane); break;
+        case 32: col_warp<32>(J, c0 + wi, tx, ty, lane); break;
+        default: break;
+    }
+    __syncthreads();
+    float2 *sx = J.spec, *sy = J.spec + (size_t)Y * n1;
+    for (uint32_t i = threadIdx.x; i < Y * WARPS; i += NT) {
+        const uint32_t j = i / WARPS, col = i - j * WARPS;
+        const size_t g = (size_t)j * n1 + c0 + col;
+        sx[g] = TX[(size_t)col * ystride + j];
+        sy[g] = TY[(size_t)col * fstride + j];
+    }
+}
+
+// Inverse transform of spectrum row y of one field; real part of the first X
+// outputs, masked.
+template <int M> __device__ __forceinline__ void row_inv_warp(const Job &J, uint32_t field, uint32_t y, int lane) {
+    const float2 *src = J.spec + ((size_t)field * J.Y + y) * J.n1;
+    float2 v[M];
+#pragma unroll
+    for (int k = 0; k < M; ++k) v[k] = src[32 * k + lane];
+    WarpFft<M>::inverse(v, J.tw1, lane);
+    float *out = field ? J.gy : J.gx;
+#pragma unroll
+    for (int j1 = 0; j1 < M; ++j1) {
+        const uint32_t x = 32u * j1 + lane;
+        if (x < J.X) {
+            const size_t c = (size_t)y * J.pitch + x;
+            out[c] = __ldg(J.mask + c) != 0u ? v[j1].x : 0.0f;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(NT) rows_inverse_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
+                                                     uint32_t nrefs, const JobIO io) {
+    const uint32_t w = blockIdx.x * WARPS + threadIdx.x / 32;
+    if (w >= nrefs) return;
+    const int lane = threadIdx.x & 31;
+    const BlockRef r = refs[w];
+    const Job J = load_job(jobs, r.job, io);
+    const uint32_t field = r.item / J.Y, y = r.item - field * J.Y;
+    switch (J.n1 >> 5) {
+        case 1: row_inv_warp<1>(J, field, y, lane); break;
+        case 2: row_inv_warp<2>(J, field, y, lane); break;
+        case 4: row_inv_warp<4>(J, field, y, lane); break;
+        case 8: row_inv_warp<8>(J, field, y, lane); break;
+        case 16: row_inv_warp<16>(J, field, y, lane); break;
+        case 32: row_inv_warp<32>(J, field, y, lane); break;
+        default: break;
+    }
+}
+
+// Kernel spectra from the natural order (row ky, column kx) into the warp
+// form's layout: storage column c (frequency kx of permuted position c along
+// x), then permuted position p along y.
+__global__ void permute_spectrum(const float2 *__restrict__ nat, float2 *__restrict__ out, uint32_t n1, uint32_t n2) {
+    const size_t id = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (size_t)n1 * n2) return;
+    const uint32_t c = (uint32_t)(id / n2), p = (uint32_t)(id - (size_t)c * n2);
+    const uint32_t m1 = n1 / 32, m2 = n2 / 32;
+    const uint32_t kx = (c / 32) + m1 * (uint32_t)brev_c((int)(c % 32), 5);
+    const uint32_t ky = (p / 32) + m2 * (uint32_t)brev_c((int)(p % 32), 5);
+    out[id] = nat[(size_t)ky * n1 + kx];
+}
+
 // ---- kernel spectra, FP64 (once per plan) ---------------------------------
 // build_kernel_field_kernel (crates/tpt-sim/src/gravity_gpu/fft.rs:208-237)
 // in double: K(d) = scale * d / |d|^3 with d folded into (-N/2, N/2].
@@ -133,9 +301,10 @@ __global__ void spectrum_cols_f64(const double2 *buf, uint32_t n1, uint32_t n2, 
     }
 }
 
-// Twiddle table exp(-2 pi i k / n), k < n/2, evaluated in double.
-template <typename T2> static std::vector<T2> twiddles(uint32_t n) {
-    std::vector<T2> t(std::max<uint32_t>(n / 2, 1));
+// Twiddle table exp(-2 pi i k / n), k < n/2 (or k < n: `full`), evaluated in
+// double.
+template <typename T2> static std::vector<T2> twiddles(uint32_t n, bool full = false) {
+    std::vector<T2> t(std::max<uint32_t>(full ? n : n / 2, 1));
     for (uint32_t k = 0; k < t.size(); ++k) {
         double a = -2.0 * M_PI * (double)k / (double)n;
         t[k].x = cos(a);
@@ -170,6 +339,7 @@ int init_kernel_attrs() {
     TPT_CUDA(cudaFuncSetAttribute(rows_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024));
     TPT_CUDA(cudaFuncSetAttribute(spectrum_rows_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
     TPT_CUDA(cudaFuncSetAttribute(spectrum_cols_f64, cudaFuncAttributeMaxDynamicSharedMemorySize, 128 * 1024));
+    TPT_CUDA(cudaFuncSetAttribute(cols_convolve_w, cudaFuncAttributeMaxDynamicSharedMemorySize, WARPS * (512 + 1024) * 8));
     done = true;
     return TPT_OK;
 }
@@ -206,6 +376,29 @@ int build_spectra(uint32_t n1, uint32_t n2, double scale, float2 *kx, float2 *ky
     return TPT_OK;
 }
 
+// The same spectra in the warp form's layout (permute_spectrum).
+int build_spectra_permuted(uint32_t n1, uint32_t n2, double scale, float2 *kx, float2 *ky) {
+    const size_t cells = (size_t)n1 * n2;
+    float2 *nat = nullptr;
+    TPT_CUDA(cudaMalloc(&nat, 2 * cells * sizeof(float2)));
+    int rc = build_spectra(n1, n2, scale, nat, nat + cells, nullptr);
+    if (rc == TPT_OK) {
+        const unsigned blocks = (unsigned)((cells + 255) / 256);
+        permute_spectrum<<<blocks, 256>>>(nat, kx, n1, n2);
+        count_launch();
+        permute_spectrum<<<blocks, 256>>>(nat + cells, ky, n1, n2);
+        count_launch();
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            set_error("gravity spectrum permutation failed: %s", cudaGetErrorString(e));
+            rc = TPT_ERR_CUDA;
+        }
+    }
+    cudaFree(nat);
+    return rc;
+}
+
 // ---- FFT gravity set (one plan or a batch) --------------------------------
 int FftSet::create(const std::vector<JobShape> &shapes) {
     int rc = init_kernel_attrs();
@@ -213,6 +406,13 @@ int FftSet::create(const std::vector<JobShape> &shapes) {
     destroy();
     const size_t nj = shapes.size();
     jobs_host.resize(nj);
+    warp = true;
+    for (const JobShape &sh : shapes)
+        if (next_pow2(2 * sh.X) > 1024u || next_pow2(2 * sh.Y) > 1024u) warp = false;
+    // padded lengths: next_pow2(2X) as the reference pads (gravity_gpu/mod.rs:
+    // 140-167), at least 32 in the warp form (any length >= 2X gives the same
+    // linear convolution)
+    auto pad = [&](uint32_t v) { return warp ? std::max<uint32_t>(32u, next_pow2(2 * v)) : next_pow2(2 * v); };
     std::vector<BlockRef> rr, cr, ir;
     size_t work_elems = 0, spec_elems = 0, kern_elems = 0;
     std::vector<size_t> woff(nj), soff(nj), koff(nj);
@@ -220,7 +420,7 @@ int FftSet::create(const std::vector<JobShape> &shapes) {
     std::vector<size_t> size_off;
     for (size_t j = 0; j < nj; ++j) {
         const JobShape &s = shapes[j];
-        uint32_t n1 = next_pow2(2 * s.X), n2 = next_pow2(2 * s.Y);
+        uint32_t n1 = pad(s.X), n2 = pad(s.Y);
         woff[j] = work_elems;
         work_elems += (size_t)s.Y * n1;
         soff[j] = spec_elems;
@@ -241,8 +441,8 @@ int FftSet::create(const std::vector<JobShape> &shapes) {
     // one twiddle table per distinct length
     std::vector<uint32_t> lens;
     for (auto &s : shapes) {
-        lens.push_back(next_pow2(2 * s.X));
-        lens.push_back(next_pow2(2 * s.Y));
+        lens.push_back(pad(s.X));
+        lens.push_back(pad(s.Y));
     }
     std::sort(lens.begin(), lens.end());
     lens.erase(std::unique(lens.begin(), lens.end()), lens.end());
@@ -250,7 +450,7 @@ int FftSet::create(const std::vector<JobShape> &shapes) {
     std::vector<size_t> twoff(lens.size());
     for (size_t i = 0; i < lens.size(); ++i) {
         twoff[i] = tw_elems;
-        tw_elems += std::max<uint32_t>(lens[i] / 2, 1);
+        tw_elems += std::max<uint32_t>(warp ? lens[i] : lens[i] / 2, 1);
     }
     TPT_CUDA(cudaMalloc(&work, std::max<size_t>(work_elems, 1) * sizeof(float2)));
     TPT_CUDA(cudaMalloc(&spec, std::max<size_t>(spec_elems, 1) * sizeof(float2)));
@@ -258,7 +458,7 @@ int FftSet::create(const std::vector<JobShape> &shapes) {
     TPT_CUDA(cudaMalloc(&tw, std::max<size_t>(tw_elems, 1) * sizeof(float2)));
     std::vector<float2> twh(tw_elems);
     for (size_t i = 0; i < lens.size(); ++i) {
-        auto t = twiddles<float2>(lens[i]);
+        auto t = twiddles<float2>(lens[i], warp);
         std::copy(t.begin(), t.end(), twh.begin() + twoff[i]);
     }
     TPT_CUDA(cudaMemcpy(tw, twh.data(), tw_elems * sizeof(float2), cudaMemcpyHostToDevice));
@@ -277,8 +477,8 @@ int FftSet::create(const std::vector<JobShape> &shapes) {
         J.X = s.X;
         J.pitch = s.X;
         J.Y = s.Y;
-        J.n1 = next_pow2(2 * s.X);
-        J.n2 = next_pow2(2 * s.Y);
+        J.n1 = pad(s.X);
+        J.n2 = pad(s.Y);
         J.l1 = log2u(J.n1);
         J.l2 = log2u(J.n2);
         J.mass_scale_inv = 1.0f / 65536.0f;
@@ -292,7 +492,8 @@ int FftSet::create(const std::vector<JobShape> &shapes) {
         if (it == built.end()) {
             float2 *kx = kern + koff[j], *ky = kx + plane;
             double scale = -(double)6.673e-1f / ((double)J.n1 * (double)J.n2);
-            int brc = build_spectra(J.n1, J.n2, scale, kx, ky, nullptr);
+            int brc = warp ? build_spectra_permuted(J.n1, J.n2, scale, kx, ky)
+                           : build_spectra(J.n1, J.n2, scale, kx, ky, nullptr);
             if (brc) return brc;
             built.push_back(key);
             built_off.push_back(koff[j]);
@@ -310,9 +511,13 @@ int FftSet::create(const std::vector<JobShape> &shapes) {
         for (uint32_t i = 0; i < 2 * s.Y; ++i) ir.push_back({(uint32_t)j, i});
     }
     // the column kernel needs one cb for the whole launch: use the smallest
-    // needed by any job (power-of-two, divides every n1)
+    // needed by any job (power-of-two, divides every n1); the warp form
+    // takes WARPS columns per block
     cb_launch = 16;
     for (auto &J : jobs_host) cb_launch = std::min(cb_launch, std::min<int>(col_block(J.n2), (int)J.n1));
+    if (warp) cb_launch = WARPS;
+    max_y = 0;
+    for (auto &J : jobs_host) max_y = std::max(max_y, J.Y);
     cr.clear();
     for (size_t j = 0; j < nj; ++j)
         for (uint32_t c = 0; c < jobs_host[j].n1; c += cb_launch) cr.push_back({(uint32_t)j, c});
@@ -351,6 +556,16 @@ int FftSet::launch(cudaStream_t st, const JobIO *io) const {
     if (n_rows == 0) return TPT_OK;
     JobIO none{};
     const JobIO &a = io ? *io : none;
+    if (warp) {
+        rows_forward_w<<<(n_rows + WARPS - 1) / WARPS, NT, 0, st>>>(jobs, refs, n_rows, a);
+        TPT_LAUNCHED();
+        cols_convolve_w<<<n_cols, NT, (size_t)WARPS * (max_y + max_n2) * sizeof(float2), st>>>(jobs, refs + n_rows,
+                                                                                               max_y, max_n2);
+        TPT_LAUNCHED();
+        rows_inverse_w<<<(n_inv + WARPS - 1) / WARPS, NT, 0, st>>>(jobs, refs + n_rows + n_cols, n_inv, a);
+        TPT_LAUNCHED();
+        return TPT_OK;
+    }
     rows_forward<<<n_rows, NT, max_n1 * sizeof(float2), st>>>(jobs, refs, a);
     TPT_LAUNCHED();
     cols_convolve<<<n_cols, NT, (size_t)cb_launch * 2 * max_n2 * sizeof(float2), st>>>(jobs, refs + n_rows,
@@ -373,7 +588,8 @@ void FftSet::destroy() {
     refs = nullptr;
     jobs_host.clear();
     n_rows = n_cols = n_inv = 0;
-    max_n1 = max_n2 = 0;
+    max_n1 = max_n2 = max_y = 0;
+    warp = false;
 }
 
 }  // namespace gfft

@@ -14,10 +14,16 @@
 //      column DFT, keeping only the Y output rows both fields need
 //   I  inverse rows: 2*Y rows -> real part of X outputs, masked
 //
-// Transforms: forward is decimation-in-time fed in bit-reversed order,
-// inverse is decimation-in-frequency read out in bit-reversed order, so no
-// separate permutation pass exists. Twiddles come from a per-length table
-// computed in double on the host and rounded once.
+// Two forms of the transforms. The warp form (grav_fft_warp.cuh), for
+// padded lengths 32 .. 1024 (lengths below 32 are padded up to 32): every
+// 1-D transform is one warp's registers, the four-step factorisation with
+// shuffles across lanes, no block barriers; the spectra stay in the warp
+// FFT's permuted order between the passes, and the kernel spectra are stored
+// in that order (column-major, so a warp's loads are coalesced). The shared-
+// memory form, for longer lengths: forward is decimation-in-time fed in
+// bit-reversed order, inverse is decimation-in-frequency read out in
+// bit-reversed order, so no separate permutation pass exists. Twiddles come
+// from a per-length table computed in double on the host and rounded once.
 #pragma once
 
 #include "common.cuh"
@@ -107,8 +113,8 @@ struct Job {
     const uint32_t *mask;
     float2 *work;                 // Y x n1 forward row spectra
     float2 *spec;                 // 2 x Y x n1 (x field, then y field)
-    const float2 *kx, *ky;        // n2 x n1 kernel spectra
-    const float2 *tw1, *tw2;      // twiddles of length n1, n2
+    const float2 *kx, *ky;        // n2 x n1 kernel spectra (warp form: permuted, column-major)
+    const float2 *tw1, *tw2;      // twiddles of length n1, n2 (n/2 entries; full circle in the warp form)
     float *gx, *gy;
 };
 

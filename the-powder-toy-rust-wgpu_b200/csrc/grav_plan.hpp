@@ -23,8 +23,9 @@ struct FftSet {
     Job *jobs = nullptr;
     BlockRef *refs = nullptr;
     float2 *work = nullptr, *spec = nullptr, *kern = nullptr, *tw = nullptr;
-    uint32_t n_rows = 0, n_cols = 0, n_inv = 0, max_n1 = 0, max_n2 = 0;
+    uint32_t n_rows = 0, n_cols = 0, n_inv = 0, max_n1 = 0, max_n2 = 0, max_y = 0;
     int cb_launch = 1, max_cb = 1;
+    bool warp = false;  // every job's padded lengths lie in 32 .. 1024: the warp-register form
 
     int create(const std::vector<JobShape> &shapes);
     // Points job j at its inputs/outputs; returns 1 if anything changed
