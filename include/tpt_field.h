@@ -342,18 +342,31 @@ int tpt_batch_write_field(tpt_batch *batch, int field, const void *host,
 int tpt_batch_read_field(tpt_batch *batch, int field, void *host,
                          size_t bytes, tpt_stream_t stream);
 
+/* Forms of the batch's air tick (tpt_batch_tuning.air_form). */
+enum {
+    /* Two launches per tick over 32x8-cell tiles, halos staged by TMA: pass A
+     * (pressure, velocity) writes opv/ovx/ovy, pass B (smoothing, advection,
+     * vorticity, fans, heat, convection, masks) reads them. */
+    TPT_AIR_FORM_TILES = 0,
+    /* One fused launch per tick: CTAs sweep down column strips with every
+     * stage pipelined over the rows (no intermediate grid in memory), plus a
+     * velocity pre-pass that only works for instances whose air moves far. */
+    TPT_AIR_FORM_SWEEP = 1
+};
+
 /* Tuning knobs the autotuner picks (and a caller may pin). Results are the
  * same for every value: they change how the work is laid out, not what is
  * computed. */
 typedef struct tpt_batch_tuning {
-    /* The air tick's work unit: a CTA of tile_x lanes (a multiple of 32 in
+    /* The sweep form's work unit: a CTA of tile_x lanes (a multiple of 32 in
      * 64..256) sweeps down strips of about tile_y rows (8..2048). Each lane
      * owns a column; a strip is at most tile_x - 12 columns wide (six halo
      * columns on each side), and strips of narrow instances are packed side
-     * by side into one CTA. */
+     * by side into one CTA. The tile form's tiles are 32x8 cells. */
     uint32_t tile_x, tile_y;
     uint32_t temporal_depth;  /* ticks per air launch (1 = no blocking)   */
-    /* Resident sweep CTAs per SM (0 = as many as fit). */
+    /* Resident CTAs per SM of the air form's persistent launches (0 = as
+     * many as fit). */
     uint32_t ctas_per_sm;
     /* Split-BF16 gravity of a batch holding both kinds of y stage (groups of
      * many equal-shape instances take the Toeplitz GEMM, the others the y
@@ -363,6 +376,7 @@ typedef struct tpt_batch_tuning {
      * Must be 0 for other batches; at most half the SMs. Results are the same
      * for every value. */
     uint32_t grav_side_ctas;
+    uint32_t air_form;  /* TPT_AIR_FORM_TILES or TPT_AIR_FORM_SWEEP */
 } tpt_batch_tuning;
 
 /*
@@ -382,8 +396,9 @@ int tpt_batch_fields(tpt_batch *batch, uint32_t instance,
  */
 int tpt_batch_step(tpt_batch *batch, uint32_t ticks, tpt_stream_t stream);
 /* Times candidate tunings on the batch's own data (state is saved and
- * restored) and keeps the fastest: sweep shapes (tile_x x tile_y) with
- * their CTAs per SM, then the gravity branch split. The choice is cached in
+ * restored) and keeps the fastest: the air form with its CTAs per SM (and
+ * for the sweep form its shape, tile_x x tile_y), then the gravity branch
+ * split. The choice is cached in
  * the process per batch composition -- the instances' (xcells, ycells)
  * buckets (powers of two) with their counts, and the gravity precision -- so
  * tuning a batch of the same composition again only applies the cached

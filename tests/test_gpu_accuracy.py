@@ -111,7 +111,8 @@ def test_gravity_error_c5_batch_both_y_forms(cuda, tf, oracle):
     assert worst <= 1e-4
 
 
-def test_c5_every_instance_air_and_gravity(cuda, tf, oracle):
+@pytest.mark.parametrize("form", [0, 1])
+def test_c5_every_instance_air_and_gravity(cuda, tf, oracle, form):
     """The whole C5 batch as benchmarked (64 x 400x225 + 64 heavy-tailed,
     split-BF16 gravity) after 20 ticks: every instance's air bit-exact
     against the oracle, and every instance's gx/gy within 1e-4 (rel-max and
@@ -123,6 +124,9 @@ def test_c5_every_instance_air_and_gravity(cuda, tf, oracle):
     insts = W.config_instances(5)
     assert len(insts) == 128
     b = tf.Batch(insts, tf.PRECISION_SPLIT_BF16)
+    t = b.tuning()
+    t.air_form = form
+    b.set_tuning(t)
     b.step(20)
     cuda.cuda.synchronize()
     assert tf.lib().tpt_check_device_errors() == 0
@@ -133,7 +137,7 @@ def test_c5_every_instance_air_and_gravity(cuda, tf, oracle):
         dx, dy = oracle.grav_solve(inst.xcells, inst.ycells, inst.gmask, mass_fx=inst.mass_fx, dtype=np.float64)
         e = max(*_err(st["gx"], dx), *_err(st["gy"], dy))
         worst = max(worst, (e, i))
-    REPORT["gravity/split_bf16/C5 batch, all 128 instances, worst"] = {
+    REPORT[f"gravity/split_bf16/C5 batch, all 128 instances, worst (air form {form})"] = {
         "rel_err": worst[0], "instance": worst[1],
         "shape": f"{insts[worst[1]].xcells}x{insts[worst[1]].ycells}"}
     _dump()

@@ -38,10 +38,20 @@ def check_against_oracle(tf, oracle, batch, insts, ticks, ctx):
             assert not got["gx"].any() and not got["gy"].any()
 
 
+def set_form(tf, b, form, **kw):
+    t = b.tuning()
+    t.air_form = form
+    for k, v in kw.items():
+        setattr(t, k, v)
+    b.set_tuning(t)
+
+
+@pytest.mark.parametrize("form", [0, 1])
 @pytest.mark.parametrize("ticks", [1, 7, 50, 57])
-def test_batch_matches_single_grid_oracle(cuda, tf, oracle, ticks):
+def test_batch_matches_single_grid_oracle(cuda, tf, oracle, ticks, form):
     insts = mixed_instances()
     b = tf.Batch(insts)
+    set_form(tf, b, form)
     b.step(ticks)
     cuda.cuda.synchronize()
     check_against_oracle(tf, oracle, b, insts, ticks, f"{ticks} ticks")
@@ -64,8 +74,11 @@ def test_tune_keeps_state_and_results(cuda, tf, oracle):
     b = tf.Batch(insts)
     b.tune()
     t = b.tuning()
-    assert t.tile_x in (128, 160, 192, 224, 256) and t.tile_y in (32, 64, 128) and t.temporal_depth == 1
-    assert t.ctas_per_sm >= 1
+    assert t.air_form in (tf.AIR_FORM_TILES, tf.AIR_FORM_SWEEP) and t.temporal_depth == 1
+    if t.air_form == tf.AIR_FORM_TILES:
+        assert t.ctas_per_sm in (2, 3, 4, 6, 8)
+    else:
+        assert (t.tile_x, t.tile_y) in ((224, 64), (256, 64), (256, 32))
     b.step(5)
     cuda.cuda.synchronize()
     check_against_oracle(tf, oracle, b, insts, 5, "tuned")
@@ -85,9 +98,7 @@ def test_every_sweep_shape_gives_the_same_fields(cuda, tf, oracle, tile_x, tile_
     whole-grid strips) the fields after 9 ticks are bit-exact."""
     insts = mixed_instances()
     b = tf.Batch(insts)
-    t = b.tuning()
-    t.tile_x, t.tile_y, t.ctas_per_sm = tile_x, tile_y, per_sm
-    b.set_tuning(t)
+    set_form(tf, b, tf.AIR_FORM_SWEEP, tile_x=tile_x, tile_y=tile_y, ctas_per_sm=per_sm)
     b.step(9)
     cuda.cuda.synchronize()
     assert tf.lib().tpt_check_device_errors() == 0
@@ -95,10 +106,35 @@ def test_every_sweep_shape_gives_the_same_fields(cuda, tf, oracle, tile_x, tile_
     b.close()
 
 
+@pytest.mark.parametrize("per_sm", [1, 3, 6, 8])
+def test_tile_form_at_every_grid_size(cuda, tf, oracle, per_sm):
+    insts = mixed_instances()
+    b = tf.Batch(insts)
+    set_form(tf, b, tf.AIR_FORM_TILES, ctas_per_sm=per_sm)
+    b.step(9)
+    cuda.cuda.synchronize()
+    assert tf.lib().tpt_check_device_errors() == 0
+    check_against_oracle(tf, oracle, b, insts, 9, f"tiles {per_sm}/SM")
+    b.close()
+
+
+def test_switching_forms_between_steps(cuda, tf, oracle):
+    """The state sits in the canonical buffers between steps whatever the
+    form, so a batch may change form from one step to the next."""
+    insts = mixed_instances()
+    b = tf.Batch(insts)
+    for form, ticks in ((1, 3), (0, 4), (1, 1), (0, 2)):
+        set_form(tf, b, form)
+        b.step(ticks)
+    cuda.cuda.synchronize()
+    check_against_oracle(tf, oracle, b, insts, 10, "form switches")
+    b.close()
+
+
 def test_bad_tunings_are_rejected(cuda, tf):
     b = tf.Batch(mixed_instances()[:2])
     for kw in (dict(tile_x=100), dict(tile_x=32), dict(tile_x=288), dict(tile_y=4), dict(temporal_depth=2),
-               dict(ctas_per_sm=64)):
+               dict(ctas_per_sm=64), dict(air_form=2), dict(air_form=1, ctas_per_sm=9)):
         t = b.tuning()
         for k, v in kw.items():
             setattr(t, k, v)
@@ -121,6 +157,7 @@ def test_packed_narrow_instances_and_modes(cuda, tf, oracle):
         insts.append(W.make_stress_instance(X, Y, 500 + k, config=cfg))
     insts.append(W.make_stress_instance(300, 20, 599))
     b = tf.Batch(insts)
+    set_form(tf, b, tf.AIR_FORM_SWEEP)
     for ticks in (1, 3):
         b.step(ticks)
     cuda.cuda.synchronize()
@@ -135,12 +172,14 @@ def test_nonfinite_inputs_in_a_batch(cuda, tf, oracle):
     from test_oracle_air_numpy import nonfinite_instance
 
     insts = [nonfinite_instance(), nonfinite_instance(70, 50, 32)]
-    b = tf.Batch(insts)
-    b.step(3)
-    cuda.cuda.synchronize()
-    for i, inst in enumerate(insts):
-        assert_bit_exact(b.state(i), oracle.air_steps(inst, 3), f"non-finite {i}", nan_equal=True)
-    b.close()
+    for form in (tf.AIR_FORM_TILES, tf.AIR_FORM_SWEEP):
+        b = tf.Batch(insts)
+        set_form(tf, b, form)
+        b.step(3)
+        cuda.cuda.synchronize()
+        for i, inst in enumerate(insts):
+            assert_bit_exact(b.state(i), oracle.air_steps(inst, 3), f"form {form} non-finite {i}", nan_equal=True)
+        b.close()
 
 
 def test_batch_measured_config_subset(cuda, tf, oracle):
@@ -154,7 +193,8 @@ def test_batch_measured_config_subset(cuda, tf, oracle):
     b.close()
 
 
-def test_c4_every_instance_20_ticks(cuda, tf, oracle):
+@pytest.mark.parametrize("form", [0, 1])
+def test_c4_every_instance_20_ticks(cuda, tf, oracle, form):
     """The whole C4 batch (256 instances, W, H log-uniform 32..512, FP32
     gravity) after 20 ticks: every instance's air bit-exact against the
     oracle and its gx/gy within 1e-5 of max|g| against FP64."""
@@ -163,6 +203,7 @@ def test_c4_every_instance_20_ticks(cuda, tf, oracle):
     insts = W.config_instances(4)
     assert len(insts) == 256
     b = tf.Batch(insts)
+    set_form(tf, b, form)
     b.step(20)
     cuda.cuda.synchronize()
     assert tf.lib().tpt_check_device_errors() == 0

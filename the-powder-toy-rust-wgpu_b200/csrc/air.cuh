@@ -22,10 +22,11 @@
 // The one global dependency of a tick is between A and B: the far-advection
 // sample can reach any cell of ovx/ovy (0.7*|v| <= 179 cells).
 //
-// The tile code is written over a shared-memory layout policy `L`: the
-// single-grid kernels and the batch's velocity pre-pass stage each array with
-// its own halo (Reg<H>). The batch's own tick is the row sweep of
-// air_sweep.cu, which reuses the per-cell helpers below.
+// The tile code is written once over a shared-memory layout policy `L`:
+// the single-grid kernels and the sweep form's velocity pre-pass stage each
+// array with its own halo (Reg<H>); the batch's tile form stages every array
+// as one TMA box of the tile plus a 4-cell (x) by 3-cell (y) halo. The
+// batch's sweep form (air_sweep.cu) reuses the per-cell helpers below.
 #pragma once
 
 #include "common.cuh"
@@ -43,6 +44,16 @@ template <int H> struct Reg {
     static constexpr int N = W * HGT;
     __device__ static __forceinline__ int at(int gx, int gy, int x0, int y0) {
         return (gy - y0 + H) * W + (gx - x0 + H);
+    }
+};
+
+// The TMA box of the batched kernels: x halo 4 (keeps the box start 16-byte
+// aligned), y halo 3.
+struct Box {
+    static constexpr int HX = 4, HY = 3, W = TX + 2 * HX, HGT = TY + 2 * HY, N = W * HGT;
+    static constexpr int NP = (N + 31) / 32 * 32;  // array stride: TMA destinations are 128-byte aligned
+    __device__ static __forceinline__ int at(int gx, int gy, int x0, int y0) {
+        return (gy - y0 + HY) * W + (gx - x0 + HX);
     }
 };
 
@@ -90,6 +101,22 @@ struct LayoutA1 {  // single grid: per-array halos, masks as flags
     __device__ __forceinline__ float &OPV(int x, int y, int x0, int y0) { return opv[Reg<1>::at(x, y, x0, y0)]; }
 };
 
+struct __align__(128) BoxA {  // batched: one TMA box per array
+    float pv[Box::NP];
+    float vx[Box::NP];
+    float vy[Box::NP];
+    uint32_t b[Box::NP];
+};
+struct LayoutA2 {
+    BoxA *in;
+    float *opv;  // Box::N
+    __device__ __forceinline__ bool blk(int x, int y, int x0, int y0) const { return in->b[Box::at(x, y, x0, y0)] != 0u; }
+    __device__ __forceinline__ float &VX(int x, int y, int x0, int y0) { return in->vx[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &VY(int x, int y, int x0, int y0) { return in->vy[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float PV(int x, int y, int x0, int y0) const { return in->pv[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &OPV(int x, int y, int x0, int y0) { return opv[Box::at(x, y, x0, y0)]; }
+};
+
 // Pass B working set: staged ovx/ovy/opv/hv, the two masks, and the
 // computed vorticity (+2 ring) and smoothed/advected velocity and pressure
 // (+1 ring).
@@ -118,6 +145,39 @@ struct LayoutB1 {
     __device__ __forceinline__ float &NVX(int x, int y, int x0, int y0) { return nvx[Reg<1>::at(x, y, x0, y0)]; }
     __device__ __forceinline__ float &NVY(int x, int y, int x0, int y0) { return nvy[Reg<1>::at(x, y, x0, y0)]; }
     __device__ __forceinline__ float &NPV(int x, int y, int x0, int y0) { return npv[Reg<1>::at(x, y, x0, y0)]; }
+};
+
+struct __align__(128) BoxB {  // batched: one TMA box per array
+    float ovx[Box::NP];  // ovx (or vx when the pressure/velocity pass is off)
+    float ovy[Box::NP];
+    float opv[Box::NP];
+    float hv[Box::NP];
+    uint32_t b[Box::NP];
+    uint32_t bh[Box::NP];
+};
+struct WorkB2 {
+    float vort[Box::N], nvx[Box::N], nvy[Box::N], npv[Box::N];
+};
+struct LayoutB2 {
+    BoxB *in;
+    WorkB2 *w;
+    // every staged grid covers the whole box
+    __device__ __forceinline__ static bool has3(int x, int y, int x0, int y0) {
+        return x >= x0 - Box::HX && x < x0 + TX + Box::HX && y >= y0 - Box::HY && y < y0 + TY + Box::HY;
+    }
+    __device__ __forceinline__ static bool hasH(int x, int y, int x0, int y0) { return has3(x, y, x0, y0); }
+    __device__ __forceinline__ bool blk(int x, int y, int x0, int y0) const { return in->b[Box::at(x, y, x0, y0)] != 0u; }
+    __device__ __forceinline__ bool hblk(int x, int y, int x0, int y0) const {
+        return (in->bh[Box::at(x, y, x0, y0)] & 0x8u) != 0u;
+    }
+    __device__ __forceinline__ float OVX(int x, int y, int x0, int y0) const { return in->ovx[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float OVY(int x, int y, int x0, int y0) const { return in->ovy[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float OPV(int x, int y, int x0, int y0) const { return in->opv[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float HV(int x, int y, int x0, int y0) const { return in->hv[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &VORT(int x, int y, int x0, int y0) { return w->vort[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &NVX(int x, int y, int x0, int y0) { return w->nvx[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &NVY(int x, int y, int x0, int y0) { return w->nvy[Box::at(x, y, x0, y0)]; }
+    __device__ __forceinline__ float &NPV(int x, int y, int x0, int y0) { return w->npv[Box::at(x, y, x0, y0)]; }
 };
 
 // ---- staging by loads (single-grid path) -------------------------------------
@@ -605,20 +665,25 @@ template <class L> __device__ __forceinline__ void pass_b(const AirInst &I, int 
 }
 
 // ---- settle --------------------------------------------------------------------
-// settle.rs:50-93 for one cell: emap decay and the two masks.
-__device__ __forceinline__ void masks_cell(const AirInst &I, size_t g, uint32_t &bair, uint32_t &bairh) {
-    uint32_t w = __ldg(I.wall + g) & 0xFFu;
-    uint32_t raw = I.emap[g];
+// settle.rs:50-93 for one cell from its loaded words: wall id, emap before the
+// decay, element stamps -> the two masks.
+__device__ __forceinline__ void masks_of(uint32_t wall, uint32_t raw, uint32_t eair, uint32_t eairh, uint32_t &bair,
+                                        uint32_t &bairh) {
+    const uint32_t w = wall & 0xFFu;
     uint32_t e = raw;
-    if (raw != 0u) {
-        e = raw - 1u;
-        I.emap[g] = e;
-    }
+    if (raw != 0u) e = raw - 1u;
     e &= 0xFFu;
     uint32_t blocked = (w == 8u || w == 1u || w == 16u || (w == 2u && e == 0u)) ? 1u : 0u;
-    bair = blocked | (I.eair ? __ldg(I.eair + g) : 0u);
+    bair = blocked | eair;
     uint32_t heat = (blocked != 0u || w == 14u) ? 0x8u : 0u;
-    bairh = heat | (I.eairh ? __ldg(I.eairh + g) : 0u);
+    bairh = heat | eairh;
+}
+
+// The same for cell g of an instance, decaying its emap in place.
+__device__ __forceinline__ void masks_cell(const AirInst &I, size_t g, uint32_t &bair, uint32_t &bairh) {
+    const uint32_t raw = I.emap[g];
+    if (raw != 0u) I.emap[g] = raw - 1u;
+    masks_of(__ldg(I.wall + g), raw, I.eair ? __ldg(I.eair + g) : 0u, I.eairh ? __ldg(I.eairh + g) : 0u, bair, bairh);
 }
 
 }  // namespace air

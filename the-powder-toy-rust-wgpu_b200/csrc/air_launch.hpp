@@ -1,6 +1,8 @@
 // air_launch.hpp -- host entry points of the air kernels.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace tpt {
@@ -13,7 +15,20 @@ struct TileRef {
     uint16_t tx, ty;
 };
 
-// ---- row sweeps (air_sweep.cu) -------------------------------------------------
+// ---- the tile form (air_batch.cu) ---------------------------------------------
+// Tensor maps of one batched instance: the grids the two passes stage, with
+// the two halves of the heat and mask ping-pong.
+enum TensorMapSlot {
+    TM_PV, TM_VX, TM_VY, TM_OVX, TM_OVY, TM_OPV, TM_BA0, TM_BA1, TM_BH0, TM_BH1, TM_HV0, TM_HV1, TM_COUNT
+};
+
+// One tick of every instance in the tile form. `insts` holds two AirInst per
+// instance (parity 0 and 1 of the hv / mask ping-pong; pv/vx/vy are updated in
+// place); `tmaps` TM_COUNT tensor maps per instance.
+int launch_tile_tick(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles,
+                     uint32_t grid, uint32_t parity, bool any_noupdate_heat, cudaStream_t st);
+
+// ---- the sweep form (air_sweep.cu) ----------------------------------------------
 // Lanes of halo on each side of a segment: the tick's stencil reaches six
 // columns (block_air of the effective velocity's wall clear, five more stages
 // of one column each).

@@ -144,6 +144,10 @@ __global__ void __launch_bounds__(SWEEP_MAX_LANES, 2) kb_air_sweep(const AirInst
                                                                uint32_t *__restrict__ ctl, uint32_t *__restrict__ want) {
     extern __shared__ float sm[];
     __shared__ SweepItem s_it;
+    // the item's segments' instance parameters: read from shared memory, which
+    // the kernel's global stores cannot alias, so they are never reloaded from
+    // global memory after a store
+    __shared__ AirInst s_inst[SW_MAXSEG];
     __shared__ uint32_t s_next;
     uint32_t *smu = reinterpret_cast<uint32_t *>(sm);
     const int NL = (int)blockDim.x, P = NL + 2, l = (int)threadIdx.x;
@@ -159,6 +163,15 @@ __global__ void __launch_bounds__(SWEEP_MAX_LANES, 2) kb_air_sweep(const AirInst
             for (int k = l; k < (int)(sizeof(SweepItem) / 4); k += NL) dst[k] = __ldg(src + k);
         }
         __syncthreads();
+        {
+            constexpr int W = (int)(sizeof(AirInst) / 4);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(s_inst);
+            for (int k = l; k < (int)s_it.nseg * W; k += NL) {
+                const int sg = k / W, w = k - sg * W;
+                dst[k] = __ldg(reinterpret_cast<const uint32_t *>(insts + 2 * (size_t)s_it.seg[sg].inst + parity) + w);
+            }
+        }
+        __syncthreads();
 
         // ---- this lane's segment
         Lane L{};
@@ -169,7 +182,7 @@ __global__ void __launch_bounds__(SWEEP_MAX_LANES, 2) kb_air_sweep(const AirInst
         if (seg >= 0) {
             const SweepSeg S = s_it.seg[seg];
             inst = S.inst;
-            L.I = insts + 2 * (size_t)S.inst + parity;
+            L.I = &s_inst[seg];
             L.X = (int)L.I->X;
             L.Y = (int)L.I->Y;
             L.pitch = (int)L.I->pitch;
@@ -183,7 +196,7 @@ __global__ void __launch_bounds__(SWEEP_MAX_LANES, 2) kb_air_sweep(const AirInst
             L.colok = L.c >= 0 && L.c < L.X;
             L.out = (l - (int)S.lane0) >= SW_H && (l - (int)S.lane0) < SW_H + (int)S.nx;
         } else {
-            L.I = insts;  // any valid pointer; every access below is predicated off
+            L.I = &s_inst[0];  // any valid pointer; every access below is predicated off
             L.lo = L.hi = 0;
             L.y0 = 0;
             L.ny = -100;  // no stage row range is ever entered
@@ -203,39 +216,60 @@ __global__ void __launch_bounds__(SWEEP_MAX_LANES, 2) kb_air_sweep(const AirInst
         float opv2 = 0.f, opv3 = 0.f, opv4 = 0.f;
         float ovx3 = 0.f, ovx4 = 0.f, ovx5 = 0.f;
         float vt4 = 0.f, vt5 = 0.f, vt6 = 0.f;
-        float lvx = 0.f, lvy = 0.f;
+        float vx0 = 0.f, vy0 = 0.f;
+
+        // The loads of a step's rows are issued one step ahead (the previous
+        // step's compute hides their latency): row r of block_air and, while
+        // the velocity pass runs, pv/vx/vy (NoUpdate: pv/vx/vy of row r - 5,
+        // which that mode uses directly); row r - 5 of block_airh, walls and
+        // heat.
+        uint32_t n_b = 0u, n_bh = 0u, n_wall = 0u, n_emap = 0u, n_ea = 0u, n_eh = 0u;
+        float n_pv = 0.f, n_vx = 0.f, n_vy = 0.f, n_hv = 0.f;
+        auto issue_loads = [&](int rload) {
+            const int rhl = rload - 5, rv = upd ? rload : rhl;
+            n_b = 0u;
+            n_bh = 0u;
+            n_wall = 0u;
+            n_emap = n_ea = n_eh = 0u;
+            n_pv = n_vx = n_vy = n_hv = 0.f;
+            if (L.colok && rload >= 0 && rload < Y) n_b = __ldg(I.bair + (size_t)rload * L.pitch + c) != 0u ? 1u : 0u;
+            if (L.colok && rv >= 0 && rv < Y) {
+                const size_t g = (size_t)rv * L.pitch + c;
+                n_pv = __ldg(I.pv + g);
+                n_vx = __ldg(I.vx + g);
+                n_vy = __ldg(I.vy + g);
+            }
+            if (L.colok && rhl >= 0 && rhl < Y) {
+                const size_t g = (size_t)rhl * L.pitch + c;
+                n_bh = (__ldg(I.bairh + g) & 0x8u) != 0u ? 1u : 0u;
+                n_wall = __ldg(I.wall + g);
+                if (aheat) n_hv = __ldg(I.hv + g);
+                if (L.out) {  // the mask rebuild's inputs (own cell, output columns)
+                    n_emap = I.emap[g];
+                    n_ea = I.eair ? __ldg(I.eair + g) : 0u;
+                    n_eh = I.eairh ? __ldg(I.eairh + g) : 0u;
+                }
+            }
+        };
+        issue_loads(L.y0 - 6);
 
         const int steps = (int)s_it.steps;
         for (int rr = -6; rr <= steps + 6; ++rr) {
             const int r = L.y0 + rr;  // row loaded at this step
             const int rh = r - 5;     // row of the smoothing stage, the heat loads and the masks
-            // ---- loads
+            // ---- this step's loaded values, then the next step's loads
+            const uint32_t lb = n_b, lbh = n_bh, lwall = n_wall, lemap = n_emap, lea = n_ea, leh = n_eh;
+            const float lhv = n_hv, cpv = n_pv, cvx = n_vx, cvy = n_vy;
+            issue_loads(r + 1);
             pv2 = pv1;
             pv1 = pv0;
-            vx1 = lvx;
-            vy1 = lvy;
-            pv0 = 0.f;
-            lvx = 0.f;
-            lvy = 0.f;
-            uint32_t lb = 0u;
-            if (L.colok && r >= 0 && r < Y) {
-                const size_t g = (size_t)r * L.pitch + c;
-                lb = __ldg(I.bair + g) != 0u ? 1u : 0u;
-                if (upd) {
-                    pv0 = __ldg(I.pv + g);
-                    lvx = __ldg(I.vx + g);
-                    lvy = __ldg(I.vy + g);
-                }
-            }
+            pv0 = cpv;
+            vx1 = vx0;
+            vy1 = vy0;
+            vx0 = cvx;
+            vy0 = cvy;
             const bool hok = L.colok && rh >= 0 && rh < Y;
             const size_t gh = (size_t)(hok ? rh : 0) * L.pitch + (hok ? c : 0);
-            uint32_t lbh = 0u, lwall = 0u;
-            float lhv = 0.f;
-            if (hok) {
-                lbh = (__ldg(I.bairh + gh) & 0x8u) != 0u ? 1u : 0u;
-                lwall = __ldg(I.wall + gh);
-                if (aheat) lhv = __ldg(I.hv + gh);
-            }
             hb = (hb << 1) | lb;
             hh = (hh << 1) | lbh;
             smu[(OFF_HIST + (rr & 1)) * P + l + 1] = (hb & 0xFFFFu) | (hh << 16);
@@ -450,10 +484,10 @@ __global__ void __launch_bounds__(SWEEP_MAX_LANES, 2) kb_air_sweep(const AirInst
                         nvy = 0.0f;
                         npv = 0.0f;
                     }
-                } else {  // NoUpdate (mod.rs:150): the stored velocity and pressure
-                    nvx = hok ? __ldg(I.vx + gh) : 0.0f;
-                    nvy = hok ? __ldg(I.vy + gh) : 0.0f;
-                    npv = hok ? __ldg(I.pv + gh) : 0.0f;
+                } else {  // NoUpdate (mod.rs:150): the stored velocity and pressure of row r - 5
+                    nvx = cvx;
+                    nvy = cvy;
+                    npv = cpv;
                 }
                 ring(sm, OFF_NVX, RG_NV, q5, P)[l] = nvx;
                 ring(sm, OFF_NVY, RG_NV, q5, P)[l] = nvy;
@@ -465,7 +499,8 @@ __global__ void __launch_bounds__(SWEEP_MAX_LANES, 2) kb_air_sweep(const AirInst
                     }
                     // settle.rs:50-93: emap decay and the masks the next tick reads
                     uint32_t ba, bh;
-                    masks_cell(I, gh, ba, bh);
+                    masks_of(lwall, lemap, lea, leh, ba, bh);
+                    if (lemap != 0u) I.emap[gh] = lemap - 1u;
                     I.bair_out[gh] = ba;
                     I.bairh_out[gh] = bh;
                 }

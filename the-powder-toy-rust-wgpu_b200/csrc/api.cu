@@ -12,6 +12,7 @@
 #include "grav_dft.hpp"
 #include "grav_particles.hpp"
 #include "grav_plan.hpp"
+#include "tmap.hpp"
 
 namespace tpt {
 
@@ -36,6 +37,35 @@ int require_sm100() {
     if (major != 10 || minor != 0)
         TPT_FAIL(TPT_ERR_UNSUPPORTED, "device %d is sm_%d%d; this library is built for sm_100a only", dev, major,
                  minor);
+    return TPT_OK;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+int make_grid_tmap(CUtensorMap *out, const void *base, bool is_float, uint32_t cols, uint32_t rows, uint32_t pitch,
+                   uint32_t box_cols, uint32_t box_rows) {
+    auto fn = tensor_map_encoder();
+    if (!fn) TPT_FAIL(TPT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available from the driver");
+    cuuint64_t dims[2] = {cols, rows};
+    cuuint64_t strides[1] = {(cuuint64_t)pitch * 4};
+    cuuint32_t box[2] = {box_cols, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(out, is_float ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT32, 2,
+                    const_cast<void *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) TPT_FAIL(TPT_ERR_CUDA, "cuTensorMapEncodeTiled (grid %ux%u pitch %u) failed (%d)", cols, rows,
+                                    pitch, (int)r);
     return TPT_OK;
 }
 

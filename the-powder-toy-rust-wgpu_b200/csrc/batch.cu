@@ -26,6 +26,7 @@
 #include "air_launch.hpp"
 #include "grav_dft.hpp"
 #include "grav_plan.hpp"
+#include "tmap.hpp"
 
 using namespace tpt;
 
@@ -142,8 +143,14 @@ struct tpt_batch {
     float *f32 = nullptr;
     uint32_t *u32 = nullptr;
     int32_t *i32 = nullptr;
-    std::vector<AirInst> insts_host;
+    // two AirInst per instance for each form: the sweep form's (every state
+    // grid in ping-pong halves) and the tile form's (pv/vx/vy in place; heat
+    // and masks in ping-pong halves), and the tile form's tensor maps
+    std::vector<AirInst> insts_host, insts_tile_host;
     AirInst *insts = nullptr;
+    AirInst *insts_tile = nullptr;
+    CUtensorMap *tmaps = nullptr;
+    bool any_noupdate_heat = false;
     air::TileRef *tiles = nullptr;
     uint32_t ntiles = 0;
     // the sweep form of the air tick: work items (device), the queue counter
@@ -153,7 +160,7 @@ struct tpt_batch {
     uint32_t *ctl = nullptr;
     uint32_t *want = nullptr;
     bool any_grav = false;
-    tpt_batch_tuning tuning{DEFAULT_LANES, DEFAULT_ROWS, 1, 0, 0};
+    tpt_batch_tuning tuning{DEFAULT_LANES, DEFAULT_ROWS, 1, 0, 0, TPT_AIR_FORM_TILES};
     int sweep_occupancy = 1;  // resident sweep CTAs per SM at tuning.tile_x lanes
     int sms = 148;
     gfft::FftSet fft;
@@ -188,7 +195,17 @@ struct tpt_batch {
         L.want = want;
         return L;
     }
-    int air_tick(uint32_t parity, cudaStream_t st) const { return air::launch_sweep_tick(sweep(), parity, st); }
+    // the tile form's persistent grid: ctas_per_sm per SM (0: six, the
+    // residency of its advection/heat pass)
+    uint32_t tile_grid() const {
+        return std::min<uint32_t>(ntiles, (uint32_t)sms * (tuning.ctas_per_sm ? tuning.ctas_per_sm : 6u));
+    }
+    bool sweep_form() const { return tuning.air_form == TPT_AIR_FORM_SWEEP; }
+    const AirInst *form_insts() const { return sweep_form() ? insts : insts_tile; }
+    int air_tick(uint32_t parity, cudaStream_t st) const {
+        if (sweep_form()) return air::launch_sweep_tick(sweep(), parity, st);
+        return air::launch_tile_tick(insts_tile, tmaps, tiles, ntiles, tile_grid(), parity, any_noupdate_heat, st);
+    }
     int grav_solve(cudaStream_t st) const {
         return precision == TPT_PRECISION_FP32 ? fft.launch(st) : dft.launch(st);
     }
@@ -203,6 +220,8 @@ struct tpt_batch {
         cudaFree(u32);
         cudaFree(i32);
         cudaFree(insts);
+        cudaFree(insts_tile);
+        cudaFree(tmaps);
         cudaFree(stage);
         cudaFree(io);
         cudaFree(tiles);
@@ -231,7 +250,7 @@ static int record_ticks(tpt_batch *b, uint32_t ticks, cudaStream_t st) {
         if (rc) return rc;
     }
     if (ticks & 1u) {
-        rc = air::launch_copy_back(b->insts, b->tiles, b->ntiles, b->grid(), st);
+        rc = air::launch_copy_back(b->form_insts(), b->tiles, b->ntiles, b->grid(), st);
         if (rc) return rc;
     }
     if (b->any_grav) {
@@ -367,6 +386,7 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     }
     int rc = require_sm100();
     if (rc) return rc;
+    if (!tensor_map_encoder()) TPT_FAIL(TPT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available");
     tpt_batch *b = new (std::nothrow) tpt_batch();
     if (!b) TPT_FAIL(TPT_ERR_OUT_OF_MEMORY, "host allocation failed");
     auto bail = [&](int code) {
@@ -402,6 +422,8 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     // the second copies; parity 1 the reverse.
     std::vector<air::TileRef> tiles;
     b->insts_host.resize(2 * (size_t)n);
+    b->insts_tile_host.resize(2 * (size_t)n);
+    std::vector<CUtensorMap> tm((size_t)n * air::TM_COUNT);
     std::vector<JobShape> gshapes;
     std::vector<uint32_t> gidx;
     for (uint32_t i = 0; i < n; ++i) {
@@ -437,7 +459,36 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
             J.bair_out = b->u(par ? U_BA : U_BA2, i);
             J.bairh_out = b->u(par ? U_BH : U_BH2, i);
             b->insts_host[2 * (size_t)i + par] = J;
+            // the tile form: pv/vx/vy in their canonical buffers, updated in place
+            AirInst T = J;
+            T.pv = b->f(F_PV, i);
+            T.vx = b->f(F_VX, i);
+            T.vy = b->f(F_VY, i);
+            T.pv_out = T.vx_out = T.vy_out = nullptr;
+            b->insts_tile_host[2 * (size_t)i + par] = T;
         }
+        // tensor maps of the grids the tile form's two passes stage (box = tile + halo)
+        CUtensorMap *m = &tm[(size_t)i * air::TM_COUNT];
+        const uint32_t X = p.xcells, Y = p.ycells, P = b->pitch[i];
+        const uint32_t BW = AIR_TX + 8, BH = AIR_TY + 6;
+        struct Slot {
+            int slot;
+            const void *base;
+            bool f;
+        } slots[] = {
+            {air::TM_PV, b->f(F_PV, i), true},        {air::TM_VX, b->f(F_VX, i), true},
+            {air::TM_VY, b->f(F_VY, i), true},        {air::TM_OVX, b->f(F_OVX, i), true},
+            {air::TM_OVY, b->f(F_OVY, i), true},      {air::TM_OPV, b->f(F_OPV, i), true},
+            {air::TM_BA0, b->u(U_BA, i), false},      {air::TM_BA1, b->u(U_BA2, i), false},
+            {air::TM_BH0, b->u(U_BH, i), false},      {air::TM_BH1, b->u(U_BH2, i), false},
+            {air::TM_HV0, b->insts_tile_host[2 * (size_t)i].hv, true},
+            {air::TM_HV1, b->insts_tile_host[2 * (size_t)i + 1].hv, true},
+        };
+        for (const Slot &sl : slots) {
+            rc = make_grid_tmap(&m[sl.slot], sl.base, sl.f, X, Y, P, BW, BH);
+            if (rc) return bail(rc);
+        }
+        if (p.air_mode == 4u && p.aheat_enable) b->any_noupdate_heat = true;
         for (uint32_t ty = 0; ty * AIR_TY < p.ycells; ++ty)
             for (uint32_t tx = 0; tx * AIR_TX < p.xcells; ++tx) tiles.push_back({i, (uint16_t)tx, (uint16_t)ty});
         if (descs[i].newton_grav) {
@@ -447,6 +498,12 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     }
     b->ntiles = (uint32_t)tiles.size();
     e = cudaMalloc(&b->insts, b->insts_host.size() * sizeof(AirInst));
+    if (e == cudaSuccess) e = cudaMalloc(&b->insts_tile, b->insts_tile_host.size() * sizeof(AirInst));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->insts_tile, b->insts_tile_host.data(), b->insts_tile_host.size() * sizeof(AirInst),
+                       cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&b->tmaps, tm.size() * sizeof(CUtensorMap));
+    if (e == cudaSuccess) e = cudaMemcpy(b->tmaps, tm.data(), tm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&b->tiles, tiles.size() * sizeof(air::TileRef));
     if (e == cudaSuccess)
         e = cudaMemcpy(b->insts, b->insts_host.data(), b->insts_host.size() * sizeof(AirInst), cudaMemcpyHostToDevice);
@@ -642,6 +699,8 @@ int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
                  TPT_MAX_CELLS_PER_SIDE);
     if (t->temporal_depth != 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "temporal depth %u not built", t->temporal_depth);
     if (t->ctas_per_sm > 32) TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm must be 0 (as many as fit) .. 32");
+    if (t->air_form != TPT_AIR_FORM_TILES && t->air_form != TPT_AIR_FORM_SWEEP)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "air_form %u is neither TPT_AIR_FORM_TILES nor TPT_AIR_FORM_SWEEP", t->air_form);
     const bool split = b->any_grav && b->precision == TPT_PRECISION_SPLIT_BF16 && b->dft.can_split();
     if (t->grav_side_ctas && !split)
         TPT_FAIL(TPT_ERR_INVALID_ARG, "grav_side_ctas must be 0: the batch's gravity has one kind of y stage");
@@ -653,7 +712,7 @@ int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
         int rc = set_sweep_shape(b, t->tile_x, t->tile_y);
         if (rc) return rc;
     }
-    if (t->ctas_per_sm > (uint32_t)b->sweep_occupancy)
+    if (t->air_form == TPT_AIR_FORM_SWEEP && t->ctas_per_sm > (uint32_t)b->sweep_occupancy)
         TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm %u exceeds the %d sweep CTAs of %u lanes that fit an SM",
                  t->ctas_per_sm, b->sweep_occupancy, t->tile_x);
     b->drop_graphs();
@@ -675,7 +734,10 @@ int tpt_batch_profile_phases(tpt_batch *b, uint32_t ticks, tpt_stream_t stream, 
         out->cells += c;
         if (b->descs[i].newton_grav) out->grav_cells += c;
     }
-    out->air_launches_per_tick = 2;  // velocity pre-pass (flagged instances only) + sweep
+    // sweep form: velocity pre-pass (flagged instances only) + sweep; tile
+    // form: pass A + pass B (+ a settle pass when an instance is NoUpdate with
+    // ambient heat)
+    out->air_launches_per_tick = b->sweep_form() ? 2 : (b->any_noupdate_heat ? 3 : 2);
     out->grav_launches_per_tick = b->any_grav ? (b->precision == TPT_PRECISION_FP32 ? 3 : b->dft.launches()) : 0;
     out->grav_flops_per_tick = b->any_grav && b->precision != TPT_PRECISION_FP32 ? b->dft.flops() : 0.0;
     cudaEvent_t e0, e1, e2;
@@ -744,44 +806,41 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    // Phase 1: the sweep's shape (lanes per CTA x rows per strip) and its
-    // resident CTAs per SM, by timing 20 air ticks of each candidate.
-    const uint32_t lane_c[] = {128, 160, 192, 224, 256};
-    const uint32_t row_c[] = {32, 64, 128};
+    // Phase 1: the air form and its layout, by timing 20 air ticks of each
+    // candidate: the tile form at 2..8 CTAs per SM, the sweep form at a few
+    // shapes (lanes per CTA x rows per strip) with as many CTAs as fit.
+    struct Cand {
+        uint32_t form, lanes, rows, per_sm;
+    };
+    std::vector<Cand> cands;
+    for (uint32_t c : {2u, 3u, 4u, 6u, 8u}) cands.push_back({TPT_AIR_FORM_TILES, b->tuning.tile_x, b->tuning.tile_y, c});
+    for (auto sh : {std::make_pair(224u, 64u), std::make_pair(256u, 64u), std::make_pair(256u, 32u)})
+        cands.push_back({TPT_AIR_FORM_SWEEP, sh.first, sh.second, 0u});
     tpt_batch_tuning best = b->tuning;
     float best_ms = 1e30f;
     int rc = TPT_OK;
-    for (uint32_t lanes : lane_c) {
-        for (uint32_t rows : row_c) {
-            tpt_batch_tuning t = b->tuning;
-            t.tile_x = lanes;
-            t.tile_y = rows;
-            t.ctas_per_sm = 0;
-            rc = tpt_batch_set_tuning(b, &t);
-            if (rc) break;
-            const uint32_t occ = (uint32_t)b->sweep_occupancy;
-            for (uint32_t per_sm = occ; per_sm + 1 >= occ && per_sm >= 1 && rc == TPT_OK; --per_sm) {
-                t.ctas_per_sm = per_sm;
-                rc = tpt_batch_set_tuning(b, &t);
-                const uint32_t trial = 20;
-                for (int rep = 0; rep < 2 && rc == TPT_OK; ++rep) {  // warm-up, then timed
-                    cudaEventRecord(e0, st);
-                    for (uint32_t k = 0; k < trial && rc == TPT_OK; ++k) rc = b->air_tick(k & 1u, st);
-                    cudaEventRecord(e1, st);
-                }
-                if (rc) break;
-                cudaEventSynchronize(e1);
-                float ms = 0;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (ms < best_ms) {
-                    best_ms = ms;
-                    best = t;
-                }
-                if (per_sm == 1) break;
-            }
-            if (rc) break;
+    for (const Cand &cd : cands) {
+        tpt_batch_tuning t = b->tuning;
+        t.air_form = cd.form;
+        t.tile_x = cd.lanes;
+        t.tile_y = cd.rows;
+        t.ctas_per_sm = cd.per_sm;
+        rc = tpt_batch_set_tuning(b, &t);
+        if (rc) break;
+        const uint32_t trial = 20;
+        for (int rep = 0; rep < 2 && rc == TPT_OK; ++rep) {  // warm-up, then timed
+            cudaEventRecord(e0, st);
+            for (uint32_t k = 0; k < trial && rc == TPT_OK; ++k) rc = b->air_tick(k & 1u, st);
+            cudaEventRecord(e1, st);
         }
         if (rc) break;
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+        }
     }
     // Phase 2, with that air shape: the gravity split -- the graph a step
     // replays (air and gravity chains together) per candidate CTA count of the
