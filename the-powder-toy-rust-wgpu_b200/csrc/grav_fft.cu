@@ -127,13 +127,23 @@ __global__ void __launch_bounds__(NT) rows_forward_w(const Job *__restrict__ job
     }
 }
 
+// The mass and the kernels are real, so the x spectrum of every row is
+// Hermitian: column n1 - kx of the convolved spectra is the conjugate of
+// column kx. Only the n1/2 + 1 columns with kx <= n1/2 are convolved; in the
+// warp FFT's storage order they are the even lanes' positions plus position 1
+// (kx = n1/2). Half-column index h maps to its storage column:
+__device__ __forceinline__ uint32_t half_col(uint32_t h, uint32_t m1) {
+    return h < 16u * m1 ? (h >> 4) * 32u + 2u * (h & 15u) : 1u;
+}
+
 // One column (storage column c of the row spectra): forward transform down
 // the column, product with each field's kernel spectrum, inverse transform;
 // the Y rows both fields need are left in tx / ty (shared memory). tx holds
 // the column's input before; fs (n2 entries, the same memory as ty) holds the
 // forward spectrum while the two products are taken, in the lane order the
 // registers use, so each lane reads back only what it wrote and the y field's
-// rows overwrite only entries their own lane has read.
+// rows overwrite only entries their own lane has read. The two fields share
+// one copy of the inverse transform's code (a loop that is not unrolled).
 template <int M>
 __device__ __forceinline__ void col_warp(const Job &J, uint32_t c, float2 *tx, float2 *fs, int lane) {
     float2 g[M];
@@ -145,78 +155,98 @@ __device__ __forceinline__ void col_warp(const Job &J, uint32_t c, float2 *tx, f
     WarpFft<M>::forward(g, J.tw2, lane);
 #pragma unroll
     for (int k = 0; k < M; ++k) fs[32 * k + lane] = g[k];
-    const float2 *kx = J.kx + (size_t)c * J.n2, *ky = J.ky + (size_t)c * J.n2;
+    __syncwarp();
+#pragma unroll 1
+    for (int f = 0; f < 2; ++f) {
+        const float2 *kf = (f ? J.ky : J.kx) + (size_t)c * J.n2;
 #pragma unroll
-    for (int k = 0; k < M; ++k) g[k] = cmulf(g[k], __ldg(kx + 32 * k + lane));
-    WarpFft<M>::inverse(g, J.tw2, lane);
+        for (int k = 0; k < M; ++k) g[k] = cmulf(fs[32 * k + lane], __ldg(kf + 32 * k + lane));
+        WarpFft<M>::inverse(g, J.tw2, lane);
+        float2 *dst = f ? fs : tx;
 #pragma unroll
-    for (int j1 = 0; j1 < M; ++j1) {
-        const uint32_t j = 32u * j1 + lane;
-        if (j < J.Y) tx[j] = g[j1];
-    }
-#pragma unroll
-    for (int k = 0; k < M; ++k) g[k] = cmulf(fs[32 * k + lane], __ldg(ky + 32 * k + lane));
-    WarpFft<M>::inverse(g, J.tw2, lane);
-#pragma unroll
-    for (int j1 = 0; j1 < M; ++j1) {
-        const uint32_t j = 32u * j1 + lane;
-        if (j < J.Y) fs[j] = g[j1];
+        for (int j1 = 0; j1 < M; ++j1) {
+            const uint32_t j = 32u * j1 + lane;
+            if (j < J.Y) dst[j] = g[j1];
+        }
     }
 }
 
-// A block takes WARPS consecutive storage columns of one job: the Y x WARPS
-// tile is staged through shared memory (row runs of WARPS columns are
-// contiguous), each warp transforms one column, and both fields' Y x WARPS
-// tiles go back the same way. Per warp: `ystride` entries of the x field
-// tile, `fstride` (>= n2) of the spectrum stash / y field tile.
+// A block takes WARPS consecutive half-column indices of one job: the Y x
+// WARPS tile is staged through shared memory (each row's columns lie within
+// 2 * WARPS consecutive positions), each warp transforms one column, and both
+// fields' Y x WARPS tiles go back the same way. Per warp: `ystride` entries of
+// the x field tile, `fstride` (>= n2) of the spectrum stash / y field tile.
 __global__ void __launch_bounds__(NT) cols_convolve_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
                                                       uint32_t ystride, uint32_t fstride) {
     extern __shared__ float2 sm2[];
     const BlockRef r = refs[blockIdx.x];
     const Job J = jobs[r.job];
-    const uint32_t c0 = r.item, n1 = J.n1, Y = J.Y;
+    const uint32_t h0 = r.item, n1 = J.n1, Y = J.Y, m1 = n1 >> 5, nh = n1 / 2 + 1;
     float2 *TX = sm2, *TY = sm2 + (size_t)WARPS * ystride;
     for (uint32_t i = threadIdx.x; i < Y * WARPS; i += NT) {
         const uint32_t j = i / WARPS, col = i - j * WARPS;
-        TX[(size_t)col * ystride + j] = J.work[(size_t)j * n1 + c0 + col];
+        if (h0 + col < nh) TX[(size_t)col * ystride + j] = J.work[(size_t)j * n1 + half_col(h0 + col, m1)];
     }
     __syncthreads();
     const int wi = threadIdx.x / 32, lane = threadIdx.x & 31;
     float2 *tx = TX + (size_t)wi * ystride, *ty = TY + (size_t)wi * fstride;
-    switch (J.n2 >> 5) {
-        case 1: col_warp<1>(J, c0 + wi, tx, ty, lane); break;
-        case 2: col_warp<2>(J, c0 + wi, tx, ty, lane); break;
-        case 4: col_warp<4>(J, c0 + wi, tx, ty, lane); break;
-        case 8: col_warp<8>(J, c0 + wi, tx, ty, lane); break;
-        case 16: col_warp<16>(J, c0 + wi, tx, ty, lane); break;
-        case 32: col_warp<32>(J, c0 + wi, tx, ty, lane); break;
-        default: break;
+    if (h0 + wi < nh) {
+        const uint32_t c = half_col(h0 + wi, m1);
+        switch (J.n2 >> 5) {
+            case 1: col_warp<1>(J, c, tx, ty, lane); break;
+            case 2: col_warp<2>(J, c, tx, ty, lane); break;
+            case 4: col_warp<4>(J, c, tx, ty, lane); break;
+            case 8: col_warp<8>(J, c, tx, ty, lane); break;
+            case 16: col_warp<16>(J, c, tx, ty, lane); break;
+            case 32: col_warp<32>(J, c, tx, ty, lane); break;
+            default: break;
+        }
     }
     __syncthreads();
     float2 *sx = J.spec, *sy = J.spec + (size_t)Y * n1;
     for (uint32_t i = threadIdx.x; i < Y * WARPS; i += NT) {
         const uint32_t j = i / WARPS, col = i - j * WARPS;
-        const size_t g = (size_t)j * n1 + c0 + col;
+        if (h0 + col >= nh) continue;
+        const size_t g = (size_t)j * n1 + half_col(h0 + col, m1);
         sx[g] = TX[(size_t)col * ystride + j];
         sy[g] = TY[(size_t)col * fstride + j];
     }
 }
 
-// Inverse transform of spectrum row y of one field; real part of the first X
-// outputs, masked.
-template <int M> __device__ __forceinline__ void row_inv_warp(const Job &J, uint32_t field, uint32_t y, int lane) {
-    const float2 *src = J.spec + ((size_t)field * J.Y + y) * J.n1;
+// Inverse transform of spectrum row y of both fields at once: both outputs
+// are real, so gx + i gy is the inverse of Sx + i Sy. The full row spectra
+// are rebuilt from the convolved half: position p of the permuted order holds
+// frequency kx; an odd lane's position (except kx = n1/2) holds kx > n1/2,
+// whose value is the conjugate of the stored kx' = n1 - kx. Outputs: the first
+// X, masked.
+template <int M> __device__ __forceinline__ void row_inv_warp(const Job &J, uint32_t y, int lane) {
+    const float2 *rx = J.spec + (size_t)y * J.n1, *ry = J.spec + ((size_t)J.Y + y) * J.n1;
     float2 v[M];
 #pragma unroll
-    for (int k = 0; k < M; ++k) v[k] = src[32 * k + lane];
+    for (int k1 = 0; k1 < M; ++k1) {
+        const bool direct = (lane & 1) == 0 || (k1 == 0 && lane == 1);
+        uint32_t p = 32u * k1 + lane;
+        if (!direct) {
+            const uint32_t kx = (uint32_t)k1 + (uint32_t)M * (uint32_t)brev_c(lane, 5);
+            const uint32_t km = J.n1 - kx;
+            p = (km % (uint32_t)M) * 32u + (__brev(km / (uint32_t)M) >> 27);
+        }
+        float2 sx = rx[p], sy = ry[p];
+        if (!direct) {
+            sx.y = -sx.y;
+            sy.y = -sy.y;
+        }
+        v[k1] = make_float2(sx.x - sy.y, sx.y + sy.x);  // sx + i sy
+    }
     WarpFft<M>::inverse(v, J.tw1, lane);
-    float *out = field ? J.gy : J.gx;
 #pragma unroll
     for (int j1 = 0; j1 < M; ++j1) {
         const uint32_t x = 32u * j1 + lane;
         if (x < J.X) {
             const size_t c = (size_t)y * J.pitch + x;
-            out[c] = __ldg(J.mask + c) != 0u ? v[j1].x : 0.0f;
+            const bool on = __ldg(J.mask + c) != 0u;
+            J.gx[c] = on ? v[j1].x : 0.0f;
+            J.gy[c] = on ? v[j1].y : 0.0f;
         }
     }
 }
@@ -228,14 +258,13 @@ __global__ void __launch_bounds__(NT) rows_inverse_w(const Job *__restrict__ job
     const int lane = threadIdx.x & 31;
     const BlockRef r = refs[w];
     const Job J = load_job(jobs, r.job, io);
-    const uint32_t field = r.item / J.Y, y = r.item - field * J.Y;
     switch (J.n1 >> 5) {
-        case 1: row_inv_warp<1>(J, field, y, lane); break;
-        case 2: row_inv_warp<2>(J, field, y, lane); break;
-        case 4: row_inv_warp<4>(J, field, y, lane); break;
-        case 8: row_inv_warp<8>(J, field, y, lane); break;
-        case 16: row_inv_warp<16>(J, field, y, lane); break;
-        case 32: row_inv_warp<32>(J, field, y, lane); break;
+        case 1: row_inv_warp<1>(J, r.item, lane); break;
+        case 2: row_inv_warp<2>(J, r.item, lane); break;
+        case 4: row_inv_warp<4>(J, r.item, lane); break;
+        case 8: row_inv_warp<8>(J, r.item, lane); break;
+        case 16: row_inv_warp<16>(J, r.item, lane); break;
+        case 32: row_inv_warp<32>(J, r.item, lane); break;
         default: break;
     }
 }
@@ -507,8 +536,9 @@ int FftSet::create(const std::vector<JobShape> &shapes) {
         for (uint32_t y = 0; y < s.Y; ++y) rr.push_back({(uint32_t)j, y});
         int cb = std::min<int>(col_block(J.n2), (int)J.n1);
         max_cb = std::max(max_cb, cb);
-        for (uint32_t c = 0; c < J.n1; c += cb) cr.push_back({(uint32_t)j, c});
-        for (uint32_t i = 0; i < 2 * s.Y; ++i) ir.push_back({(uint32_t)j, i});
+        // warp form: one inverse row per y (both fields); shared-memory form:
+        // one per (field, y)
+        for (uint32_t i = 0; i < (warp ? 1u : 2u) * s.Y; ++i) ir.push_back({(uint32_t)j, i});
     }
     // the column kernel needs one cb for the whole launch: use the smallest
     // needed by any job (power-of-two, divides every n1); the warp form
@@ -519,8 +549,25 @@ int FftSet::create(const std::vector<JobShape> &shapes) {
     max_y = 0;
     for (auto &J : jobs_host) max_y = std::max(max_y, J.Y);
     cr.clear();
-    for (size_t j = 0; j < nj; ++j)
-        for (uint32_t c = 0; c < jobs_host[j].n1; c += cb_launch) cr.push_back({(uint32_t)j, c});
+    for (size_t j = 0; j < nj; ++j) {
+        // warp form: WARPS half-column indices per block (n1/2 + 1 columns)
+        const uint32_t ncol = warp ? jobs_host[j].n1 / 2 + 1 : jobs_host[j].n1;
+        for (uint32_t c = 0; c < ncol; c += cb_launch) cr.push_back({(uint32_t)j, c});
+    }
+    if (warp) {
+        // blocks of the same transform length run the same code: keep them
+        // together so that co-resident blocks share the instruction cache
+        auto by = [&](bool col) {
+            return [&, col](const BlockRef &a, const BlockRef &b) {
+                const uint32_t la = col ? jobs_host[a.job].n2 : jobs_host[a.job].n1;
+                const uint32_t lb = col ? jobs_host[b.job].n2 : jobs_host[b.job].n1;
+                return la > lb;
+            };
+        };
+        std::stable_sort(rr.begin(), rr.end(), by(false));
+        std::stable_sort(cr.begin(), cr.end(), by(true));
+        std::stable_sort(ir.begin(), ir.end(), by(false));
+    }
     n_rows = (uint32_t)rr.size();
     n_cols = (uint32_t)cr.size();
     n_inv = (uint32_t)ir.size();
