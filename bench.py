@@ -44,10 +44,12 @@ import numpy as np  # noqa: E402
 
 B_AIR = 52  # algorithmic bytes per cell-tick of the air step (reference layout)
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one air tick
-# (both launches) and of one gravity solve of the whole batch (the five GEMM
-# launches), from one ncu capture of each kernel on that workload at the tuned
-# setting; workloads without a capture report null.
-MEASURED_DRAM_BYTES = {5: {"air_tick": 532.8e6, "grav_solve": 418.4e6}}
+# (both tile-form launches) and of one gravity solve of the whole batch (the
+# GEMM launches), from ncu captures; workloads without a capture report null.
+# Air: 74.7 bytes per cell-tick measured on the first 32 instances of the
+# 128-instance batch (2.88 M cells, well above L2) after 900 ticks, scaled by
+# its 6,121,601 cells (traffic grows with the cells staged).
+MEASURED_DRAM_BYTES = {5: {"air_tick": 457.3e6, "grav_solve": 418.4e6}}
 WORKLOAD_NAMES = {
     1: "C1 plain FP32 air+gravity, 153x96 cells (612x384 canvas)",
     2: "C2 plain FP32 air+gravity, 400x225 cells (1600x900 canvas)",
@@ -280,6 +282,8 @@ def run_ours(args, rank, world, local):
     tf.lib()
     cid = args.workload
     insts = workload(cid)
+    if args.instances:  # a prefix of the workload, for profiling captures
+        insts = insts[: args.instances]
     total_cells = sum(i.cells for i in insts)
     cfg = config_of(cid, insts, args.ticks or None)
     if args.scaling == "strong" and world > 1:  # this rank's share, no exchange between ranks
@@ -288,7 +292,13 @@ def run_ours(args, rank, world, local):
     precision = tf.PRECISION_SPLIT_BF16 if cid == 5 else tf.PRECISION_FP32
     stream = torch.cuda.current_stream()
     batch = tf.Batch(insts, precision)
-    batch.tune()
+    if not args.skip_tune:
+        batch.tune()
+    if args.air_form != "tuned":
+        t = batch.tuning()
+        t.air_form = tf.AIR_FORM_SWEEP if args.air_form == "sweep" else tf.AIR_FORM_TILES
+        t.ctas_per_sm = 0
+        batch.set_tuning(t)
     cells = sum(i.cells for i in insts)
     # cells all ranks advance per tick: every rank has a full copy (weak) or
     # a share of one copy (strong)
@@ -734,6 +744,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer run (profiling captures)")
     ap.add_argument("--phase-ticks", type=int, default=200, help="even tick count of the per-phase timing")
+    ap.add_argument("--air-form", choices=("tuned", "tiles", "sweep"), default="tuned",
+                    help="air tick form of the batched workloads (default: the autotuner's choice)")
+    ap.add_argument("--skip-tune", action="store_true", help="keep the batch's default tuning (profiling captures)")
+    ap.add_argument("--instances", type=int, default=0,
+                    help="only the first N instances of the workload (profiling captures on a smaller case)")
     ap.add_argument("--voxel3d", action="store_true", help="the 3-D sandbox's field step instead of the 2-D one")
     ap.add_argument("--worlds", type=int, default=1, help="3-D worlds per rank (--voxel3d)")
     ap.add_argument("--save-io", action="store_true", help="host timing of the .tptrs save codec")

@@ -87,7 +87,11 @@ __global__ void __launch_bounds__(NT) rows_inverse(const Job *__restrict__ jobs,
 }
 
 // ---- the warp form: one warp per 1-D transform ---------------------------------
-constexpr int WARPS = NT / 32;
+// 128-thread CTAs: the kernels hold a whole transform per warp in registers
+// (91 to 168 per thread), so CTAs of four warps let three or more share an SM
+// where CTAs of eight warps left registers unused (C4 solve 1.36 -> 1.06 ms).
+constexpr int NTW = 128;
+constexpr int WARPS = NTW / 32;
 
 // Forward transform of mass row y (real, zero beyond X and where the mask is
 // clear), stored in the warp FFT's permuted order.
@@ -109,7 +113,7 @@ template <int M> __device__ __forceinline__ void row_fwd_warp(const Job &J, uint
     for (int k = 0; k < M; ++k) dst[32 * k + lane] = v[k];
 }
 
-__global__ void __launch_bounds__(NT) rows_forward_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
+__global__ void __launch_bounds__(NTW) rows_forward_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
                                                      uint32_t nrefs, const JobIO io) {
     const uint32_t w = blockIdx.x * WARPS + threadIdx.x / 32;
     if (w >= nrefs) return;
@@ -176,14 +180,14 @@ __device__ __forceinline__ void col_warp(const Job &J, uint32_t c, float2 *tx, f
 // 2 * WARPS consecutive positions), each warp transforms one column, and both
 // fields' Y x WARPS tiles go back the same way. Per warp: `ystride` entries of
 // the x field tile, `fstride` (>= n2) of the spectrum stash / y field tile.
-__global__ void __launch_bounds__(NT) cols_convolve_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
+__global__ void __launch_bounds__(NTW) cols_convolve_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
                                                       uint32_t ystride, uint32_t fstride) {
     extern __shared__ float2 sm2[];
     const BlockRef r = refs[blockIdx.x];
     const Job J = jobs[r.job];
     const uint32_t h0 = r.item, n1 = J.n1, Y = J.Y, m1 = n1 >> 5, nh = n1 / 2 + 1;
     float2 *TX = sm2, *TY = sm2 + (size_t)WARPS * ystride;
-    for (uint32_t i = threadIdx.x; i < Y * WARPS; i += NT) {
+    for (uint32_t i = threadIdx.x; i < Y * WARPS; i += NTW) {
         const uint32_t j = i / WARPS, col = i - j * WARPS;
         if (h0 + col < nh) TX[(size_t)col * ystride + j] = J.work[(size_t)j * n1 + half_col(h0 + col, m1)];
     }
@@ -204,7 +208,7 @@ __global__ void __launch_bounds__(NT) cols_convolve_w(const Job *__restrict__ jo
     }
     __syncthreads();
     float2 *sx = J.spec, *sy = J.spec + (size_t)Y * n1;
-    for (uint32_t i = threadIdx.x; i < Y * WARPS; i += NT) {
+    for (uint32_t i = threadIdx.x; i < Y * WARPS; i += NTW) {
         const uint32_t j = i / WARPS, col = i - j * WARPS;
         if (h0 + col >= nh) continue;
         const size_t g = (size_t)j * n1 + half_col(h0 + col, m1);
@@ -251,7 +255,7 @@ template <int M> __device__ __forceinline__ void row_inv_warp(const Job &J, uint
     }
 }
 
-__global__ void __launch_bounds__(NT) rows_inverse_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
+__global__ void __launch_bounds__(NTW) rows_inverse_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
                                                      uint32_t nrefs, const JobIO io) {
     const uint32_t w = blockIdx.x * WARPS + threadIdx.x / 32;
     if (w >= nrefs) return;
@@ -604,12 +608,12 @@ int FftSet::launch(cudaStream_t st, const JobIO *io) const {
     JobIO none{};
     const JobIO &a = io ? *io : none;
     if (warp) {
-        rows_forward_w<<<(n_rows + WARPS - 1) / WARPS, NT, 0, st>>>(jobs, refs, n_rows, a);
+        rows_forward_w<<<(n_rows + WARPS - 1) / WARPS, NTW, 0, st>>>(jobs, refs, n_rows, a);
         TPT_LAUNCHED();
-        cols_convolve_w<<<n_cols, NT, (size_t)WARPS * (max_y + max_n2) * sizeof(float2), st>>>(jobs, refs + n_rows,
+        cols_convolve_w<<<n_cols, NTW, (size_t)WARPS * (max_y + max_n2) * sizeof(float2), st>>>(jobs, refs + n_rows,
                                                                                                max_y, max_n2);
         TPT_LAUNCHED();
-        rows_inverse_w<<<(n_inv + WARPS - 1) / WARPS, NT, 0, st>>>(jobs, refs + n_rows + n_cols, n_inv, a);
+        rows_inverse_w<<<(n_inv + WARPS - 1) / WARPS, NTW, 0, st>>>(jobs, refs + n_rows + n_cols, n_inv, a);
         TPT_LAUNCHED();
         return TPT_OK;
     }
