@@ -297,6 +297,7 @@ def run_ours(args, rank, world, local):
     if args.air_form != "tuned":
         t = batch.tuning()
         t.air_form = tf.AIR_FORM_SWEEP if args.air_form == "sweep" else tf.AIR_FORM_TILES
+        t.tile_x, t.tile_y = args.air_shape or ((224, 64) if args.air_form == "sweep" else tf.TILE_SHAPES[0])
         t.ctas_per_sm = 0
         batch.set_tuning(t)
     cells = sum(i.cells for i in insts)
@@ -746,6 +747,8 @@ def main():
     ap.add_argument("--phase-ticks", type=int, default=200, help="even tick count of the per-phase timing")
     ap.add_argument("--air-form", choices=("tuned", "tiles", "sweep"), default="tuned",
                     help="air tick form of the batched workloads (default: the autotuner's choice)")
+    ap.add_argument("--air-shape", type=lambda v: tuple(int(x) for x in v.split("x")), default=None,
+                    help="with --air-form: tile (tiles) or lanes x rows (sweep), e.g. 64x16")
     ap.add_argument("--skip-tune", action="store_true", help="keep the batch's default tuning (profiling captures)")
     ap.add_argument("--instances", type=int, default=0,
                     help="only the first N instances of the workload (profiling captures on a smaller case)")

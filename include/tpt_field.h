@@ -344,9 +344,10 @@ int tpt_batch_read_field(tpt_batch *batch, int field, void *host,
 
 /* Forms of the batch's air tick (tpt_batch_tuning.air_form). */
 enum {
-    /* Two launches per tick over 32x8-cell tiles, halos staged by TMA: pass A
-     * (pressure, velocity) writes opv/ovx/ovy, pass B (smoothing, advection,
-     * vorticity, fans, heat, convection, masks) reads them. */
+    /* Two launches per tick over tiles (32x8, 64x8, 32x16 or 64x16 cells),
+     * halos staged by TMA: pass A (pressure, velocity) writes opv/ovx/ovy,
+     * pass B (smoothing, advection, vorticity, fans, heat, convection, masks)
+     * reads them. */
     TPT_AIR_FORM_TILES = 0,
     /* One fused launch per tick: CTAs sweep down column strips with every
      * stage pipelined over the rows (no intermediate grid in memory), plus a
@@ -358,11 +359,13 @@ enum {
  * same for every value: they change how the work is laid out, not what is
  * computed. */
 typedef struct tpt_batch_tuning {
-    /* The sweep form's work unit: a CTA of tile_x lanes (a multiple of 32 in
-     * 64..256) sweeps down strips of about tile_y rows (8..2048). Each lane
-     * owns a column; a strip is at most tile_x - 12 columns wide (six halo
-     * columns on each side), and strips of narrow instances are packed side
-     * by side into one CTA. The tile form's tiles are 32x8 cells. */
+    /* The air form's work unit. Tile form: the tile, tile_x x tile_y cells,
+     * one of 32x8 (the default), 64x8, 32x16 and 64x16, one thread per cell.
+     * Sweep form: a CTA of tile_x lanes (a multiple of 32 in 64..256) sweeps
+     * down strips of about tile_y rows (8..2048); each lane owns a column, a
+     * strip is at most tile_x - 12 columns wide (six halo columns on each
+     * side), and strips of narrow instances are packed side by side into one
+     * CTA. */
     uint32_t tile_x, tile_y;
     uint32_t temporal_depth;  /* ticks per air launch (1 = no blocking)   */
     /* Resident CTAs per SM of the air form's persistent launches (0 = as
@@ -396,9 +399,8 @@ int tpt_batch_fields(tpt_batch *batch, uint32_t instance,
  */
 int tpt_batch_step(tpt_batch *batch, uint32_t ticks, tpt_stream_t stream);
 /* Times candidate tunings on the batch's own data (state is saved and
- * restored) and keeps the fastest: the air form with its CTAs per SM (and
- * for the sweep form its shape, tile_x x tile_y), then the gravity branch
- * split. The choice is cached in
+ * restored) and keeps the fastest: the air form with its shape (tile_x x
+ * tile_y) and CTAs per SM, then the gravity branch split. The choice is cached in
  * the process per batch composition -- the instances' (xcells, ycells)
  * buckets (powers of two) with their counts, and the gravity precision -- so
  * tuning a batch of the same composition again only applies the cached

@@ -39,8 +39,12 @@ def check_against_oracle(tf, oracle, batch, insts, ticks, ctx):
 
 
 def set_form(tf, b, form, **kw):
+    """Switches the batch's air form; tile_x / tile_y default to the form's
+    default shape (32x8 tiles, 224-lane x 64-row sweeps), ctas_per_sm to 0."""
     t = b.tuning()
     t.air_form = form
+    t.tile_x, t.tile_y = (224, 64) if form == tf.AIR_FORM_SWEEP else tf.TILE_SHAPES[0]
+    t.ctas_per_sm = 0
     for k, v in kw.items():
         setattr(t, k, v)
     b.set_tuning(t)
@@ -76,7 +80,7 @@ def test_tune_keeps_state_and_results(cuda, tf, oracle):
     t = b.tuning()
     assert t.air_form in (tf.AIR_FORM_TILES, tf.AIR_FORM_SWEEP) and t.temporal_depth == 1
     if t.air_form == tf.AIR_FORM_TILES:
-        assert t.ctas_per_sm in (2, 3, 4, 6, 8)
+        assert (t.tile_x, t.tile_y) in tf.TILE_SHAPES and 1 <= t.ctas_per_sm <= 8
     else:
         assert (t.tile_x, t.tile_y) in ((224, 64), (256, 64), (256, 32))
     b.step(5)
@@ -106,6 +110,23 @@ def test_every_sweep_shape_gives_the_same_fields(cuda, tf, oracle, tile_x, tile_
     b.close()
 
 
+@pytest.mark.parametrize("shape", [(32, 8), (64, 8), (32, 16), (64, 16)])
+@pytest.mark.parametrize("per_sm", [0, 1, 2])
+def test_every_tile_shape_gives_the_same_fields(cuda, tf, oracle, shape, per_sm):
+    """Every tile shape of the tile form (its own kernels, tile list and
+    tensor-map boxes) at as many CTAs per SM as fit, one and two: the fields
+    after 9 ticks (odd: the copy-back runs) are bit-exact."""
+    assert shape in tf.TILE_SHAPES
+    insts = mixed_instances()
+    b = tf.Batch(insts)
+    set_form(tf, b, tf.AIR_FORM_TILES, tile_x=shape[0], tile_y=shape[1], ctas_per_sm=per_sm)
+    b.step(9)
+    cuda.cuda.synchronize()
+    assert tf.lib().tpt_check_device_errors() == 0
+    check_against_oracle(tf, oracle, b, insts, 9, f"tiles {shape[0]}x{shape[1]} {per_sm}/SM")
+    b.close()
+
+
 @pytest.mark.parametrize("per_sm", [1, 3, 6, 8])
 def test_tile_form_at_every_grid_size(cuda, tf, oracle, per_sm):
     insts = mixed_instances()
@@ -123,23 +144,35 @@ def test_switching_forms_between_steps(cuda, tf, oracle):
     form, so a batch may change form from one step to the next."""
     insts = mixed_instances()
     b = tf.Batch(insts)
-    for form, ticks in ((1, 3), (0, 4), (1, 1), (0, 2)):
-        set_form(tf, b, form)
+    for form, shape, ticks in ((1, (224, 64), 3), (0, (32, 8), 4), (1, (256, 32), 1), (0, (64, 16), 2),
+                               (0, (32, 16), 1)):
+        set_form(tf, b, form, tile_x=shape[0], tile_y=shape[1])
         b.step(ticks)
     cuda.cuda.synchronize()
-    check_against_oracle(tf, oracle, b, insts, 10, "form switches")
+    check_against_oracle(tf, oracle, b, insts, 11, "form switches")
     b.close()
 
 
 def test_bad_tunings_are_rejected(cuda, tf):
     b = tf.Batch(mixed_instances()[:2])
-    for kw in (dict(tile_x=100), dict(tile_x=32), dict(tile_x=288), dict(tile_y=4), dict(temporal_depth=2),
-               dict(ctas_per_sm=64), dict(air_form=2), dict(air_form=1, ctas_per_sm=9)):
+    before = b.tuning_dict()
+    tiles, sweep = tf.AIR_FORM_TILES, tf.AIR_FORM_SWEEP
+    for kw in (
+        # tile form: only the four shapes
+        dict(air_form=tiles, tile_x=48, tile_y=8), dict(air_form=tiles, tile_x=64, tile_y=32),
+        dict(air_form=tiles, tile_x=224, tile_y=64), dict(air_form=tiles, tile_x=32, tile_y=8, ctas_per_sm=64),
+        # sweep form: lanes a multiple of 32 in 64..256, rows >= 8, CTAs that fit
+        dict(air_form=sweep, tile_x=100, tile_y=64), dict(air_form=sweep, tile_x=32, tile_y=64),
+        dict(air_form=sweep, tile_x=288, tile_y=64), dict(air_form=sweep, tile_x=224, tile_y=4),
+        dict(air_form=sweep, tile_x=224, tile_y=64, ctas_per_sm=9),
+        dict(temporal_depth=2), dict(air_form=2),
+    ):
         t = b.tuning()
         for k, v in kw.items():
             setattr(t, k, v)
         with pytest.raises(tf.TptError):
             b.set_tuning(t)
+    assert b.tuning_dict() == before
     b.close()
 
 
@@ -193,8 +226,8 @@ def test_batch_measured_config_subset(cuda, tf, oracle):
     b.close()
 
 
-@pytest.mark.parametrize("form", [0, 1])
-def test_c4_every_instance_20_ticks(cuda, tf, oracle, form):
+@pytest.mark.parametrize("form,shape", [(0, (32, 8)), (0, (64, 8)), (0, (32, 16)), (1, (224, 64))])
+def test_c4_every_instance_20_ticks(cuda, tf, oracle, form, shape):
     """The whole C4 batch (256 instances, W, H log-uniform 32..512, FP32
     gravity) after 20 ticks: every instance's air bit-exact against the
     oracle and its gx/gy within 1e-5 of max|g| against FP64."""
@@ -203,11 +236,11 @@ def test_c4_every_instance_20_ticks(cuda, tf, oracle, form):
     insts = W.config_instances(4)
     assert len(insts) == 256
     b = tf.Batch(insts)
-    set_form(tf, b, form)
+    set_form(tf, b, form, tile_x=shape[0], tile_y=shape[1])
     b.step(20)
     cuda.cuda.synchronize()
     assert tf.lib().tpt_check_device_errors() == 0
-    check_against_oracle(tf, oracle, b, insts, 20, "C4")
+    check_against_oracle(tf, oracle, b, insts, 20, f"C4 form {form} {shape[0]}x{shape[1]}")
     b.close()
 
 

@@ -27,15 +27,27 @@
 // array with its own halo (Reg<H>); the batch's tile form stages every array
 // as one TMA box of the tile plus a 4-cell (x) by 3-cell (y) halo. The
 // batch's sweep form (air_sweep.cu) reuses the per-cell helpers below.
+//
+// The tile is AIR_TX x AIR_TY (32 x 8) cells, one thread per cell, unless the
+// including file defines AIR_TILE_X / AIR_TILE_Y: the batch's tile form is
+// compiled once per tile shape it offers (air_tiles.cu), each copy in its own
+// namespace AIR_SHAPE_NS.
 #pragma once
 
 #include "common.cuh"
 #include "exact_div.cuh"
 
+#ifndef AIR_TILE_X
+#define AIR_TILE_X AIR_TX
+#define AIR_TILE_Y AIR_TY
+#define AIR_SHAPE_NS s32x8
+#endif
+
 namespace tpt {
 namespace air {
+inline namespace AIR_SHAPE_NS {
 
-constexpr int TX = AIR_TX, TY = AIR_TY, NT = TX * TY;
+constexpr int TX = AIR_TILE_X, TY = AIR_TILE_Y, NT = TX * TY;
 
 // Tile plus an H-cell halo on every side.
 template <int H> struct Reg {
@@ -686,5 +698,6 @@ __device__ __forceinline__ void masks_cell(const AirInst &I, size_t g, uint32_t 
     masks_of(__ldg(I.wall + g), raw, I.eair ? __ldg(I.eair + g) : 0u, I.eairh ? __ldg(I.eairh + g) : 0u, bair, bairh);
 }
 
+}  // namespace AIR_SHAPE_NS
 }  // namespace air
 }  // namespace tpt

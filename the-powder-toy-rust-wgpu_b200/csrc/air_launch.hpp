@@ -8,25 +8,42 @@
 namespace tpt {
 namespace air {
 
-// One AIR_TX x AIR_TY tile of one batched instance (the pre-pass and the
-// copy-back walk these).
+// One tile of one batched instance: AIR_TX x AIR_TY cells for the pre-pass and
+// the copy-back, the tile form's shape for its passes.
 struct TileRef {
     uint32_t inst;
     uint16_t tx, ty;
 };
 
-// ---- the tile form (air_batch.cu) ---------------------------------------------
+// ---- the tile form (air_tiles.cu) ---------------------------------------------
 // Tensor maps of one batched instance: the grids the two passes stage, with
 // the two halves of the heat and mask ping-pong.
 enum TensorMapSlot {
     TM_PV, TM_VX, TM_VY, TM_OVX, TM_OVY, TM_OPV, TM_BA0, TM_BA1, TM_BH0, TM_BH1, TM_HV0, TM_HV1, TM_COUNT
 };
 
-// One tick of every instance in the tile form. `insts` holds two AirInst per
-// instance (parity 0 and 1 of the hv / mask ping-pong; pv/vx/vy are updated in
-// place); `tmaps` TM_COUNT tensor maps per instance.
-int launch_tile_tick(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles,
-                     uint32_t grid, uint32_t parity, bool any_noupdate_heat, cudaStream_t st);
+// One tile shape of the tile form (air_tiles.cu, compiled once per shape).
+// Its tiles are tx x ty cells, one thread per cell, each staged as a TMA box
+// of (tx + 8) x (ty + 6) cells: the tensor maps and the tile list of a batch
+// are built for the shape in use.
+struct TileShape {
+    uint32_t tx, ty;
+    // sets the kernels' shared-memory limits and returns the resident CTAs
+    // per SM of the advection/heat pass
+    int (*prepare)(int *occupancy);
+    // One tick of every instance. `insts` holds two AirInst per instance
+    // (parity 0 and 1 of the hv / mask ping-pong; pv/vx/vy are updated in
+    // place); `tmaps` TM_COUNT tensor maps per instance.
+    int (*launch)(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
+                  uint32_t parity, bool any_noupdate_heat, cudaStream_t st);
+    // reads and clears the shape's device error word
+    int (*read_errors)(uint32_t *out);
+};
+extern const TileShape tile_shape_s32x8, tile_shape_s64x8, tile_shape_s32x16, tile_shape_s64x16;
+constexpr int TILE_SHAPES = 4;
+// The offered shapes, 32x8 first; tile_shape(tx, ty) is null for any other.
+const TileShape *const *tile_shapes();
+const TileShape *tile_shape(uint32_t tx, uint32_t ty);
 
 // ---- the sweep form (air_sweep.cu) ----------------------------------------------
 // Lanes of halo on each side of a segment: the tick's stencil reaches six

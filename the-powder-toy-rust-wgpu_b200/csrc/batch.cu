@@ -5,10 +5,12 @@
 // `pitch_i` elements (pitch = xcells rounded up to 32, so rows start on
 // 128-byte boundaries as TMA needs); cell (cx, cy) is at cy * pitch + cx.
 // The air state (pv, vx, vy, hv and the two wall masks) has a second copy
-// (ping-pong): a tick reads one half and writes the other, so the whole air
-// tick is one sweep launch (air_sweep.cu) plus a velocity pre-pass that only
-// works for instances flagged by the previous tick; after an odd tick count
-// one copy-back restores the canonical buffers. Gravity (instances with
+// (ping-pong) for the air tick's two forms, chosen by the tuning: the tile
+// form (air_tiles.cu; two TMA-staged tile passes per tick, heat and masks in
+// the ping-pong halves, pv/vx/vy in place) or the row sweep (air_sweep.cu;
+// one launch per tick plus a velocity pre-pass that only works for instances
+// flagged by the previous tick, every state grid in ping-pong halves). After
+// an odd tick count one copy-back restores the canonical buffers. Gravity (instances with
 // newton_grav) is independent of air in the field step
 // (crates/tpt-sim/src/air_kernel/heat.rs:182-203 uses the configured
 // direction, not the Newtonian field), so it runs on a second stream branch
@@ -66,8 +68,9 @@ __global__ void k_batch_io(const IoInst *io, uint32_t base, uint32_t *arena, uin
 }  // namespace
 
 // Default sweep shape: 224 lanes (a 400-column grid in two 200-column strips
-// plus halos) by 64-row strips.
+// plus halos) by 64-row strips. Default tile form shape: 32 x 8 cells.
 constexpr uint32_t DEFAULT_LANES = 224, DEFAULT_ROWS = 64;
+constexpr uint32_t DEFAULT_TILE_X = 32, DEFAULT_TILE_Y = 8;
 
 // Splits every instance into column strips of at most lanes - 2 * SW_H
 // columns and row strips of about `rows` rows (sizes balanced within an
@@ -149,19 +152,27 @@ struct tpt_batch {
     std::vector<AirInst> insts_host, insts_tile_host;
     AirInst *insts = nullptr;
     AirInst *insts_tile = nullptr;
-    CUtensorMap *tmaps = nullptr;
     bool any_noupdate_heat = false;
+    // AIR_TX x AIR_TY tiles (the sweep's pre-pass, the copy-back)
     air::TileRef *tiles = nullptr;
     uint32_t ntiles = 0;
+    // the tile form at its current shape: tiles, tensor maps (boxes of the
+    // shape) and the advection/heat pass's resident CTAs per SM
+    const air::TileShape *shape = nullptr;
+    air::TileRef *form_tiles = nullptr;
+    uint32_t nform_tiles = 0;
+    CUtensorMap *tmaps = nullptr;
+    int tile_occupancy = 1;
     // the sweep form of the air tick: work items (device), the queue counter
     // and the pre-pass flags ([2][n], zeroed at creation)
     air::SweepItem *items = nullptr;
     uint32_t nitems = 0;
     uint32_t *ctl = nullptr;
     uint32_t *want = nullptr;
+    uint32_t sweep_lanes = 0, sweep_rows = 0;  // the shape the items are planned for
     bool any_grav = false;
-    tpt_batch_tuning tuning{DEFAULT_LANES, DEFAULT_ROWS, 1, 0, 0, TPT_AIR_FORM_TILES};
-    int sweep_occupancy = 1;  // resident sweep CTAs per SM at tuning.tile_x lanes
+    tpt_batch_tuning tuning{DEFAULT_TILE_X, DEFAULT_TILE_Y, 1, 0, 0, TPT_AIR_FORM_TILES};
+    int sweep_occupancy = 1;  // resident sweep CTAs per SM at sweep_lanes
     int sms = 148;
     gfft::FftSet fft;
     dft::DftSet dft;
@@ -187,7 +198,7 @@ struct tpt_batch {
         L.items = items;
         L.nitems = nitems;
         L.ninst = n;
-        L.lanes = tuning.tile_x;
+        L.lanes = sweep_lanes;
         const uint32_t per_sm = tuning.ctas_per_sm ? tuning.ctas_per_sm : (uint32_t)sweep_occupancy;
         L.grid = std::max<uint32_t>(1u, std::min<uint32_t>(nitems, (uint32_t)sms * per_sm));
         L.prepass_grid = grid();
@@ -195,16 +206,17 @@ struct tpt_batch {
         L.want = want;
         return L;
     }
-    // the tile form's persistent grid: ctas_per_sm per SM (0: six, the
-    // residency of its advection/heat pass)
+    // the tile form's persistent grid: ctas_per_sm per SM (0: as many as fit,
+    // the residency of its advection/heat pass)
     uint32_t tile_grid() const {
-        return std::min<uint32_t>(ntiles, (uint32_t)sms * (tuning.ctas_per_sm ? tuning.ctas_per_sm : 6u));
+        const uint32_t per_sm = tuning.ctas_per_sm ? tuning.ctas_per_sm : (uint32_t)tile_occupancy;
+        return std::max<uint32_t>(1u, std::min<uint32_t>(nform_tiles, (uint32_t)sms * per_sm));
     }
     bool sweep_form() const { return tuning.air_form == TPT_AIR_FORM_SWEEP; }
     const AirInst *form_insts() const { return sweep_form() ? insts : insts_tile; }
     int air_tick(uint32_t parity, cudaStream_t st) const {
         if (sweep_form()) return air::launch_sweep_tick(sweep(), parity, st);
-        return air::launch_tile_tick(insts_tile, tmaps, tiles, ntiles, tile_grid(), parity, any_noupdate_heat, st);
+        return shape->launch(insts_tile, tmaps, form_tiles, nform_tiles, tile_grid(), parity, any_noupdate_heat, st);
     }
     int grav_solve(cudaStream_t st) const {
         return precision == TPT_PRECISION_FP32 ? fft.launch(st) : dft.launch(st);
@@ -225,6 +237,7 @@ struct tpt_batch {
         cudaFree(stage);
         cudaFree(io);
         cudaFree(tiles);
+        cudaFree(form_tiles);
         cudaFree(items);
         cudaFree(ctl);
         if (side) cudaStreamDestroy(side);
@@ -362,8 +375,61 @@ static int set_sweep_shape(tpt_batch *b, uint32_t lanes, uint32_t rows) {
     b->items = d;
     b->nitems = (uint32_t)items.size();
     b->sweep_occupancy = occ;
-    b->tuning.tile_x = lanes;
-    b->tuning.tile_y = rows;
+    b->sweep_lanes = lanes;
+    b->sweep_rows = rows;
+    return TPT_OK;
+}
+
+// Builds the tile form's tile list and tensor maps for tile shape `sh` (the
+// boxes are the tile plus a 4-cell x and 3-cell y halo) and uploads them.
+static int set_tile_shape(tpt_batch *b, const air::TileShape *sh) {
+    int occ = 0;
+    int rc = sh->prepare(&occ);
+    if (rc) return rc;
+    if (occ < 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "the %ux%u tile kernels do not fit an SM", sh->tx, sh->ty);
+    std::vector<air::TileRef> tiles;
+    std::vector<CUtensorMap> tm((size_t)b->n * air::TM_COUNT);
+    for (uint32_t i = 0; i < b->n; ++i) {
+        const uint32_t X = b->descs[i].air.xcells, Y = b->descs[i].air.ycells, P = b->pitch[i];
+        CUtensorMap *m = &tm[(size_t)i * air::TM_COUNT];
+        struct Slot {
+            int slot;
+            const void *base;
+            bool f;
+        } slots[] = {
+            {air::TM_PV, b->f(F_PV, i), true},        {air::TM_VX, b->f(F_VX, i), true},
+            {air::TM_VY, b->f(F_VY, i), true},        {air::TM_OVX, b->f(F_OVX, i), true},
+            {air::TM_OVY, b->f(F_OVY, i), true},      {air::TM_OPV, b->f(F_OPV, i), true},
+            {air::TM_BA0, b->u(U_BA, i), false},      {air::TM_BA1, b->u(U_BA2, i), false},
+            {air::TM_BH0, b->u(U_BH, i), false},      {air::TM_BH1, b->u(U_BH2, i), false},
+            {air::TM_HV0, b->insts_tile_host[2 * (size_t)i].hv, true},
+            {air::TM_HV1, b->insts_tile_host[2 * (size_t)i + 1].hv, true},
+        };
+        for (const Slot &sl : slots) {
+            rc = make_grid_tmap(&m[sl.slot], sl.base, sl.f, X, Y, P, sh->tx + 8, sh->ty + 6);
+            if (rc) return rc;
+        }
+        for (uint32_t ty = 0; ty * sh->ty < Y; ++ty)
+            for (uint32_t tx = 0; tx * sh->tx < X; ++tx) tiles.push_back({i, (uint16_t)tx, (uint16_t)ty});
+    }
+    air::TileRef *dt = nullptr;
+    CUtensorMap *dm = nullptr;
+    cudaError_t e = cudaMalloc(&dt, tiles.size() * sizeof(air::TileRef));
+    if (e == cudaSuccess) e = cudaMalloc(&dm, tm.size() * sizeof(CUtensorMap));
+    if (e == cudaSuccess) e = cudaMemcpy(dt, tiles.data(), tiles.size() * sizeof(air::TileRef), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dm, tm.data(), tm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(dt);
+        cudaFree(dm);
+        TPT_FAIL(TPT_ERR_CUDA, "tile form upload failed: %s", cudaGetErrorString(e));
+    }
+    cudaFree(b->form_tiles);
+    cudaFree(b->tmaps);
+    b->form_tiles = dt;
+    b->nform_tiles = (uint32_t)tiles.size();
+    b->tmaps = dm;
+    b->shape = sh;
+    b->tile_occupancy = occ;
     return TPT_OK;
 }
 
@@ -423,7 +489,6 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     std::vector<air::TileRef> tiles;
     b->insts_host.resize(2 * (size_t)n);
     b->insts_tile_host.resize(2 * (size_t)n);
-    std::vector<CUtensorMap> tm((size_t)n * air::TM_COUNT);
     std::vector<JobShape> gshapes;
     std::vector<uint32_t> gidx;
     for (uint32_t i = 0; i < n; ++i) {
@@ -467,27 +532,6 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
             T.pv_out = T.vx_out = T.vy_out = nullptr;
             b->insts_tile_host[2 * (size_t)i + par] = T;
         }
-        // tensor maps of the grids the tile form's two passes stage (box = tile + halo)
-        CUtensorMap *m = &tm[(size_t)i * air::TM_COUNT];
-        const uint32_t X = p.xcells, Y = p.ycells, P = b->pitch[i];
-        const uint32_t BW = AIR_TX + 8, BH = AIR_TY + 6;
-        struct Slot {
-            int slot;
-            const void *base;
-            bool f;
-        } slots[] = {
-            {air::TM_PV, b->f(F_PV, i), true},        {air::TM_VX, b->f(F_VX, i), true},
-            {air::TM_VY, b->f(F_VY, i), true},        {air::TM_OVX, b->f(F_OVX, i), true},
-            {air::TM_OVY, b->f(F_OVY, i), true},      {air::TM_OPV, b->f(F_OPV, i), true},
-            {air::TM_BA0, b->u(U_BA, i), false},      {air::TM_BA1, b->u(U_BA2, i), false},
-            {air::TM_BH0, b->u(U_BH, i), false},      {air::TM_BH1, b->u(U_BH2, i), false},
-            {air::TM_HV0, b->insts_tile_host[2 * (size_t)i].hv, true},
-            {air::TM_HV1, b->insts_tile_host[2 * (size_t)i + 1].hv, true},
-        };
-        for (const Slot &sl : slots) {
-            rc = make_grid_tmap(&m[sl.slot], sl.base, sl.f, X, Y, P, BW, BH);
-            if (rc) return bail(rc);
-        }
         if (p.air_mode == 4u && p.aheat_enable) b->any_noupdate_heat = true;
         for (uint32_t ty = 0; ty * AIR_TY < p.ycells; ++ty)
             for (uint32_t tx = 0; tx * AIR_TX < p.xcells; ++tx) tiles.push_back({i, (uint16_t)tx, (uint16_t)ty});
@@ -502,8 +546,6 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
     if (e == cudaSuccess)
         e = cudaMemcpy(b->insts_tile, b->insts_tile_host.data(), b->insts_tile_host.size() * sizeof(AirInst),
                        cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMalloc(&b->tmaps, tm.size() * sizeof(CUtensorMap));
-    if (e == cudaSuccess) e = cudaMemcpy(b->tmaps, tm.data(), tm.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&b->tiles, tiles.size() * sizeof(air::TileRef));
     if (e == cudaSuccess)
         e = cudaMemcpy(b->insts, b->insts_host.data(), b->insts_host.size() * sizeof(AirInst), cudaMemcpyHostToDevice);
@@ -519,7 +561,9 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
         return bail(TPT_ERR_CUDA);
     }
     b->want = b->ctl + 1;
-    rc = set_sweep_shape(b, b->tuning.tile_x, b->tuning.tile_y);
+    rc = set_tile_shape(b, air::tile_shape(DEFAULT_TILE_X, DEFAULT_TILE_Y));
+    if (rc) return bail(rc);
+    rc = set_sweep_shape(b, DEFAULT_LANES, DEFAULT_ROWS);
     if (rc) return bail(rc);
     b->any_grav = !gshapes.empty();
     if (b->any_grav) {
@@ -691,30 +735,43 @@ int tpt_batch_get_tuning(const tpt_batch *b, tpt_batch_tuning *t) {
 
 int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
     if (!b || !t) TPT_FAIL(TPT_ERR_NULL_POINTER, "tpt_batch_set_tuning: NULL pointer");
-    if (t->tile_x < 64 || t->tile_x > (uint32_t)air::SWEEP_MAX_LANES || t->tile_x % 32u)
-        TPT_FAIL(TPT_ERR_INVALID_ARG, "tile_x (sweep lanes) %u must be a multiple of 32 in 64..%d", t->tile_x,
-                 air::SWEEP_MAX_LANES);
-    if (t->tile_y < 8 || t->tile_y > TPT_MAX_CELLS_PER_SIDE)
-        TPT_FAIL(TPT_ERR_INVALID_ARG, "tile_y (rows per strip) %u must be in 8..%u", t->tile_y,
-                 TPT_MAX_CELLS_PER_SIDE);
-    if (t->temporal_depth != 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "temporal depth %u not built", t->temporal_depth);
-    if (t->ctas_per_sm > 32) TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm must be 0 (as many as fit) .. 32");
     if (t->air_form != TPT_AIR_FORM_TILES && t->air_form != TPT_AIR_FORM_SWEEP)
         TPT_FAIL(TPT_ERR_INVALID_ARG, "air_form %u is neither TPT_AIR_FORM_TILES nor TPT_AIR_FORM_SWEEP", t->air_form);
+    const bool sweep = t->air_form == TPT_AIR_FORM_SWEEP;
+    const air::TileShape *sh = nullptr;
+    if (sweep) {
+        if (t->tile_x < 64 || t->tile_x > (uint32_t)air::SWEEP_MAX_LANES || t->tile_x % 32u)
+            TPT_FAIL(TPT_ERR_INVALID_ARG, "tile_x (sweep lanes) %u must be a multiple of 32 in 64..%d", t->tile_x,
+                     air::SWEEP_MAX_LANES);
+        if (t->tile_y < 8 || t->tile_y > TPT_MAX_CELLS_PER_SIDE)
+            TPT_FAIL(TPT_ERR_INVALID_ARG, "tile_y (rows per strip) %u must be in 8..%u", t->tile_y,
+                     TPT_MAX_CELLS_PER_SIDE);
+    } else {
+        sh = air::tile_shape(t->tile_x, t->tile_y);
+        if (!sh)
+            TPT_FAIL(TPT_ERR_INVALID_ARG, "tile %ux%u is not a tile form shape (32x8, 64x8, 32x16, 64x16)", t->tile_x,
+                     t->tile_y);
+    }
+    if (t->temporal_depth != 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "temporal depth %u not built", t->temporal_depth);
+    if (t->ctas_per_sm > 32) TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm must be 0 (as many as fit) .. 32");
     const bool split = b->any_grav && b->precision == TPT_PRECISION_SPLIT_BF16 && b->dft.can_split();
     if (t->grav_side_ctas && !split)
         TPT_FAIL(TPT_ERR_INVALID_ARG, "grav_side_ctas must be 0: the batch's gravity has one kind of y stage");
+    if (sweep && (t->tile_x != b->sweep_lanes || t->tile_y != b->sweep_rows)) {
+        int rc = set_sweep_shape(b, t->tile_x, t->tile_y);
+        if (rc) return rc;
+    }
+    if (sweep && t->ctas_per_sm > (uint32_t)b->sweep_occupancy)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm %u exceeds the %d sweep CTAs of %u lanes that fit an SM",
+                 t->ctas_per_sm, b->sweep_occupancy, t->tile_x);
+    if (!sweep && sh != b->shape) {
+        int rc = set_tile_shape(b, sh);
+        if (rc) return rc;
+    }
     if (split) {
         int rc = b->dft.set_side_ctas(t->grav_side_ctas);
         if (rc) return rc;
     }
-    if (t->tile_x != b->tuning.tile_x || t->tile_y != b->tuning.tile_y) {
-        int rc = set_sweep_shape(b, t->tile_x, t->tile_y);
-        if (rc) return rc;
-    }
-    if (t->air_form == TPT_AIR_FORM_SWEEP && t->ctas_per_sm > (uint32_t)b->sweep_occupancy)
-        TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm %u exceeds the %d sweep CTAs of %u lanes that fit an SM",
-                 t->ctas_per_sm, b->sweep_occupancy, t->tile_x);
     b->drop_graphs();
     b->tuning = *t;
     return TPT_OK;
@@ -803,27 +860,40 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
     StateCopy saved;
     int src = saved.save(b, st);
     if (src) return src;
+    // Phase 1: the air form and its layout, by timing 20 air ticks of each
+    // candidate: the tile form at every tile shape (32x8 at 2..8 CTAs per SM,
+    // the larger tiles at as many CTAs as fit and one fewer), the sweep form at
+    // a few shapes (lanes per CTA x rows per strip) with as many CTAs as fit.
+    struct Cand {
+        uint32_t form, x, y, per_sm;
+    };
+    std::vector<Cand> cands;
+    for (int k = 0; k < air::TILE_SHAPES; ++k) {
+        const air::TileShape *sh = air::tile_shapes()[k];
+        if (sh->tx == DEFAULT_TILE_X && sh->ty == DEFAULT_TILE_Y) {
+            for (uint32_t c : {2u, 3u, 4u, 6u, 8u}) cands.push_back({TPT_AIR_FORM_TILES, sh->tx, sh->ty, c});
+            continue;
+        }
+        int occ = 0;
+        int prc = sh->prepare(&occ);
+        if (prc) return prc;
+        if (occ < 1) continue;
+        cands.push_back({TPT_AIR_FORM_TILES, sh->tx, sh->ty, (uint32_t)occ});
+        if (occ > 1) cands.push_back({TPT_AIR_FORM_TILES, sh->tx, sh->ty, (uint32_t)occ - 1u});
+    }
+    for (auto sh : {std::make_pair(224u, 64u), std::make_pair(256u, 64u), std::make_pair(256u, 32u)})
+        cands.push_back({TPT_AIR_FORM_SWEEP, sh.first, sh.second, 0u});
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    // Phase 1: the air form and its layout, by timing 20 air ticks of each
-    // candidate: the tile form at 2..8 CTAs per SM, the sweep form at a few
-    // shapes (lanes per CTA x rows per strip) with as many CTAs as fit.
-    struct Cand {
-        uint32_t form, lanes, rows, per_sm;
-    };
-    std::vector<Cand> cands;
-    for (uint32_t c : {2u, 3u, 4u, 6u, 8u}) cands.push_back({TPT_AIR_FORM_TILES, b->tuning.tile_x, b->tuning.tile_y, c});
-    for (auto sh : {std::make_pair(224u, 64u), std::make_pair(256u, 64u), std::make_pair(256u, 32u)})
-        cands.push_back({TPT_AIR_FORM_SWEEP, sh.first, sh.second, 0u});
     tpt_batch_tuning best = b->tuning;
     float best_ms = 1e30f;
     int rc = TPT_OK;
     for (const Cand &cd : cands) {
         tpt_batch_tuning t = b->tuning;
         t.air_form = cd.form;
-        t.tile_x = cd.lanes;
-        t.tile_y = cd.rows;
+        t.tile_x = cd.x;
+        t.tile_y = cd.y;
         t.ctas_per_sm = cd.per_sm;
         rc = tpt_batch_set_tuning(b, &t);
         if (rc) break;

@@ -128,6 +128,8 @@ class BatchTuning(ctypes.Structure):
 
 
 AIR_FORM_TILES, AIR_FORM_SWEEP = 0, 1
+# (tile_x, tile_y) of the tile form's shapes, the default first
+TILE_SHAPES = ((32, 8), (64, 8), (32, 16), (64, 16))
 
 
 _lib = None
