@@ -272,6 +272,29 @@ def run_plain(ticks: int):
     return inst.cells * ticks / (ms / 1e3), ms / ticks
 
 
+def air_launches(ticks, tuning, per_tick, chunk=50):
+    """Air launches of `ticks` ticks stepped in graphs of `chunk` ticks.
+    `per_tick` is the profile's unblocked count (2, or 3 with a NoUpdate +
+    heat instance in the tile form); the tile form at temporal depth k runs
+    each block of n <= k ticks (cut at the chunk's end) as n + 1 launches,
+    plus one settle launch per tick with a NoUpdate + heat instance."""
+    import tpt_field as tf
+
+    k = tuning.temporal_depth if tuning.air_form == tf.AIR_FORM_TILES else 1
+    if k <= 1:
+        return per_tick * ticks
+    total, left = 0, ticks
+    while left:
+        c = min(chunk, left)
+        left -= c
+        t = 0
+        while t < c:
+            n = min(k, c - t)
+            total += n + 1 + (per_tick - 2) * n
+            t += n
+    return total
+
+
 def run_ours(args, rank, world, local):
     import torch
 
@@ -299,6 +322,7 @@ def run_ours(args, rank, world, local):
         t.air_form = tf.AIR_FORM_SWEEP if args.air_form == "sweep" else tf.AIR_FORM_TILES
         t.tile_x, t.tile_y = args.air_shape or ((224, 64) if args.air_form == "sweep" else tf.TILE_SHAPES[0])
         t.ctas_per_sm = 0
+        t.temporal_depth = args.temporal_depth
         batch.set_tuning(t)
     cells = sum(i.cells for i in insts)
     # cells all ranks advance per tick: every rank has a full copy (weak) or
@@ -365,7 +389,8 @@ def run_ours(args, rank, world, local):
     prof = batch.profile_phases(args.phase_ticks)
     hbm, bf16, bf16s, peak_src = load_peaks()
     air_gbs = prof.cells * prof.ticks * B_AIR / (prof.air_ms / 1e3) / 1e9
-    air_launch_ms = prof.air_ms / (prof.ticks * prof.air_launches_per_tick)
+    tuning = batch.tuning()
+    air_launch_ms = prof.air_ms / air_launches(prof.ticks, tuning, prof.air_launches_per_tick, chunk=prof.ticks)
     roof_air = {"kernel": "air tick (pressure+velocity, advection+heat+masks)", "bound": "hbm",
                 "achieved": round(air_gbs, 1), "peak": hbm, "unit": "GB/s", "frac": round(air_gbs / hbm, 4),
                 "peak_source": peak_src, "algorithmic_bytes_per_cell_tick": B_AIR,
@@ -383,8 +408,8 @@ def run_ours(args, rank, world, local):
     else:
         roof_grav = None
     dominant = roof_grav if (roof_grav and prof.grav_ms > prof.air_ms) else roof_air
-    launches = (prof.air_launches_per_tick + prof.grav_launches_per_tick) * ticks * args.steps + \
-        (args.steps if ticks % 2 else 0)
+    launches = (air_launches(ticks, tuning, prof.air_launches_per_tick) + prof.grav_launches_per_tick * ticks) * \
+        args.steps + (args.steps if ticks % 2 else 0)
 
     plain = None
     if rank == 0 and world == 1 and args.plain_ticks > 0:
@@ -749,6 +774,8 @@ def main():
                     help="air tick form of the batched workloads (default: the autotuner's choice)")
     ap.add_argument("--air-shape", type=lambda v: tuple(int(x) for x in v.split("x")), default=None,
                     help="with --air-form: tile (tiles) or lanes x rows (sweep), e.g. 64x16")
+    ap.add_argument("--temporal-depth", type=int, default=1,
+                    help="with --air-form tiles: ticks per temporally blocked run (1 = none)")
     ap.add_argument("--skip-tune", action="store_true", help="keep the batch's default tuning (profiling captures)")
     ap.add_argument("--instances", type=int, default=0,
                     help="only the first N instances of the workload (profiling captures on a smaller case)")

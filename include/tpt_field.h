@@ -367,7 +367,13 @@ typedef struct tpt_batch_tuning {
      * side), and strips of narrow instances are packed side by side into one
      * CTA. */
     uint32_t tile_x, tile_y;
-    uint32_t temporal_depth;  /* ticks per air launch (1 = no blocking)   */
+    /* Temporal blocking of the tile form: ticks per block (1..50; 1 = none).
+     * A block of k ticks is k + 1 launches: the first tick's velocity pass,
+     * k - 1 launches that each finish one tick and start the next over 32x16
+     * tiles (the velocity pass of tick t + 1 reads tick t's state from
+     * shared memory), and the last tick's advection pass. The sweep form
+     * takes 1. */
+    uint32_t temporal_depth;
     /* Resident CTAs per SM of the air form's persistent launches (0 = as
      * many as fit). */
     uint32_t ctas_per_sm;
@@ -400,7 +406,8 @@ int tpt_batch_fields(tpt_batch *batch, uint32_t instance,
 int tpt_batch_step(tpt_batch *batch, uint32_t ticks, tpt_stream_t stream);
 /* Times candidate tunings on the batch's own data (state is saved and
  * restored) and keeps the fastest: the air form with its shape (tile_x x
- * tile_y) and CTAs per SM, then the gravity branch split. The choice is cached in
+ * tile_y) and CTAs per SM, the temporal depth (tile form), then the gravity
+ * branch split. The choice is cached in
  * the process per batch composition -- the instances' (xcells, ycells)
  * buckets (powers of two) with their counts, and the gravity precision -- so
  * tuning a batch of the same composition again only applies the cached
@@ -414,6 +421,9 @@ typedef struct tpt_batch_profile {
     float air_ms;              /* `ticks` air ticks alone (all instances)  */
     float grav_ms;             /* `ticks` gravity solves alone             */
     uint32_t ticks;
+    /* Air launches per tick without temporal blocking: 2 (3 in the tile
+     * form with a NoUpdate + heat instance: its settle). At temporal depth
+     * k, a block of n <= k ticks makes n + 1 launches (plus the n settles). */
     uint32_t air_launches_per_tick;
     uint32_t grav_launches_per_tick;
     uint64_t cells;            /* sum of xcells*ycells over instances      */

@@ -40,11 +40,13 @@ def check_against_oracle(tf, oracle, batch, insts, ticks, ctx):
 
 def set_form(tf, b, form, **kw):
     """Switches the batch's air form; tile_x / tile_y default to the form's
-    default shape (32x8 tiles, 224-lane x 64-row sweeps), ctas_per_sm to 0."""
+    default shape (32x8 tiles, 224-lane x 64-row sweeps), ctas_per_sm to 0,
+    temporal_depth to 1."""
     t = b.tuning()
     t.air_form = form
     t.tile_x, t.tile_y = (224, 64) if form == tf.AIR_FORM_SWEEP else tf.TILE_SHAPES[0]
     t.ctas_per_sm = 0
+    t.temporal_depth = 1
     for k, v in kw.items():
         setattr(t, k, v)
     b.set_tuning(t)
@@ -78,11 +80,12 @@ def test_tune_keeps_state_and_results(cuda, tf, oracle):
     b = tf.Batch(insts)
     b.tune()
     t = b.tuning()
-    assert t.air_form in (tf.AIR_FORM_TILES, tf.AIR_FORM_SWEEP) and t.temporal_depth == 1
+    assert t.air_form in (tf.AIR_FORM_TILES, tf.AIR_FORM_SWEEP)
     if t.air_form == tf.AIR_FORM_TILES:
         assert (t.tile_x, t.tile_y) in tf.TILE_SHAPES and 1 <= t.ctas_per_sm <= 8
+        assert t.temporal_depth in (1, 2, 4, 10, 20)
     else:
-        assert (t.tile_x, t.tile_y) in ((224, 64), (256, 64), (256, 32))
+        assert (t.tile_x, t.tile_y) in ((224, 64), (256, 64), (256, 32)) and t.temporal_depth == 1
     b.step(5)
     cuda.cuda.synchronize()
     check_against_oracle(tf, oracle, b, insts, 5, "tuned")
@@ -127,6 +130,40 @@ def test_every_tile_shape_gives_the_same_fields(cuda, tf, oracle, shape, per_sm)
     b.close()
 
 
+@pytest.mark.parametrize("depth", [2, 3, 5, 50])
+@pytest.mark.parametrize("ticks", [1, 2, 7, 57])
+def test_temporal_blocking_is_bit_exact(cuda, tf, oracle, depth, ticks):
+    """Temporal blocking: blocks of `depth` ticks as A, (depth - 1) fused
+    B(t) + A(t + 1) launches and B, with the emap decays deferred to the
+    block's last launch (the stress instances' electrified walls decay over
+    three ticks), NoUpdate and no-heat instances, blocks cut short by the
+    step's tick count and by the 50-tick graph chunks: bit-exact after every
+    step length."""
+    insts = mixed_instances()
+    b = tf.Batch(insts)
+    set_form(tf, b, tf.AIR_FORM_TILES, temporal_depth=depth)
+    b.step(ticks)
+    cuda.cuda.synchronize()
+    assert tf.lib().tpt_check_device_errors() == 0
+    check_against_oracle(tf, oracle, b, insts, ticks, f"depth {depth}, {ticks} ticks")
+    b.close()
+
+
+@pytest.mark.parametrize("shape", [(64, 8), (64, 16)])
+def test_temporal_blocking_with_other_tile_shapes(cuda, tf, oracle, shape):
+    """The block's first and last launches at another tile shape than the
+    fused launches' 32x16."""
+    insts = mixed_instances()
+    b = tf.Batch(insts)
+    set_form(tf, b, tf.AIR_FORM_TILES, tile_x=shape[0], tile_y=shape[1], temporal_depth=4)
+    for ticks in (3, 6):
+        b.step(ticks)
+    cuda.cuda.synchronize()
+    assert tf.lib().tpt_check_device_errors() == 0
+    check_against_oracle(tf, oracle, b, insts, 9, f"depth 4 at {shape[0]}x{shape[1]}")
+    b.close()
+
+
 @pytest.mark.parametrize("per_sm", [1, 3, 6, 8])
 def test_tile_form_at_every_grid_size(cuda, tf, oracle, per_sm):
     insts = mixed_instances()
@@ -165,7 +202,10 @@ def test_bad_tunings_are_rejected(cuda, tf):
         dict(air_form=sweep, tile_x=100, tile_y=64), dict(air_form=sweep, tile_x=32, tile_y=64),
         dict(air_form=sweep, tile_x=288, tile_y=64), dict(air_form=sweep, tile_x=224, tile_y=4),
         dict(air_form=sweep, tile_x=224, tile_y=64, ctas_per_sm=9),
-        dict(temporal_depth=2), dict(air_form=2),
+        # temporal depth 1..50, tile form only
+        dict(temporal_depth=0), dict(temporal_depth=51),
+        dict(air_form=sweep, tile_x=224, tile_y=64, temporal_depth=2),
+        dict(air_form=2),
     ):
         t = b.tuning()
         for k, v in kw.items():
@@ -205,13 +245,14 @@ def test_nonfinite_inputs_in_a_batch(cuda, tf, oracle):
     from test_oracle_air_numpy import nonfinite_instance
 
     insts = [nonfinite_instance(), nonfinite_instance(70, 50, 32)]
-    for form in (tf.AIR_FORM_TILES, tf.AIR_FORM_SWEEP):
+    for form, depth in ((tf.AIR_FORM_TILES, 1), (tf.AIR_FORM_TILES, 3), (tf.AIR_FORM_SWEEP, 1)):
         b = tf.Batch(insts)
-        set_form(tf, b, form)
+        set_form(tf, b, form, temporal_depth=depth)
         b.step(3)
         cuda.cuda.synchronize()
         for i, inst in enumerate(insts):
-            assert_bit_exact(b.state(i), oracle.air_steps(inst, 3), f"form {form} non-finite {i}", nan_equal=True)
+            assert_bit_exact(b.state(i), oracle.air_steps(inst, 3), f"form {form} depth {depth} non-finite {i}",
+                             nan_equal=True)
         b.close()
 
 
@@ -226,8 +267,9 @@ def test_batch_measured_config_subset(cuda, tf, oracle):
     b.close()
 
 
-@pytest.mark.parametrize("form,shape", [(0, (32, 8)), (0, (64, 8)), (0, (32, 16)), (1, (224, 64))])
-def test_c4_every_instance_20_ticks(cuda, tf, oracle, form, shape):
+@pytest.mark.parametrize("form,shape,depth", [(0, (32, 8), 1), (0, (64, 8), 1), (0, (32, 16), 1), (0, (32, 8), 4),
+                                              (1, (224, 64), 1)])
+def test_c4_every_instance_20_ticks(cuda, tf, oracle, form, shape, depth):
     """The whole C4 batch (256 instances, W, H log-uniform 32..512, FP32
     gravity) after 20 ticks: every instance's air bit-exact against the
     oracle and its gx/gy within 1e-5 of max|g| against FP64."""
@@ -236,11 +278,11 @@ def test_c4_every_instance_20_ticks(cuda, tf, oracle, form, shape):
     insts = W.config_instances(4)
     assert len(insts) == 256
     b = tf.Batch(insts)
-    set_form(tf, b, form, tile_x=shape[0], tile_y=shape[1])
+    set_form(tf, b, form, tile_x=shape[0], tile_y=shape[1], temporal_depth=depth)
     b.step(20)
     cuda.cuda.synchronize()
     assert tf.lib().tpt_check_device_errors() == 0
-    check_against_oracle(tf, oracle, b, insts, 20, f"C4 form {form} {shape[0]}x{shape[1]}")
+    check_against_oracle(tf, oracle, b, insts, 20, f"C4 form {form} {shape[0]}x{shape[1]} depth {depth}")
     b.close()
 
 

@@ -691,10 +691,22 @@ __device__ __forceinline__ void masks_of(uint32_t wall, uint32_t raw, uint32_t e
     bairh = heat | eairh;
 }
 
-// The same for cell g of an instance, decaying its emap in place.
-__device__ __forceinline__ void masks_cell(const AirInst &I, size_t g, uint32_t &bair, uint32_t &bairh) {
-    const uint32_t raw = I.emap[g];
-    if (raw != 0u) I.emap[g] = raw - 1u;
+// The emap value a tick's mask rebuild sees at cell g when the stored value
+// still lacks `lag` decays: inside a temporally blocked run of ticks the
+// rebuilds read emap without writing it, and the last one writes it (the
+// decay saturates at 0, so `lag` decays subtract lag, down to 0).
+__device__ __forceinline__ uint32_t emap_seen(uint32_t stored, uint32_t lag) {
+    return stored > lag ? stored - lag : 0u;
+}
+
+// The same for cell g of an instance, decaying its emap in place (after the
+// `lag` decays it still lacks).
+__device__ __forceinline__ void masks_cell(const AirInst &I, size_t g, uint32_t &bair, uint32_t &bairh,
+                                           uint32_t lag = 0u) {
+    const uint32_t stored = I.emap[g];
+    const uint32_t raw = emap_seen(stored, lag);
+    const uint32_t next = raw != 0u ? raw - 1u : 0u;
+    if (next != stored) I.emap[g] = next;
     masks_of(__ldg(I.wall + g), raw, I.eair ? __ldg(I.eair + g) : 0u, I.eairh ? __ldg(I.eairh + g) : 0u, bair, bairh);
 }
 

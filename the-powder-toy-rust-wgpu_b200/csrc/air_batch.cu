@@ -99,10 +99,13 @@ const TileShape *tile_shape(uint32_t tx, uint32_t ty) {
     return nullptr;
 }
 
-// The batched air kernels' error words: the tile form's, one per shape (the
-// sweep form and the pre-pass have no waits).
+// The batched air kernels' error words: the tile form's, one per shape, and
+// the temporally blocked launches' (the sweep form and the pre-pass have no
+// waits).
 int read_errors(uint32_t *out) {
     uint32_t all = 0;
+    int frc = read_fused_errors(&all);
+    if (frc) return frc;
     for (int k = 0; k < TILE_SHAPES; ++k) {
         uint32_t v = 0;
         int rc = tile_shapes()[k]->read_errors(&v);

@@ -18,8 +18,14 @@ struct TileRef {
 // ---- the tile form (air_tiles.cu) ---------------------------------------------
 // Tensor maps of one batched instance: the grids the two passes stage, with
 // the two halves of the heat and mask ping-pong.
+// The velocity pass's outputs (ovx, ovy, opv) alternate between two sets by
+// tick parity, so a launch that ends one tick and starts the next (the
+// temporally blocked form) reads one set while it writes the other.
 enum TensorMapSlot {
-    TM_PV, TM_VX, TM_VY, TM_OVX, TM_OVY, TM_OPV, TM_BA0, TM_BA1, TM_BH0, TM_BH1, TM_HV0, TM_HV1, TM_COUNT
+    TM_PV, TM_VX, TM_VY,
+    TM_OV0, TM_OVX0 = TM_OV0, TM_OVY0, TM_OPV0,
+    TM_OV1, TM_OVX1 = TM_OV1, TM_OVY1, TM_OPV1,
+    TM_BA0, TM_BA1, TM_BH0, TM_BH1, TM_HV0, TM_HV1, TM_COUNT
 };
 
 // One tile shape of the tile form (air_tiles.cu, compiled once per shape).
@@ -36,6 +42,16 @@ struct TileShape {
     // place); `tmaps` TM_COUNT tensor maps per instance.
     int (*launch)(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
                   uint32_t parity, bool any_noupdate_heat, cudaStream_t st);
+    // the passes of one tick separately: the velocity pass (pass A), and the
+    // advection / heat / mask pass (pass B, with its NoUpdate settle) whose
+    // mask rebuild applies `emap_lag` pending emap decays
+    int (*launch_a)(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles,
+                    uint32_t grid, uint32_t parity, cudaStream_t st);
+    int (*launch_b)(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles,
+                    uint32_t grid, uint32_t parity, uint32_t emap_lag, bool any_noupdate_heat, cudaStream_t st);
+    // the copy-back of NoUpdate instances' convected velocity after a pass B
+    int (*launch_settle)(const AirInst *insts, const TileRef *tiles, uint32_t ntiles, uint32_t grid, uint32_t parity,
+                         cudaStream_t st);
     // reads and clears the shape's device error word
     int (*read_errors)(uint32_t *out);
 };
@@ -44,6 +60,19 @@ constexpr int TILE_SHAPES = 4;
 // The offered shapes, 32x8 first; tile_shape(tx, ty) is null for any other.
 const TileShape *const *tile_shapes();
 const TileShape *tile_shape(uint32_t tx, uint32_t ty);
+
+// ---- temporal blocking of the tile form (air_fused.cu) ----------------------------
+// k ticks as A(t0), then k - 1 launches of B(t) + A(t + 1) over FUSED_TX x
+// FUSED_TY tiles (each staged as one TMA box of (FUSED_TX + 16) x (FUSED_TY +
+// 10) cells: its own tensor maps), then B(t0 + k - 1) with the k - 1 deferred
+// emap decays.
+constexpr int FUSED_TX = 32, FUSED_TY = 16;
+int fused_tile_prepare(int *occupancy);
+// B(t) + A(t + 1) of every instance: tick t reads parity `parity` of `insts`
+// (two per instance, as the tile form's), `emap_lag` emap decays are pending.
+int launch_fused_ba(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles,
+                    uint32_t grid, uint32_t parity, uint32_t emap_lag, cudaStream_t st);
+int read_fused_errors(uint32_t *out);
 
 // ---- the sweep form (air_sweep.cu) ----------------------------------------------
 // Lanes of halo on each side of a segment: the tick's stencil reaches six

@@ -143,9 +143,10 @@ __device__ __forceinline__ void issue_b(const AirInst &I, const CUtensorMap *m, 
     const uint32_t n = b_loads(I);
     tc::mbar_arrive_expect_tx(bar, n * BOX_BYTES);
     if (I.air_mode != 4u) {
-        load_box(buf->ovx, m + TM_OVX, x0, y0, bar);
-        load_box(buf->ovy, m + TM_OVY, x0, y0, bar);
-        load_box(buf->opv, m + TM_OPV, x0, y0, bar);
+        const CUtensorMap *ov = m + TM_OV0 + 3 * parity;  // this tick's velocity-pass outputs
+        load_box(buf->ovx, ov + 0, x0, y0, bar);
+        load_box(buf->ovy, ov + 1, x0, y0, bar);
+        load_box(buf->opv, ov + 2, x0, y0, bar);
         load_box(buf->b, m + TM_BA0 + parity, x0, y0, bar);
     } else {  // NoUpdate: the heat pass reads the stored velocity
         load_box(buf->ovx, m + TM_VX, x0, y0, bar);
@@ -168,7 +169,7 @@ __device__ __forceinline__ void issue_b(const AirInst &I, const CUtensorMap *m, 
 __global__ void __launch_bounds__(NT, B_MIN_CTAS) kb_advect_heat(const AirInst *__restrict__ insts,
                                                               const CUtensorMap *__restrict__ tmaps,
                                                               const TileRef *__restrict__ tiles, uint32_t ntiles,
-                                                              uint32_t parity) {
+                                                              uint32_t parity, uint32_t emap_lag) {
     BoxB *buf = reinterpret_cast<BoxB *>(air_tile_smem);
     WorkB2 *work = reinterpret_cast<WorkB2 *>(buf + 2);
     __shared__ uint64_t full[2];
@@ -222,7 +223,7 @@ __global__ void __launch_bounds__(NT, B_MIN_CTAS) kb_advect_heat(const AirInst *
         if (in_grid(gx, gy, I)) {
             size_t g = (size_t)gy * I.pitch + gx;
             uint32_t ba, bh;
-            masks_cell(I, g, ba, bh);
+            masks_cell(I, g, ba, bh, emap_lag);
             I.bair_out[g] = ba;
             I.bairh_out[g] = bh;
         }
@@ -269,18 +270,34 @@ int tile_prepare(int *occupancy) {
     return TPT_OK;
 }
 
-int tile_launch(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
-                uint32_t parity, bool any_noupdate_heat, cudaStream_t st) {
+int tile_launch_a(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
+                  uint32_t parity, cudaStream_t st) {
     using namespace AIR_SHAPE_NS;
     kb_pressure_velocity<<<grid, NT, SMEM_A, st>>>(insts, tmaps, tiles, ntiles, parity);
     TPT_LAUNCHED();
-    kb_advect_heat<<<grid, NT, SMEM_B, st>>>(insts, tmaps, tiles, ntiles, parity);
-    TPT_LAUNCHED();
-    if (any_noupdate_heat) {
-        kb_noupdate_settle<<<grid, NT, 0, st>>>(insts, tiles, ntiles, parity);
-        TPT_LAUNCHED();
-    }
     return TPT_OK;
+}
+
+int tile_launch_settle(const AirInst *insts, const TileRef *tiles, uint32_t ntiles, uint32_t grid, uint32_t parity,
+                       cudaStream_t st) {
+    using namespace AIR_SHAPE_NS;
+    kb_noupdate_settle<<<grid, NT, 0, st>>>(insts, tiles, ntiles, parity);
+    TPT_LAUNCHED();
+    return TPT_OK;
+}
+
+int tile_launch_b(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
+                  uint32_t parity, uint32_t emap_lag, bool any_noupdate_heat, cudaStream_t st) {
+    using namespace AIR_SHAPE_NS;
+    kb_advect_heat<<<grid, NT, SMEM_B, st>>>(insts, tmaps, tiles, ntiles, parity, emap_lag);
+    TPT_LAUNCHED();
+    return any_noupdate_heat ? tile_launch_settle(insts, tiles, ntiles, grid, parity, st) : TPT_OK;
+}
+
+int tile_launch(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
+                uint32_t parity, bool any_noupdate_heat, cudaStream_t st) {
+    int rc = tile_launch_a(insts, tmaps, tiles, ntiles, grid, parity, st);
+    return rc ? rc : tile_launch_b(insts, tmaps, tiles, ntiles, grid, parity, 0u, any_noupdate_heat, st);
 }
 
 int tile_read_errors(uint32_t *out) {
@@ -297,7 +314,8 @@ int tile_read_errors(uint32_t *out) {
 #define AIR_CAT2(a, b) a##b
 #define AIR_CAT(a, b) AIR_CAT2(a, b)
 extern const TileShape AIR_CAT(tile_shape_, AIR_SHAPE_NS) = {(uint32_t)AIR_SHAPE_NS::TX, (uint32_t)AIR_SHAPE_NS::TY,
-                                                            tile_prepare, tile_launch, tile_read_errors};
+                                                            tile_prepare, tile_launch, tile_launch_a,
+                                                            tile_launch_b, tile_launch_settle, tile_read_errors};
 
 }  // namespace air
 }  // namespace tpt

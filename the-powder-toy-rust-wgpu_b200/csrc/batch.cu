@@ -163,6 +163,12 @@ struct tpt_batch {
     uint32_t nform_tiles = 0;
     CUtensorMap *tmaps = nullptr;
     int tile_occupancy = 1;
+    // temporal blocking (tuning.temporal_depth > 1): the B(t) + A(t + 1)
+    // launches' tiles and tensor maps (their own box), built on first use
+    air::TileRef *fused_tiles = nullptr;
+    uint32_t nfused_tiles = 0;
+    CUtensorMap *tmaps_fused = nullptr;
+    int fused_occupancy = 0;
     // the sweep form of the air tick: work items (device), the queue counter
     // and the pre-pass flags ([2][n], zeroed at creation)
     air::SweepItem *items = nullptr;
@@ -214,9 +220,35 @@ struct tpt_batch {
     }
     bool sweep_form() const { return tuning.air_form == TPT_AIR_FORM_SWEEP; }
     const AirInst *form_insts() const { return sweep_form() ? insts : insts_tile; }
-    int air_tick(uint32_t parity, cudaStream_t st) const {
-        if (sweep_form()) return air::launch_sweep_tick(sweep(), parity, st);
-        return shape->launch(insts_tile, tmaps, form_tiles, nform_tiles, tile_grid(), parity, any_noupdate_heat, st);
+    uint32_t fused_grid() const {
+        return std::max<uint32_t>(1u, std::min<uint32_t>(nfused_tiles, (uint32_t)sms * (uint32_t)fused_occupancy));
+    }
+    // `ticks` air ticks from the canonical state (tick 0 reads parity 0). The
+    // tile form at temporal depth k runs blocks of k ticks as A(t0), k - 1
+    // launches of B(t) + A(t + 1), and B(t0 + k - 1) with the block's
+    // deferred emap decays; depth 1 is A, B per tick.
+    int air_run(uint32_t ticks, cudaStream_t st) const {
+        int rc = TPT_OK;
+        if (sweep_form()) {
+            for (uint32_t t = 0; t < ticks && rc == TPT_OK; ++t) rc = air::launch_sweep_tick(sweep(), t & 1u, st);
+            return rc;
+        }
+        const uint32_t k = std::max<uint32_t>(1u, tuning.temporal_depth);
+        for (uint32_t t = 0; t < ticks && rc == TPT_OK;) {
+            const uint32_t n = std::min<uint32_t>(k, ticks - t);
+            rc = shape->launch_a(insts_tile, tmaps, form_tiles, nform_tiles, tile_grid(), t & 1u, st);
+            for (uint32_t j = 0; j + 1 < n && rc == TPT_OK; ++j) {
+                const uint32_t p = (t + j) & 1u;
+                rc = air::launch_fused_ba(insts_tile, tmaps_fused, fused_tiles, nfused_tiles, fused_grid(), p, j, st);
+                if (rc == TPT_OK && any_noupdate_heat)
+                    rc = shape->launch_settle(insts_tile, form_tiles, nform_tiles, tile_grid(), p, st);
+            }
+            if (rc == TPT_OK)
+                rc = shape->launch_b(insts_tile, tmaps, form_tiles, nform_tiles, tile_grid(), (t + n - 1) & 1u, n - 1,
+                                     any_noupdate_heat, st);
+            t += n;
+        }
+        return rc;
     }
     int grav_solve(cudaStream_t st) const {
         return precision == TPT_PRECISION_FP32 ? fft.launch(st) : dft.launch(st);
@@ -238,6 +270,8 @@ struct tpt_batch {
         cudaFree(io);
         cudaFree(tiles);
         cudaFree(form_tiles);
+        cudaFree(fused_tiles);
+        cudaFree(tmaps_fused);
         cudaFree(items);
         cudaFree(ctl);
         if (side) cudaStreamDestroy(side);
@@ -258,10 +292,8 @@ static int record_ticks(tpt_batch *b, uint32_t ticks, cudaStream_t st) {
             if (rc) return rc;
         }
     }
-    for (uint32_t t = 0; t < ticks; ++t) {
-        rc = b->air_tick(t & 1u, st);
-        if (rc) return rc;
-    }
+    rc = b->air_run(ticks, st);
+    if (rc) return rc;
     if (ticks & 1u) {
         rc = air::launch_copy_back(b->form_insts(), b->tiles, b->ntiles, b->grid(), st);
         if (rc) return rc;
@@ -380,15 +412,13 @@ static int set_sweep_shape(tpt_batch *b, uint32_t lanes, uint32_t rows) {
     return TPT_OK;
 }
 
-// Builds the tile form's tile list and tensor maps for tile shape `sh` (the
-// boxes are the tile plus a 4-cell x and 3-cell y halo) and uploads them.
-static int set_tile_shape(tpt_batch *b, const air::TileShape *sh) {
-    int occ = 0;
-    int rc = sh->prepare(&occ);
-    if (rc) return rc;
-    if (occ < 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "the %ux%u tile kernels do not fit an SM", sh->tx, sh->ty);
-    std::vector<air::TileRef> tiles;
-    std::vector<CUtensorMap> tm((size_t)b->n * air::TM_COUNT);
+// Tensor maps of every instance's grids that the tile form's launches stage,
+// with boxes of box_w x box_h cells (TM_COUNT per instance), and the tile list
+// of tiles tx x ty.
+static int build_tile_maps(const tpt_batch *b, uint32_t tx, uint32_t ty, uint32_t box_w, uint32_t box_h,
+                           std::vector<CUtensorMap> &tm, std::vector<air::TileRef> &tiles) {
+    tm.assign((size_t)b->n * air::TM_COUNT, CUtensorMap{});
+    tiles.clear();
     for (uint32_t i = 0; i < b->n; ++i) {
         const uint32_t X = b->descs[i].air.xcells, Y = b->descs[i].air.ycells, P = b->pitch[i];
         CUtensorMap *m = &tm[(size_t)i * air::TM_COUNT];
@@ -397,21 +427,29 @@ static int set_tile_shape(tpt_batch *b, const air::TileShape *sh) {
             const void *base;
             bool f;
         } slots[] = {
-            {air::TM_PV, b->f(F_PV, i), true},        {air::TM_VX, b->f(F_VX, i), true},
-            {air::TM_VY, b->f(F_VY, i), true},        {air::TM_OVX, b->f(F_OVX, i), true},
-            {air::TM_OVY, b->f(F_OVY, i), true},      {air::TM_OPV, b->f(F_OPV, i), true},
-            {air::TM_BA0, b->u(U_BA, i), false},      {air::TM_BA1, b->u(U_BA2, i), false},
-            {air::TM_BH0, b->u(U_BH, i), false},      {air::TM_BH1, b->u(U_BH2, i), false},
-            {air::TM_HV0, b->insts_tile_host[2 * (size_t)i].hv, true},
+            {air::TM_PV, b->f(F_PV, i), true},         {air::TM_VX, b->f(F_VX, i), true},
+            {air::TM_VY, b->f(F_VY, i), true},         {air::TM_OVX0, b->f(F_OVX, i), true},
+            {air::TM_OVY0, b->f(F_OVY, i), true},      {air::TM_OPV0, b->f(F_OPV, i), true},
+            {air::TM_OVX1, b->f(F_VX2, i), true},      {air::TM_OVY1, b->f(F_VY2, i), true},
+            {air::TM_OPV1, b->f(F_PV2, i), true},      {air::TM_BA0, b->u(U_BA, i), false},
+            {air::TM_BA1, b->u(U_BA2, i), false},      {air::TM_BH0, b->u(U_BH, i), false},
+            {air::TM_BH1, b->u(U_BH2, i), false},      {air::TM_HV0, b->insts_tile_host[2 * (size_t)i].hv, true},
             {air::TM_HV1, b->insts_tile_host[2 * (size_t)i + 1].hv, true},
         };
+        static_assert(sizeof(slots) / sizeof(slots[0]) == air::TM_COUNT, "every slot");
         for (const Slot &sl : slots) {
-            rc = make_grid_tmap(&m[sl.slot], sl.base, sl.f, X, Y, P, sh->tx + 8, sh->ty + 6);
+            int rc = make_grid_tmap(&m[sl.slot], sl.base, sl.f, X, Y, P, box_w, box_h);
             if (rc) return rc;
         }
-        for (uint32_t ty = 0; ty * sh->ty < Y; ++ty)
-            for (uint32_t tx = 0; tx * sh->tx < X; ++tx) tiles.push_back({i, (uint16_t)tx, (uint16_t)ty});
+        for (uint32_t y = 0; y * ty < Y; ++y)
+            for (uint32_t x = 0; x * tx < X; ++x) tiles.push_back({i, (uint16_t)x, (uint16_t)y});
     }
+    return TPT_OK;
+}
+
+// Uploads a tile list and its tensor maps, replacing *dt / *dm.
+static int upload_tile_maps(const std::vector<CUtensorMap> &tm, const std::vector<air::TileRef> &tiles,
+                            air::TileRef **dt_out, CUtensorMap **dm_out) {
     air::TileRef *dt = nullptr;
     CUtensorMap *dm = nullptr;
     cudaError_t e = cudaMalloc(&dt, tiles.size() * sizeof(air::TileRef));
@@ -423,13 +461,48 @@ static int set_tile_shape(tpt_batch *b, const air::TileShape *sh) {
         cudaFree(dm);
         TPT_FAIL(TPT_ERR_CUDA, "tile form upload failed: %s", cudaGetErrorString(e));
     }
-    cudaFree(b->form_tiles);
-    cudaFree(b->tmaps);
-    b->form_tiles = dt;
+    cudaFree(*dt_out);
+    cudaFree(*dm_out);
+    *dt_out = dt;
+    *dm_out = dm;
+    return TPT_OK;
+}
+
+// Builds the tile form's tile list and tensor maps for tile shape `sh` (the
+// boxes are the tile plus a 4-cell x and 3-cell y halo) and uploads them.
+static int set_tile_shape(tpt_batch *b, const air::TileShape *sh) {
+    int occ = 0;
+    int rc = sh->prepare(&occ);
+    if (rc) return rc;
+    if (occ < 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "the %ux%u tile kernels do not fit an SM", sh->tx, sh->ty);
+    std::vector<air::TileRef> tiles;
+    std::vector<CUtensorMap> tm;
+    rc = build_tile_maps(b, sh->tx, sh->ty, sh->tx + 8, sh->ty + 6, tm, tiles);
+    if (rc) return rc;
+    rc = upload_tile_maps(tm, tiles, &b->form_tiles, &b->tmaps);
+    if (rc) return rc;
     b->nform_tiles = (uint32_t)tiles.size();
-    b->tmaps = dm;
     b->shape = sh;
     b->tile_occupancy = occ;
+    return TPT_OK;
+}
+
+// The temporally blocked launches' tiles and tensor maps (boxes of the tile
+// plus an 8-cell x and 5-cell y halo), once per batch.
+static int set_fused(tpt_batch *b) {
+    if (b->fused_tiles) return TPT_OK;
+    int occ = 0;
+    int rc = air::fused_tile_prepare(&occ);
+    if (rc) return rc;
+    if (occ < 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "the temporally blocked air kernel does not fit an SM");
+    std::vector<air::TileRef> tiles;
+    std::vector<CUtensorMap> tm;
+    rc = build_tile_maps(b, air::FUSED_TX, air::FUSED_TY, air::FUSED_TX + 16, air::FUSED_TY + 10, tm, tiles);
+    if (rc) return rc;
+    rc = upload_tile_maps(tm, tiles, &b->fused_tiles, &b->tmaps_fused);
+    if (rc) return rc;
+    b->nfused_tiles = (uint32_t)tiles.size();
+    b->fused_occupancy = occ;
     return TPT_OK;
 }
 
@@ -530,6 +603,11 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
             T.vx = b->f(F_VX, i);
             T.vy = b->f(F_VY, i);
             T.pv_out = T.vx_out = T.vy_out = nullptr;
+            // the velocity pass's outputs alternate between two sets by tick
+            // parity (the sweep's ping-pong halves serve as the second set)
+            T.opv = b->f(par ? F_PV2 : F_OPV, i);
+            T.ovx = b->f(par ? F_VX2 : F_OVX, i);
+            T.ovy = b->f(par ? F_VY2 : F_OVY, i);
             b->insts_tile_host[2 * (size_t)i + par] = T;
         }
         if (p.air_mode == 4u && p.aheat_enable) b->any_noupdate_heat = true;
@@ -752,7 +830,10 @@ int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
             TPT_FAIL(TPT_ERR_INVALID_ARG, "tile %ux%u is not a tile form shape (32x8, 64x8, 32x16, 64x16)", t->tile_x,
                      t->tile_y);
     }
-    if (t->temporal_depth != 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "temporal depth %u not built", t->temporal_depth);
+    if (t->temporal_depth < 1 || t->temporal_depth > CHUNK)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "temporal_depth %u must be in 1..%u", t->temporal_depth, CHUNK);
+    if (sweep && t->temporal_depth != 1)
+        TPT_FAIL(TPT_ERR_UNSUPPORTED, "temporal blocking is built for the tile form; the sweep form takes depth 1");
     if (t->ctas_per_sm > 32) TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm must be 0 (as many as fit) .. 32");
     const bool split = b->any_grav && b->precision == TPT_PRECISION_SPLIT_BF16 && b->dft.can_split();
     if (t->grav_side_ctas && !split)
@@ -766,6 +847,10 @@ int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
                  t->ctas_per_sm, b->sweep_occupancy, t->tile_x);
     if (!sweep && sh != b->shape) {
         int rc = set_tile_shape(b, sh);
+        if (rc) return rc;
+    }
+    if (t->temporal_depth > 1) {
+        int rc = set_fused(b);
         if (rc) return rc;
     }
     if (split) {
@@ -801,9 +886,9 @@ int tpt_batch_profile_phases(tpt_batch *b, uint32_t ticks, tpt_stream_t stream, 
     TPT_CUDA(cudaEventCreate(&e0));
     TPT_CUDA(cudaEventCreate(&e1));
     TPT_CUDA(cudaEventCreate(&e2));
-    for (uint32_t t = 0; t < 2 && rc == TPT_OK; ++t) rc = b->air_tick(t, st);  // warm-up
+    if (rc == TPT_OK) rc = b->air_run(2, st);  // warm-up
     cudaEventRecord(e0, st);
-    for (uint32_t t = 0; t < ticks && rc == TPT_OK; ++t) rc = b->air_tick(t & 1u, st);
+    if (rc == TPT_OK) rc = b->air_run(ticks, st);
     cudaEventRecord(e1, st);
     for (uint32_t t = 0; t < ticks && rc == TPT_OK && b->any_grav; ++t) rc = b->grav_solve(st);
     cudaEventRecord(e2, st);
@@ -895,12 +980,35 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
         t.tile_x = cd.x;
         t.tile_y = cd.y;
         t.ctas_per_sm = cd.per_sm;
+        t.temporal_depth = 1;
         rc = tpt_batch_set_tuning(b, &t);
         if (rc) break;
         const uint32_t trial = 20;
         for (int rep = 0; rep < 2 && rc == TPT_OK; ++rep) {  // warm-up, then timed
             cudaEventRecord(e0, st);
-            for (uint32_t k = 0; k < trial && rc == TPT_OK; ++k) rc = b->air_tick(k & 1u, st);
+            rc = b->air_run(trial, st);
+            cudaEventRecord(e1, st);
+        }
+        if (rc) break;
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = t;
+        }
+    }
+    // Phase 1b, for the tile form: temporal depth (ticks per block of fused
+    // B(t) + A(t + 1) launches) at the chosen shape, on the same 20 ticks.
+    for (uint32_t depth : {2u, 4u, 10u, 20u}) {
+        if (rc || best.air_form != TPT_AIR_FORM_TILES) break;
+        tpt_batch_tuning t = best;
+        t.temporal_depth = depth;
+        rc = tpt_batch_set_tuning(b, &t);
+        if (rc) break;
+        for (int rep = 0; rep < 2 && rc == TPT_OK; ++rep) {  // warm-up, then timed
+            cudaEventRecord(e0, st);
+            rc = b->air_run(20, st);
             cudaEventRecord(e1, st);
         }
         if (rc) break;
