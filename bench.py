@@ -323,6 +323,7 @@ def run_ours(args, rank, world, local):
         t.tile_x, t.tile_y = args.air_shape or ((224, 64) if args.air_form == "sweep" else tf.TILE_SHAPES[0])
         t.ctas_per_sm = 0
         t.temporal_depth = args.temporal_depth
+        t.work_queue = args.work_queue
         batch.set_tuning(t)
     cells = sum(i.cells for i in insts)
     # cells all ranks advance per tick: every rank has a full copy (weak) or
@@ -403,6 +404,7 @@ def run_ours(args, rank, world, local):
         tfl = prof.grav_flops_per_tick * prof.ticks / (prof.grav_ms / 1e3) / 1e12
         roof_grav = {"kernel": "split-BF16 DFT-GEMM gravity", "bound": "tensor", "achieved": round(tfl, 2),
                      "peak": bf16, "unit": "TFLOP/s", "frac": round(tfl / bf16, 4), "peak_source": peak_src,
+                     "peak_sustained": bf16s, "frac_sustained": round(tfl / bf16s, 4),
                      "traffic": MEASURED_DRAM_BYTES.get(cid, {}).get("grav_solve"),
                      "traffic_unit": "DRAM bytes per solve of the batch, GEMM launches (ncu)"}
     else:
@@ -776,6 +778,8 @@ def main():
                     help="with --air-form: tile (tiles) or lanes x rows (sweep), e.g. 64x16")
     ap.add_argument("--temporal-depth", type=int, default=1,
                     help="with --air-form tiles: ticks per temporally blocked run (1 = none)")
+    ap.add_argument("--work-queue", type=int, choices=(0, 1), default=0,
+                    help="with --air-form tiles: 1 = atomic tile queue, 0 = static striding")
     ap.add_argument("--skip-tune", action="store_true", help="keep the batch's default tuning (profiling captures)")
     ap.add_argument("--instances", type=int, default=0,
                     help="only the first N instances of the workload (profiling captures on a smaller case)")

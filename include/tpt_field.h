@@ -386,6 +386,11 @@ typedef struct tpt_batch_tuning {
      * for every value. */
     uint32_t grav_side_ctas;
     uint32_t air_form;  /* TPT_AIR_FORM_TILES or TPT_AIR_FORM_SWEEP */
+    /* Tile form: 1 = the persistent CTAs take tiles from an atomic work
+     * queue (a counter per pass, cleared by the other pass's launch), 0 =
+     * they stride the tile list statically. The sweep form always takes its
+     * work items from a queue; 0 or 1. */
+    uint32_t work_queue;
 } tpt_batch_tuning;
 
 /*

@@ -111,8 +111,9 @@ def test_gravity_error_c5_batch_both_y_forms(cuda, tf, oracle):
     assert worst <= 1e-4
 
 
-@pytest.mark.parametrize("form,shape,depth", [(0, (32, 8), 1), (0, (64, 16), 1), (0, (32, 8), 5), (1, (224, 64), 1)])
-def test_c5_every_instance_air_and_gravity(cuda, tf, oracle, form, shape, depth):
+@pytest.mark.parametrize("form,shape,depth,queue", [(0, (32, 8), 1, 0), (0, (64, 16), 1, 1), (0, (32, 8), 5, 1),
+                                                    (1, (224, 64), 1, 0)])
+def test_c5_every_instance_air_and_gravity(cuda, tf, oracle, form, shape, depth, queue):
     """The whole C5 batch as benchmarked (64 x 400x225 + 64 heavy-tailed,
     split-BF16 gravity) after 20 ticks: every instance's air bit-exact
     against the oracle, and every instance's gx/gy within 1e-4 (rel-max and
@@ -129,6 +130,7 @@ def test_c5_every_instance_air_and_gravity(cuda, tf, oracle, form, shape, depth)
     t.tile_x, t.tile_y = shape
     t.ctas_per_sm = 0
     t.temporal_depth = depth
+    t.work_queue = queue
     b.set_tuning(t)
     b.step(20)
     cuda.cuda.synchronize()
@@ -141,7 +143,7 @@ def test_c5_every_instance_air_and_gravity(cuda, tf, oracle, form, shape, depth)
         e = max(*_err(st["gx"], dx), *_err(st["gy"], dy))
         worst = max(worst, (e, i))
     REPORT[f"gravity/split_bf16/C5 batch, all 128 instances, worst (air form {form}, {shape[0]}x{shape[1]}, "
-           f"depth {depth})"] = {
+           f"depth {depth}, queue {queue})"] = {
         "rel_err": worst[0], "instance": worst[1],
         "shape": f"{insts[worst[1]].xcells}x{insts[worst[1]].ycells}"}
     _dump()

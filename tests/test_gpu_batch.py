@@ -41,12 +41,13 @@ def check_against_oracle(tf, oracle, batch, insts, ticks, ctx):
 def set_form(tf, b, form, **kw):
     """Switches the batch's air form; tile_x / tile_y default to the form's
     default shape (32x8 tiles, 224-lane x 64-row sweeps), ctas_per_sm to 0,
-    temporal_depth to 1."""
+    temporal_depth to 1, work_queue to 1 (the default tuning's)."""
     t = b.tuning()
     t.air_form = form
     t.tile_x, t.tile_y = (224, 64) if form == tf.AIR_FORM_SWEEP else tf.TILE_SHAPES[0]
     t.ctas_per_sm = 0
     t.temporal_depth = 1
+    t.work_queue = 1
     for k, v in kw.items():
         setattr(t, k, v)
     b.set_tuning(t)
@@ -82,7 +83,7 @@ def test_tune_keeps_state_and_results(cuda, tf, oracle):
     t = b.tuning()
     assert t.air_form in (tf.AIR_FORM_TILES, tf.AIR_FORM_SWEEP)
     if t.air_form == tf.AIR_FORM_TILES:
-        assert (t.tile_x, t.tile_y) in tf.TILE_SHAPES and 1 <= t.ctas_per_sm <= 8
+        assert (t.tile_x, t.tile_y) in tf.TILE_SHAPES and t.ctas_per_sm in (0, 2, 4, 6, 8) and t.work_queue in (0, 1)
         assert t.temporal_depth in (1, 2, 4, 10, 20)
     else:
         assert (t.tile_x, t.tile_y) in ((224, 64), (256, 64), (256, 32)) and t.temporal_depth == 1
@@ -149,6 +150,25 @@ def test_temporal_blocking_is_bit_exact(cuda, tf, oracle, depth, ticks):
     b.close()
 
 
+@pytest.mark.parametrize("shape", [(32, 8), (64, 16)])
+@pytest.mark.parametrize("depth", [1, 3])
+@pytest.mark.parametrize("per_sm", [0, 1])
+def test_tile_work_queue_gives_the_same_fields(cuda, tf, oracle, shape, depth, per_sm):
+    """The tile form's CTAs taking tiles from the atomic work queues (cleared
+    by each other's launches), with and without temporal blocking, after
+    switching from static striding and back: bit-exact."""
+    insts = mixed_instances()
+    b = tf.Batch(insts)
+    for queue, ticks in ((0, 2), (1, 7), (0, 1), (1, 4)):
+        set_form(tf, b, tf.AIR_FORM_TILES, tile_x=shape[0], tile_y=shape[1], temporal_depth=depth,
+                 ctas_per_sm=per_sm, work_queue=queue)
+        b.step(ticks)
+    cuda.cuda.synchronize()
+    assert tf.lib().tpt_check_device_errors() == 0
+    check_against_oracle(tf, oracle, b, insts, 14, f"queue {shape[0]}x{shape[1]} depth {depth} {per_sm}/SM")
+    b.close()
+
+
 @pytest.mark.parametrize("shape", [(64, 8), (64, 16)])
 def test_temporal_blocking_with_other_tile_shapes(cuda, tf, oracle, shape):
     """The block's first and last launches at another tile shape than the
@@ -165,14 +185,15 @@ def test_temporal_blocking_with_other_tile_shapes(cuda, tf, oracle, shape):
 
 
 @pytest.mark.parametrize("per_sm", [1, 3, 6, 8])
-def test_tile_form_at_every_grid_size(cuda, tf, oracle, per_sm):
+@pytest.mark.parametrize("queue", [0, 1])
+def test_tile_form_at_every_grid_size(cuda, tf, oracle, per_sm, queue):
     insts = mixed_instances()
     b = tf.Batch(insts)
-    set_form(tf, b, tf.AIR_FORM_TILES, ctas_per_sm=per_sm)
+    set_form(tf, b, tf.AIR_FORM_TILES, ctas_per_sm=per_sm, work_queue=queue)
     b.step(9)
     cuda.cuda.synchronize()
     assert tf.lib().tpt_check_device_errors() == 0
-    check_against_oracle(tf, oracle, b, insts, 9, f"tiles {per_sm}/SM")
+    check_against_oracle(tf, oracle, b, insts, 9, f"tiles {per_sm}/SM queue {queue}")
     b.close()
 
 
@@ -205,7 +226,7 @@ def test_bad_tunings_are_rejected(cuda, tf):
         # temporal depth 1..50, tile form only
         dict(temporal_depth=0), dict(temporal_depth=51),
         dict(air_form=sweep, tile_x=224, tile_y=64, temporal_depth=2),
-        dict(air_form=2),
+        dict(air_form=2), dict(work_queue=2),
     ):
         t = b.tuning()
         for k, v in kw.items():
@@ -267,9 +288,9 @@ def test_batch_measured_config_subset(cuda, tf, oracle):
     b.close()
 
 
-@pytest.mark.parametrize("form,shape,depth", [(0, (32, 8), 1), (0, (64, 8), 1), (0, (32, 16), 1), (0, (32, 8), 4),
-                                              (1, (224, 64), 1)])
-def test_c4_every_instance_20_ticks(cuda, tf, oracle, form, shape, depth):
+@pytest.mark.parametrize("form,shape,depth,queue", [(0, (32, 8), 1, 0), (0, (64, 8), 1, 0), (0, (32, 16), 1, 1),
+                                                    (0, (32, 8), 4, 1), (1, (224, 64), 1, 0)])
+def test_c4_every_instance_20_ticks(cuda, tf, oracle, form, shape, depth, queue):
     """The whole C4 batch (256 instances, W, H log-uniform 32..512, FP32
     gravity) after 20 ticks: every instance's air bit-exact against the
     oracle and its gx/gy within 1e-5 of max|g| against FP64."""
@@ -278,11 +299,11 @@ def test_c4_every_instance_20_ticks(cuda, tf, oracle, form, shape, depth):
     insts = W.config_instances(4)
     assert len(insts) == 256
     b = tf.Batch(insts)
-    set_form(tf, b, form, tile_x=shape[0], tile_y=shape[1], temporal_depth=depth)
+    set_form(tf, b, form, tile_x=shape[0], tile_y=shape[1], temporal_depth=depth, work_queue=queue)
     b.step(20)
     cuda.cuda.synchronize()
     assert tf.lib().tpt_check_device_errors() == 0
-    check_against_oracle(tf, oracle, b, insts, 20, f"C4 form {form} {shape[0]}x{shape[1]} depth {depth}")
+    check_against_oracle(tf, oracle, b, insts, 20, f"C4 form {form} {shape[0]}x{shape[1]} depth {depth} queue {queue}")
     b.close()
 
 

@@ -35,20 +35,24 @@ enum TensorMapSlot {
 struct TileShape {
     uint32_t tx, ty;
     // sets the kernels' shared-memory limits and returns the resident CTAs
-    // per SM of the advection/heat pass
-    int (*prepare)(int *occupancy);
+    // per SM of the velocity pass (A) and the advection/heat pass (B)
+    int (*prepare)(int *occupancy_a, int *occupancy_b);
     // One tick of every instance. `insts` holds two AirInst per instance
     // (parity 0 and 1 of the hv / mask ping-pong; pv/vx/vy are updated in
-    // place); `tmaps` TM_COUNT tensor maps per instance.
+    // place); `tmaps` TM_COUNT tensor maps per instance. `queues`: the two
+    // passes' work-queue counters (device, zero at creation), used as queues
+    // when `use_queue` (else the CTAs stride the tile list statically) and
+    // cleared either way, each by the launch of the other pass.
     int (*launch)(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
-                  uint32_t parity, bool any_noupdate_heat, cudaStream_t st);
+                  uint32_t parity, bool any_noupdate_heat, uint32_t *queues, bool use_queue, cudaStream_t st);
     // the passes of one tick separately: the velocity pass (pass A), and the
     // advection / heat / mask pass (pass B, with its NoUpdate settle) whose
     // mask rebuild applies `emap_lag` pending emap decays
     int (*launch_a)(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles,
-                    uint32_t grid, uint32_t parity, cudaStream_t st);
+                    uint32_t grid, uint32_t parity, uint32_t *queues, bool use_queue, cudaStream_t st);
     int (*launch_b)(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles,
-                    uint32_t grid, uint32_t parity, uint32_t emap_lag, bool any_noupdate_heat, cudaStream_t st);
+                    uint32_t grid, uint32_t parity, uint32_t emap_lag, bool any_noupdate_heat, uint32_t *queues,
+                    bool use_queue, cudaStream_t st);
     // the copy-back of NoUpdate instances' convected velocity after a pass B
     int (*launch_settle)(const AirInst *insts, const TileRef *tiles, uint32_t ntiles, uint32_t grid, uint32_t parity,
                          cudaStream_t st);

@@ -83,17 +83,32 @@ __device__ __forceinline__ void issue_a(const AirInst &I, const CUtensorMap *m, 
     load_box(buf->b, m + TM_BA0 + parity, x0, y0, bar);
 }
 
+// The persistent CTAs' tile order: static striding (queue == null: tiles
+// blockIdx.x, + gridDim.x, ...) or an atomic work queue (each CTA takes the
+// next unclaimed tile; thread 0 claims it and shares it through shared
+// memory). Each pass's counter is cleared by the launch before it: pass A
+// clears pass B's (`reset`) and pass B clears pass A's.
+__device__ __forceinline__ uint32_t first_tile(uint32_t *queue) {
+    return queue ? atomicAdd(queue, 1u) : blockIdx.x;
+}
+__device__ __forceinline__ uint32_t next_tile(uint32_t *queue, uint32_t t) {
+    return queue ? atomicAdd(queue, 1u) : t + gridDim.x;
+}
+
 __global__ void __launch_bounds__(NT) kb_pressure_velocity(const AirInst *__restrict__ insts,
                                                            const CUtensorMap *__restrict__ tmaps,
                                                            const TileRef *__restrict__ tiles, uint32_t ntiles,
-                                                           uint32_t parity) {
+                                                           uint32_t parity, uint32_t *queue, uint32_t *reset) {
     BoxA *buf = reinterpret_cast<BoxA *>(air_tile_smem);
     float *opv = reinterpret_cast<float *>(buf + 2);
     __shared__ uint64_t full[2];
+    __shared__ uint32_t s_tile;
     if (threadIdx.x == 0) {
         tc::mbar_init(&full[0], 1);
         tc::mbar_init(&full[1], 1);
         tc::fence_mbar_init();
+        if (blockIdx.x == 0) *reset = 0u;
+        s_tile = first_tile(queue);
     }
     __syncthreads();
     uint32_t uses = 0;  // bit k: phase parity of full[k] (a register, not an indexed array)
@@ -106,29 +121,42 @@ __global__ void __launch_bounds__(NT) kb_pressure_velocity(const AirInst *__rest
         issue_a(I, tmaps + (size_t)i * TM_COUNT, parity, x0, y0, &buf[k], &full[k]);
         return true;
     };
-    if (threadIdx.x == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    uint32_t t = s_tile;
+    if (threadIdx.x == 0 && t < ntiles) issue(t, 0);
     int k = 0;
-    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x, k ^= 1) {
+    while (t < ntiles) {
         uint32_t i;
         int x0, y0;
         tile_of(tiles, t, i, x0, y0);
         const AirInst I = insts[2 * i + parity];
-        const uint32_t tn = t + gridDim.x;
+        uint32_t tn = 0;           // thread 0: the next tile
         bool next_issued = false;  // thread 0: a bulk copy into buf[k ^ 1] is in flight
-        if (threadIdx.x == 0 && tn < ntiles) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            next_issued = issue(tn, k ^ 1);
+        if (threadIdx.x == 0) {
+            tn = next_tile(queue, t);
+            if (tn < ntiles) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                next_issued = issue(tn, k ^ 1);
+            }
         }
-        if (!a_loads(I)) continue;
-        bool ok = tc::mbar_wait(&full[k], (uses >> k) & 1u, &g_tile_err);
-        uses ^= 1u << k;
+        const bool loads = a_loads(I) != 0u;
+        bool ok = true;
+        if (loads) {
+            ok = tc::mbar_wait(&full[k], (uses >> k) & 1u, &g_tile_err);
+            uses ^= 1u << k;
+        }
+        // every thread has read s_tile for this tile before thread 0 overwrites it
         if (!__syncthreads_and(ok)) {
             drain_on_timeout(full, k, uses, next_issued);
             return;
         }
-        LayoutA2 S{&buf[k], opv};
-        pass_a(I, x0, y0, S);
+        if (threadIdx.x == 0) s_tile = tn;
+        if (loads) {
+            LayoutA2 S{&buf[k], opv};
+            pass_a(I, x0, y0, S);
+        }
         __syncthreads();
+        t = s_tile;
+        k ^= 1;
     }
 }
 
@@ -169,14 +197,18 @@ __device__ __forceinline__ void issue_b(const AirInst &I, const CUtensorMap *m, 
 __global__ void __launch_bounds__(NT, B_MIN_CTAS) kb_advect_heat(const AirInst *__restrict__ insts,
                                                               const CUtensorMap *__restrict__ tmaps,
                                                               const TileRef *__restrict__ tiles, uint32_t ntiles,
-                                                              uint32_t parity, uint32_t emap_lag) {
+                                                              uint32_t parity, uint32_t emap_lag, uint32_t *queue,
+                                                              uint32_t *reset) {
     BoxB *buf = reinterpret_cast<BoxB *>(air_tile_smem);
     WorkB2 *work = reinterpret_cast<WorkB2 *>(buf + 2);
     __shared__ uint64_t full[2];
+    __shared__ uint32_t s_tile;
     if (threadIdx.x == 0) {
         tc::mbar_init(&full[0], 1);
         tc::mbar_init(&full[1], 1);
         tc::fence_mbar_init();
+        if (blockIdx.x == 0) *reset = 0u;
+        s_tile = first_tile(queue);
     }
     __syncthreads();
     uint32_t uses = 0;  // bit k: phase parity of full[k] (a register, not an indexed array)
@@ -189,26 +221,36 @@ __global__ void __launch_bounds__(NT, B_MIN_CTAS) kb_advect_heat(const AirInst *
         issue_b(I, tmaps + (size_t)i * TM_COUNT, parity, x0, y0, &buf[k], &full[k]);
         return true;
     };
-    if (threadIdx.x == 0 && blockIdx.x < ntiles) issue(blockIdx.x, 0);
+    uint32_t t = s_tile;
+    if (threadIdx.x == 0 && t < ntiles) issue(t, 0);
     int k = 0;
-    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x, k ^= 1) {
+    while (t < ntiles) {
         uint32_t i;
         int x0, y0;
         tile_of(tiles, t, i, x0, y0);
         const AirInst I = insts[2 * i + parity];
-        const uint32_t tn = t + gridDim.x;
+        uint32_t tn = 0;           // thread 0: the next tile
         bool next_issued = false;  // thread 0: a bulk copy into buf[k ^ 1] is in flight
-        if (threadIdx.x == 0 && tn < ntiles) {
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            next_issued = issue(tn, k ^ 1);
-        }
-        if (b_loads(I)) {
-            bool ok = tc::mbar_wait(&full[k], (uses >> k) & 1u, &g_tile_err);
-            uses ^= 1u << k;
-            if (!__syncthreads_and(ok)) {
-                drain_on_timeout(full, k, uses, next_issued);
-                return;
+        if (threadIdx.x == 0) {
+            tn = next_tile(queue, t);
+            if (tn < ntiles) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                next_issued = issue(tn, k ^ 1);
             }
+        }
+        const bool loads = b_loads(I) != 0u;
+        bool ok = true;
+        if (loads) {
+            ok = tc::mbar_wait(&full[k], (uses >> k) & 1u, &g_tile_err);
+            uses ^= 1u << k;
+        }
+        // every thread has read s_tile for this tile before thread 0 overwrites it
+        if (!__syncthreads_and(ok)) {
+            drain_on_timeout(full, k, uses, next_issued);
+            return;
+        }
+        if (threadIdx.x == 0) s_tile = tn;
+        if (loads) {
             LayoutB2 S{&buf[k], work};
             if (I.air_mode == 4u) {  // stored velocity of the +1 ring for the heat pass
                 for_ring<1>(I, x0, y0, [&](int gx, int gy) {
@@ -228,6 +270,8 @@ __global__ void __launch_bounds__(NT, B_MIN_CTAS) kb_advect_heat(const AirInst *
             I.bairh_out[g] = bh;
         }
         __syncthreads();
+        t = s_tile;
+        k ^= 1;
     }
 }
 
@@ -254,7 +298,7 @@ __global__ void kb_noupdate_settle(const AirInst *__restrict__ insts, const Tile
 
 // ---- host side of this shape ------------------------------------------------------
 namespace {
-int tile_prepare(int *occupancy) {
+int tile_prepare(int *occupancy_a, int *occupancy_b) {
     using namespace AIR_SHAPE_NS;
     TPT_CUDA(cudaFuncSetAttribute(kb_pressure_velocity, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_A));
     TPT_CUDA(cudaFuncSetAttribute(kb_advect_heat, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_B));
@@ -264,16 +308,16 @@ int tile_prepare(int *occupancy) {
                                   (int)cudaSharedmemCarveoutMaxShared));
     TPT_CUDA(cudaFuncSetAttribute(kb_advect_heat, cudaFuncAttributePreferredSharedMemoryCarveout,
                                   (int)cudaSharedmemCarveoutMaxShared));
-    int occ = 0;
-    TPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kb_advect_heat, NT, SMEM_B));
-    *occupancy = occ;
+    TPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy_a, kb_pressure_velocity, NT, SMEM_A));
+    TPT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(occupancy_b, kb_advect_heat, NT, SMEM_B));
     return TPT_OK;
 }
 
 int tile_launch_a(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
-                  uint32_t parity, cudaStream_t st) {
+                  uint32_t parity, uint32_t *queues, bool use_queue, cudaStream_t st) {
     using namespace AIR_SHAPE_NS;
-    kb_pressure_velocity<<<grid, NT, SMEM_A, st>>>(insts, tmaps, tiles, ntiles, parity);
+    kb_pressure_velocity<<<grid, NT, SMEM_A, st>>>(insts, tmaps, tiles, ntiles, parity, use_queue ? queues : nullptr,
+                                                   queues + 1);
     TPT_LAUNCHED();
     return TPT_OK;
 }
@@ -287,17 +331,20 @@ int tile_launch_settle(const AirInst *insts, const TileRef *tiles, uint32_t ntil
 }
 
 int tile_launch_b(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
-                  uint32_t parity, uint32_t emap_lag, bool any_noupdate_heat, cudaStream_t st) {
+                  uint32_t parity, uint32_t emap_lag, bool any_noupdate_heat, uint32_t *queues, bool use_queue,
+                  cudaStream_t st) {
     using namespace AIR_SHAPE_NS;
-    kb_advect_heat<<<grid, NT, SMEM_B, st>>>(insts, tmaps, tiles, ntiles, parity, emap_lag);
+    kb_advect_heat<<<grid, NT, SMEM_B, st>>>(insts, tmaps, tiles, ntiles, parity, emap_lag,
+                                             use_queue ? queues + 1 : nullptr, queues);
     TPT_LAUNCHED();
     return any_noupdate_heat ? tile_launch_settle(insts, tiles, ntiles, grid, parity, st) : TPT_OK;
 }
 
 int tile_launch(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
-                uint32_t parity, bool any_noupdate_heat, cudaStream_t st) {
-    int rc = tile_launch_a(insts, tmaps, tiles, ntiles, grid, parity, st);
-    return rc ? rc : tile_launch_b(insts, tmaps, tiles, ntiles, grid, parity, 0u, any_noupdate_heat, st);
+                uint32_t parity, bool any_noupdate_heat, uint32_t *queues, bool use_queue, cudaStream_t st) {
+    int rc = tile_launch_a(insts, tmaps, tiles, ntiles, grid, parity, queues, use_queue, st);
+    return rc ? rc
+              : tile_launch_b(insts, tmaps, tiles, ntiles, grid, parity, 0u, any_noupdate_heat, queues, use_queue, st);
 }
 
 int tile_read_errors(uint32_t *out) {

@@ -162,13 +162,14 @@ struct tpt_batch {
     air::TileRef *form_tiles = nullptr;
     uint32_t nform_tiles = 0;
     CUtensorMap *tmaps = nullptr;
-    int tile_occupancy = 1;
+    int tile_occupancy_a = 1, tile_occupancy_b = 1;  // resident CTAs per SM of pass A / pass B
     // temporal blocking (tuning.temporal_depth > 1): the B(t) + A(t + 1)
     // launches' tiles and tensor maps (their own box), built on first use
     air::TileRef *fused_tiles = nullptr;
     uint32_t nfused_tiles = 0;
     CUtensorMap *tmaps_fused = nullptr;
     int fused_occupancy = 0;
+    uint32_t *tile_queue = nullptr;  // the two passes' work-queue counters
     // the sweep form of the air tick: work items (device), the queue counter
     // and the pre-pass flags ([2][n], zeroed at creation)
     air::SweepItem *items = nullptr;
@@ -177,7 +178,7 @@ struct tpt_batch {
     uint32_t *want = nullptr;
     uint32_t sweep_lanes = 0, sweep_rows = 0;  // the shape the items are planned for
     bool any_grav = false;
-    tpt_batch_tuning tuning{DEFAULT_TILE_X, DEFAULT_TILE_Y, 1, 0, 0, TPT_AIR_FORM_TILES};
+    tpt_batch_tuning tuning{DEFAULT_TILE_X, DEFAULT_TILE_Y, 1, 0, 0, TPT_AIR_FORM_TILES, 1};
     int sweep_occupancy = 1;  // resident sweep CTAs per SM at sweep_lanes
     int sms = 148;
     gfft::FftSet fft;
@@ -214,10 +215,12 @@ struct tpt_batch {
     }
     // the tile form's persistent grid: ctas_per_sm per SM (0: as many as fit,
     // the residency of its advection/heat pass)
-    uint32_t tile_grid() const {
-        const uint32_t per_sm = tuning.ctas_per_sm ? tuning.ctas_per_sm : (uint32_t)tile_occupancy;
+    uint32_t tile_grid(int occupancy) const {
+        const uint32_t per_sm = tuning.ctas_per_sm ? tuning.ctas_per_sm : (uint32_t)occupancy;
         return std::max<uint32_t>(1u, std::min<uint32_t>(nform_tiles, (uint32_t)sms * per_sm));
     }
+    uint32_t tile_grid_a() const { return tile_grid(tile_occupancy_a); }
+    uint32_t tile_grid_b() const { return tile_grid(tile_occupancy_b); }
     bool sweep_form() const { return tuning.air_form == TPT_AIR_FORM_SWEEP; }
     const AirInst *form_insts() const { return sweep_form() ? insts : insts_tile; }
     uint32_t fused_grid() const {
@@ -236,16 +239,17 @@ struct tpt_batch {
         const uint32_t k = std::max<uint32_t>(1u, tuning.temporal_depth);
         for (uint32_t t = 0; t < ticks && rc == TPT_OK;) {
             const uint32_t n = std::min<uint32_t>(k, ticks - t);
-            rc = shape->launch_a(insts_tile, tmaps, form_tiles, nform_tiles, tile_grid(), t & 1u, st);
+            rc = shape->launch_a(insts_tile, tmaps, form_tiles, nform_tiles, tile_grid_a(), t & 1u, tile_queue,
+                                 tuning.work_queue != 0, st);
             for (uint32_t j = 0; j + 1 < n && rc == TPT_OK; ++j) {
                 const uint32_t p = (t + j) & 1u;
                 rc = air::launch_fused_ba(insts_tile, tmaps_fused, fused_tiles, nfused_tiles, fused_grid(), p, j, st);
                 if (rc == TPT_OK && any_noupdate_heat)
-                    rc = shape->launch_settle(insts_tile, form_tiles, nform_tiles, tile_grid(), p, st);
+                    rc = shape->launch_settle(insts_tile, form_tiles, nform_tiles, tile_grid_b(), p, st);
             }
             if (rc == TPT_OK)
-                rc = shape->launch_b(insts_tile, tmaps, form_tiles, nform_tiles, tile_grid(), (t + n - 1) & 1u, n - 1,
-                                     any_noupdate_heat, st);
+                rc = shape->launch_b(insts_tile, tmaps, form_tiles, nform_tiles, tile_grid_b(), (t + n - 1) & 1u, n - 1,
+                                     any_noupdate_heat, tile_queue, tuning.work_queue != 0, st);
             t += n;
         }
         return rc;
@@ -272,6 +276,7 @@ struct tpt_batch {
         cudaFree(form_tiles);
         cudaFree(fused_tiles);
         cudaFree(tmaps_fused);
+        cudaFree(tile_queue);
         cudaFree(items);
         cudaFree(ctl);
         if (side) cudaStreamDestroy(side);
@@ -471,10 +476,10 @@ static int upload_tile_maps(const std::vector<CUtensorMap> &tm, const std::vecto
 // Builds the tile form's tile list and tensor maps for tile shape `sh` (the
 // boxes are the tile plus a 4-cell x and 3-cell y halo) and uploads them.
 static int set_tile_shape(tpt_batch *b, const air::TileShape *sh) {
-    int occ = 0;
-    int rc = sh->prepare(&occ);
+    int occ_a = 0, occ_b = 0;
+    int rc = sh->prepare(&occ_a, &occ_b);
     if (rc) return rc;
-    if (occ < 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "the %ux%u tile kernels do not fit an SM", sh->tx, sh->ty);
+    if (occ_a < 1 || occ_b < 1) TPT_FAIL(TPT_ERR_UNSUPPORTED, "the %ux%u tile kernels do not fit an SM", sh->tx, sh->ty);
     std::vector<air::TileRef> tiles;
     std::vector<CUtensorMap> tm;
     rc = build_tile_maps(b, sh->tx, sh->ty, sh->tx + 8, sh->ty + 6, tm, tiles);
@@ -483,7 +488,8 @@ static int set_tile_shape(tpt_batch *b, const air::TileShape *sh) {
     if (rc) return rc;
     b->nform_tiles = (uint32_t)tiles.size();
     b->shape = sh;
-    b->tile_occupancy = occ;
+    b->tile_occupancy_a = occ_a;
+    b->tile_occupancy_b = occ_b;
     return TPT_OK;
 }
 
@@ -629,6 +635,8 @@ int tpt_batch_create(uint32_t n, const tpt_instance_desc *descs, int precision, 
         e = cudaMemcpy(b->insts, b->insts_host.data(), b->insts_host.size() * sizeof(AirInst), cudaMemcpyHostToDevice);
     if (e == cudaSuccess)
         e = cudaMemcpy(b->tiles, tiles.data(), tiles.size() * sizeof(air::TileRef), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&b->tile_queue, 2 * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(b->tile_queue, 0, 2 * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMalloc(&b->ctl, (1 + 2 * (size_t)n) * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(b->ctl, 0, (1 + 2 * (size_t)n) * sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
@@ -835,6 +843,7 @@ int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
     if (sweep && t->temporal_depth != 1)
         TPT_FAIL(TPT_ERR_UNSUPPORTED, "temporal blocking is built for the tile form; the sweep form takes depth 1");
     if (t->ctas_per_sm > 32) TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm must be 0 (as many as fit) .. 32");
+    if (t->work_queue > 1u) TPT_FAIL(TPT_ERR_INVALID_ARG, "work_queue must be 0 (static striding) or 1 (queue)");
     const bool split = b->any_grav && b->precision == TPT_PRECISION_SPLIT_BF16 && b->dft.can_split();
     if (t->grav_side_ctas && !split)
         TPT_FAIL(TPT_ERR_INVALID_ARG, "grav_side_ctas must be 0: the batch's gravity has one kind of y stage");
@@ -946,28 +955,24 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
     int src = saved.save(b, st);
     if (src) return src;
     // Phase 1: the air form and its layout, by timing 20 air ticks of each
-    // candidate: the tile form at every tile shape (32x8 at 2..8 CTAs per SM,
-    // the larger tiles at as many CTAs as fit and one fewer), the sweep form at
-    // a few shapes (lanes per CTA x rows per strip) with as many CTAs as fit.
+    // candidate: the tile form at every tile shape, with static striding and
+    // with the atomic work queue, at each pass's own residency (0) and at 4,
+    // 6 and 8 CTAs per SM (32x8; the larger tiles at 0 and 2); the sweep form
+    // at a few shapes (lanes per CTA x rows per strip) with as many CTAs as
+    // fit.
     struct Cand {
-        uint32_t form, x, y, per_sm;
+        uint32_t form, x, y, per_sm, queue;
     };
     std::vector<Cand> cands;
     for (int k = 0; k < air::TILE_SHAPES; ++k) {
         const air::TileShape *sh = air::tile_shapes()[k];
-        if (sh->tx == DEFAULT_TILE_X && sh->ty == DEFAULT_TILE_Y) {
-            for (uint32_t c : {2u, 3u, 4u, 6u, 8u}) cands.push_back({TPT_AIR_FORM_TILES, sh->tx, sh->ty, c});
-            continue;
-        }
-        int occ = 0;
-        int prc = sh->prepare(&occ);
-        if (prc) return prc;
-        if (occ < 1) continue;
-        cands.push_back({TPT_AIR_FORM_TILES, sh->tx, sh->ty, (uint32_t)occ});
-        if (occ > 1) cands.push_back({TPT_AIR_FORM_TILES, sh->tx, sh->ty, (uint32_t)occ - 1u});
+        const bool base = sh->tx == DEFAULT_TILE_X && sh->ty == DEFAULT_TILE_Y;
+        for (uint32_t q : {1u, 0u})
+            for (uint32_t c : base ? std::vector<uint32_t>{0u, 4u, 6u, 8u} : std::vector<uint32_t>{0u, 2u})
+                cands.push_back({TPT_AIR_FORM_TILES, sh->tx, sh->ty, c, q});
     }
     for (auto sh : {std::make_pair(224u, 64u), std::make_pair(256u, 64u), std::make_pair(256u, 32u)})
-        cands.push_back({TPT_AIR_FORM_SWEEP, sh.first, sh.second, 0u});
+        cands.push_back({TPT_AIR_FORM_SWEEP, sh.first, sh.second, 0u, 0u});
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -981,6 +986,7 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
         t.tile_y = cd.y;
         t.ctas_per_sm = cd.per_sm;
         t.temporal_depth = 1;
+        t.work_queue = cd.queue;
         rc = tpt_batch_set_tuning(b, &t);
         if (rc) break;
         const uint32_t trial = 20;
@@ -998,8 +1004,8 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
             best = t;
         }
     }
-    // Phase 1b, for the tile form: temporal depth (ticks per block of fused
-    // B(t) + A(t + 1) launches) at the chosen shape, on the same 20 ticks.
+    // Phase 1b, for the tile form at the chosen layout, on the same 20 ticks:
+    // the temporal depth (ticks per block of fused B(t) + A(t + 1) launches).
     for (uint32_t depth : {2u, 4u, 10u, 20u}) {
         if (rc || best.air_form != TPT_AIR_FORM_TILES) break;
         tpt_batch_tuning t = best;

@@ -124,7 +124,8 @@ class BatchProfile(ctypes.Structure):
 
 class BatchTuning(ctypes.Structure):
     _fields_ = [("tile_x", ctypes.c_uint32), ("tile_y", ctypes.c_uint32), ("temporal_depth", ctypes.c_uint32),
-                ("ctas_per_sm", ctypes.c_uint32), ("grav_side_ctas", ctypes.c_uint32), ("air_form", ctypes.c_uint32)]
+                ("ctas_per_sm", ctypes.c_uint32), ("grav_side_ctas", ctypes.c_uint32), ("air_form", ctypes.c_uint32),
+                ("work_queue", ctypes.c_uint32)]
 
 
 AIR_FORM_TILES, AIR_FORM_SWEEP = 0, 1
