@@ -411,8 +411,9 @@ int tpt_batch_fields(tpt_batch *batch, uint32_t instance,
 int tpt_batch_step(tpt_batch *batch, uint32_t ticks, tpt_stream_t stream);
 /* Times candidate tunings on the batch's own data (state is saved and
  * restored) and keeps the fastest: the air form with its shape (tile_x x
- * tile_y) and CTAs per SM, the temporal depth (tile form), then the gravity
- * branch split. The choice is cached in
+ * tile_y), CTAs per SM and tile order, the temporal depth (tile form), then,
+ * for batches with gravity, the whole step (air and gravity together) for
+ * the best few air settings and every gravity branch split. The choice is cached in
  * the process per batch composition -- the instances' (xcells, ycells)
  * buckets (powers of two) with their counts, and the gravity precision -- so
  * tuning a batch of the same composition again only applies the cached
