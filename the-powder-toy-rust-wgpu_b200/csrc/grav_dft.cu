@@ -1158,12 +1158,19 @@ int DftSet::set_io(size_t j, const SolveIO &io) {
 }
 
 // One stage's GEMM launch over a tile list, `ctas` persistent CTAs at most.
+// CTA b takes tiles b, b + grid, ..., so the launch lasts ceil(n / grid)
+// tile rounds; the grid is the fewest CTAs that need no more rounds than
+// `ctas` would (450 tiles on 148 SMs: 113 CTAs, 4 rounds each at most), which
+// leaves the SMs that would only idle in the last round to the air launches
+// running beside the gravity chain.
 template <int S>
 static int stage_launch(const DftImpl *I, const Tile *tiles, uint32_t n, uint32_t ctas, cudaStream_t st,
                         const InstIO &io0, int act) {
     if (n == 0) return TPT_OK;
-    dft_gemm<S><<<std::min(n, ctas), THREADS, SMEM_BYTES, st>>>(I->probs, tiles, n, I->groups, I->ios, io0, act,
-                                                                  I->err);
+    const uint32_t cap = std::max<uint32_t>(1u, std::min(n, ctas));
+    const uint32_t rounds = (n + cap - 1) / cap;
+    const uint32_t grid = (n + rounds - 1) / rounds;
+    dft_gemm<S><<<grid, THREADS, SMEM_BYTES, st>>>(I->probs, tiles, n, I->groups, I->ios, io0, act, I->err);
     TPT_LAUNCHED();
     return TPT_OK;
 }
