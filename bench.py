@@ -272,6 +272,46 @@ def run_plain(ticks: int):
     return inst.cells * ticks / (ms / 1e3), ms / ticks
 
 
+def run_c3(solves: int):
+    """The gravity-only configuration: one 512x512 grid with clustered f32
+    mass (all cells unmasked), `solves` solves through GravityFft.solve in
+    each precision, device time with the inputs resident. Returns
+    {precision: {ms_per_solve, ...}}; the split-BF16 line adds the
+    algorithmic rate 3F / time with F = 24 X^2 Y + 96 X Y^2 (the dense
+    separable DFT-GEMM's flops, times the 3 split products)."""
+    import torch
+
+    import tpt_field as tf
+    import workloads as W
+
+    X = Y = 512
+    mass = torch.from_numpy(W.clustered_mass(X, Y, W.instance_seed(3, 0))).cuda()
+    cfg = tf.SimulationConfig(xres=4 * X, yres=4 * Y, newton_grav=True)
+    b = tf.SimBuffers(cfg)
+    b.grav_mask.fill_(-1)
+    stream = torch.cuda.current_stream()
+    out = {}
+    for name, prec in (("split_bf16", tf.PRECISION_SPLIT_BF16), ("fp32", tf.PRECISION_FP32)):
+        solver = tf.GravityFft(prec)
+        for _ in range(5):
+            solver.solve(b, mass, stream=stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(solves):
+            solver.solve(b, mass, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / solves
+        solver.close()
+        out[name] = {"ms_per_solve": round(ms, 5)}
+        if prec == tf.PRECISION_SPLIT_BF16:
+            F = 24.0 * X * X * Y + 96.0 * X * Y * Y
+            out[name]["algorithmic_tflops_3F"] = round(3.0 * F / (ms / 1e3) / 1e12, 1)
+    out["config"] = "C3 gravity only, 512x512 cells, clustered f32 mass, %d solves" % solves
+    return out
+
+
 def air_launches(ticks, tuning, per_tick, chunk=50):
     """Air launches of `ticks` ticks stepped in graphs of `chunk` ticks.
     `per_tick` is the profile's unblocked count (2, or 3 with a NoUpdate +
@@ -420,6 +460,8 @@ def run_ours(args, rank, world, local):
                  "value": p_rate, "unit": "cell-ticks/s", "ms_per_tick": p_ms, "ticks": args.plain_ticks,
                  "speedup_of_this_line": value / world / p_rate}
 
+    c3 = run_c3(args.c3_solves) if rank == 0 and world == 1 and args.c3_solves > 0 else None
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, cores, desc = cpu_rate(insts, args.cpu_seconds)
@@ -445,6 +487,7 @@ def run_ours(args, rank, world, local):
             "clocks": clk,
             "cpu_baseline": cpu,
             "plain_fp32_single_instance": plain,
+            "gravity_c3": c3,
         }
         print(json.dumps(line), flush=True)
     batch.close()
@@ -764,6 +807,8 @@ def main():
     ap.add_argument("--workload", type=int, choices=(1, 2, 4, 5), default=5)
     ap.add_argument("--ticks", type=int, default=0)
     ap.add_argument("--plain-ticks", type=int, default=500, help="ticks of the plain FP32 comparison (0 = skip)")
+    ap.add_argument("--c3-solves", type=int, default=100,
+                    help="solves of the gravity-only 512x512 line, each precision (0 = skip)")
     ap.add_argument("--scaling", choices=("weak", "strong"), default="weak",
                     help="weak: every rank steps a full copy; strong: ranks split one copy's instances")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="host work of the GPU arm's cpu_baseline leg")

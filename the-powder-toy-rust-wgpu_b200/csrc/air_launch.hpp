@@ -37,17 +37,15 @@ struct TileShape {
     // sets the kernels' shared-memory limits and returns the resident CTAs
     // per SM of the velocity pass (A) and the advection/heat pass (B)
     int (*prepare)(int *occupancy_a, int *occupancy_b);
-    // One tick of every instance. `insts` holds two AirInst per instance
-    // (parity 0 and 1 of the hv / mask ping-pong; pv/vx/vy are updated in
-    // place); `tmaps` TM_COUNT tensor maps per instance. `queues`: the two
-    // passes' work-queue counters (device, zero at creation), used as queues
-    // when `use_queue` (else the CTAs stride the tile list statically) and
-    // cleared either way, each by the launch of the other pass.
-    int (*launch)(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
-                  uint32_t parity, bool any_noupdate_heat, uint32_t *queues, bool use_queue, cudaStream_t st);
-    // the passes of one tick separately: the velocity pass (pass A), and the
-    // advection / heat / mask pass (pass B, with its NoUpdate settle) whose
-    // mask rebuild applies `emap_lag` pending emap decays
+    // The two passes of one tick of every instance: the velocity pass (A),
+    // and the advection / heat / mask pass (B, with its NoUpdate settle)
+    // whose mask rebuild applies `emap_lag` pending emap decays. `insts` holds
+    // two AirInst per instance (parity 0 and 1 of the hv / mask ping-pong and
+    // of the velocity-pass outputs; pv/vx/vy are updated in place); `tmaps`
+    // TM_COUNT tensor maps per instance. `queues`: the two passes' work-queue
+    // counters (device, zero at creation), used as queues when `use_queue`
+    // (else the CTAs stride the tile list statically) and cleared either way,
+    // each by the launch of the other pass.
     int (*launch_a)(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles,
                     uint32_t grid, uint32_t parity, uint32_t *queues, bool use_queue, cudaStream_t st);
     int (*launch_b)(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles,

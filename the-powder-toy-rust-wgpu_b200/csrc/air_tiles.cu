@@ -340,13 +340,6 @@ int tile_launch_b(const AirInst *insts, const CUtensorMap *tmaps, const TileRef 
     return any_noupdate_heat ? tile_launch_settle(insts, tiles, ntiles, grid, parity, st) : TPT_OK;
 }
 
-int tile_launch(const AirInst *insts, const CUtensorMap *tmaps, const TileRef *tiles, uint32_t ntiles, uint32_t grid,
-                uint32_t parity, bool any_noupdate_heat, uint32_t *queues, bool use_queue, cudaStream_t st) {
-    int rc = tile_launch_a(insts, tmaps, tiles, ntiles, grid, parity, queues, use_queue, st);
-    return rc ? rc
-              : tile_launch_b(insts, tmaps, tiles, ntiles, grid, parity, 0u, any_noupdate_heat, queues, use_queue, st);
-}
-
 int tile_read_errors(uint32_t *out) {
     using namespace AIR_SHAPE_NS;
     uint32_t v = 0, z = 0;
@@ -361,8 +354,8 @@ int tile_read_errors(uint32_t *out) {
 #define AIR_CAT2(a, b) a##b
 #define AIR_CAT(a, b) AIR_CAT2(a, b)
 extern const TileShape AIR_CAT(tile_shape_, AIR_SHAPE_NS) = {(uint32_t)AIR_SHAPE_NS::TX, (uint32_t)AIR_SHAPE_NS::TY,
-                                                            tile_prepare, tile_launch, tile_launch_a,
-                                                            tile_launch_b, tile_launch_settle, tile_read_errors};
+                                                            tile_prepare, tile_launch_a, tile_launch_b,
+                                                            tile_launch_settle, tile_read_errors};
 
 }  // namespace air
 }  // namespace tpt
