@@ -312,7 +312,7 @@ def run_c3(solves: int):
     return out
 
 
-def air_launches(ticks, tuning, per_tick, chunk=50):
+def air_launches(ticks, tuning, per_tick, chunk=1000):
     """Air launches of `ticks` ticks stepped in graphs of `chunk` ticks.
     `per_tick` is the profile's unblocked count (2, or 3 with a NoUpdate +
     heat instance in the tile form); the tile form at temporal depth k runs

@@ -138,8 +138,7 @@ def test_temporal_blocking_is_bit_exact(cuda, tf, oracle, depth, ticks):
     B(t) + A(t + 1) launches and B, with the emap decays deferred to the
     block's last launch (the stress instances' electrified walls decay over
     three ticks), NoUpdate and no-heat instances, blocks cut short by the
-    step's tick count and by the 50-tick graph chunks: bit-exact after every
-    step length."""
+    step's tick count: bit-exact after every step length."""
     insts = mixed_instances()
     b = tf.Batch(insts)
     set_form(tf, b, tf.AIR_FORM_TILES, temporal_depth=depth)
@@ -148,6 +147,20 @@ def test_temporal_blocking_is_bit_exact(cuda, tf, oracle, depth, ticks):
     assert tf.lib().tpt_check_device_errors() == 0
     check_against_oracle(tf, oracle, b, insts, ticks, f"depth {depth}, {ticks} ticks")
     b.close()
+
+
+def test_steps_longer_than_one_graph(cuda, tf, oracle):
+    """A step of more ticks than one captured graph holds (1000) replays it
+    and then a graph of the rest; temporal blocks are cut at the graph's end."""
+    insts = mixed_instances()[:3]
+    for depth in (1, 3):
+        b = tf.Batch(insts)
+        set_form(tf, b, tf.AIR_FORM_TILES, temporal_depth=depth)
+        b.step(1003)
+        cuda.cuda.synchronize()
+        assert tf.lib().tpt_check_device_errors() == 0
+        check_against_oracle(tf, oracle, b, insts, 1003, f"1003 ticks depth {depth}")
+        b.close()
 
 
 @pytest.mark.parametrize("shape", [(32, 8), (64, 16)])

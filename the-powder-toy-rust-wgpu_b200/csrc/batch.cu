@@ -16,8 +16,8 @@
 // direction, not the Newtonian field), so it runs on a second stream branch
 // of the captured graph, concurrently with the air chain.
 //
-// N ticks are captured once into a CUDA graph (in chunks of CHUNK ticks so
-// instantiation stays cheap) and replayed on later calls.
+// N ticks are captured once into a CUDA graph (up to CHUNK = 1000 ticks per
+// graph; longer steps replay it) and replayed on later calls.
 #include <string.h>
 
 #include <algorithm>
@@ -33,7 +33,9 @@
 using namespace tpt;
 
 namespace {
-constexpr uint32_t CHUNK = 50;  // ticks per captured graph (even)
+constexpr uint32_t CHUNK = 1000;     // ticks per captured graph at most (even)
+constexpr uint32_t TUNE_TICKS = 50;  // ticks of the graphs the autotuner times (even)
+constexpr uint32_t MAX_DEPTH = 50;   // temporal depth at most
 constexpr size_t ALIGN = 64;    // elements (256 B) between instances
 
 enum F32 { F_PV, F_VX, F_VY, F_HV, F_PV2, F_VX2, F_VY2, F_HV2, F_OPV, F_OVX, F_OVY, F_FVX, F_FVY, F_GX, F_GY, F_N32 };
@@ -838,8 +840,8 @@ int tpt_batch_set_tuning(tpt_batch *b, const tpt_batch_tuning *t) {
             TPT_FAIL(TPT_ERR_INVALID_ARG, "tile %ux%u is not a tile form shape (32x8, 64x8, 32x16, 64x16)", t->tile_x,
                      t->tile_y);
     }
-    if (t->temporal_depth < 1 || t->temporal_depth > CHUNK)
-        TPT_FAIL(TPT_ERR_INVALID_ARG, "temporal_depth %u must be in 1..%u", t->temporal_depth, CHUNK);
+    if (t->temporal_depth < 1 || t->temporal_depth > MAX_DEPTH)
+        TPT_FAIL(TPT_ERR_INVALID_ARG, "temporal_depth %u must be in 1..%u", t->temporal_depth, MAX_DEPTH);
     if (sweep && t->temporal_depth != 1)
         TPT_FAIL(TPT_ERR_UNSUPPORTED, "temporal blocking is built for the tile form; the sweep form takes depth 1");
     if (t->ctas_per_sm > 32) TPT_FAIL(TPT_ERR_INVALID_ARG, "ctas_per_sm must be 0 (as many as fit) .. 32");
@@ -1028,8 +1030,9 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
             best = t;
         }
     }
-    // Phase 2, for batches with gravity: the whole step -- the 50-tick graph a
-    // step replays, air and gravity chains together -- since the gravity
+    // Phase 2, for batches with gravity: the whole step -- a graph of
+    // TUNE_TICKS ticks as a step captures it, air and gravity chains
+    // together -- since the gravity
     // chain runs on the SMs the air launches leave idle, the air layout that
     // is fastest alone need not be fastest beside it. Finalists: the air
     // settings within 5% of the fastest air-only time (at most four), each
@@ -1061,7 +1064,7 @@ int tpt_batch_tune(tpt_batch *b, tpt_stream_t stream) {
                     pct ? std::min<uint32_t>(cap, std::max<uint32_t>(1u, (uint32_t)b->sms * pct / 100u)) : 0u;
                 rc = tpt_batch_set_tuning(b, &t);
                 cudaGraphExec_t ex = nullptr;
-                if (rc == TPT_OK) rc = graph_for(b, CHUNK, &ex);
+                if (rc == TPT_OK) rc = graph_for(b, TUNE_TICKS, &ex);
                 float ms = 1e30f;
                 for (int rep = 0; rep < 3 && rc == TPT_OK; ++rep) {  // warm-up, then the faster of two
                     cudaEventRecord(e0, st);
