@@ -1,5 +1,5 @@
-"""CPU test of bench.py's reference arm, the line the driver compares the
-GPU line against: under two ranks (RANK / WORLD_SIZE as torchrun sets them)
+"""CPU tests of bench.py: the air launch count it claims, and the reference
+arm, the line the driver compares the GPU line against: under two ranks (RANK / WORLD_SIZE as torchrun sets them)
 rank 0 prints exactly one JSON line with the contract's keys and rank 1 exits
 0 without output. The arm times the oracle's port of the reference kernels
 on host cores on a bounded sample of the C5 workload."""
@@ -43,3 +43,28 @@ def test_reference_arm_rank0_prints_one_contract_line():
     e2e = d["e2e"]
     assert e2e["value"] == d["value"] and e2e["unit"] == d["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_air_launch_count_with_temporal_blocking():
+    """bench.py's gpu_launches claim for the air chain: 2 (or 3 with a NoUpdate
+    + heat instance) launches per tick unblocked; blocks of n <= k ticks make
+    n + 1 launches (+ n settles), cut at the end of each captured graph."""
+    import types
+
+    sys.path.insert(0, ROOT)
+    import bench
+    import tpt_field as tf
+
+    def tuning(form, depth):
+        return types.SimpleNamespace(air_form=form, temporal_depth=depth)
+
+    tiles, sweep = tf.AIR_FORM_TILES, tf.AIR_FORM_SWEEP
+    assert bench.air_launches(1000, tuning(tiles, 1), 2) == 2000
+    assert bench.air_launches(1000, tuning(tiles, 1), 3) == 3000
+    assert bench.air_launches(1000, tuning(sweep, 5), 2) == 2000
+    # 1000 ticks at depth 2: 500 blocks of 3 launches
+    assert bench.air_launches(1000, tuning(tiles, 2), 2) == 1500
+    # depth 3 over graphs of 50 ticks: 16 blocks of 3 ticks (4 launches) + one of 2 (3) per graph
+    assert bench.air_launches(100, tuning(tiles, 3), 2, chunk=50) == 2 * (16 * 4 + 3)
+    # with the NoUpdate settle: n + 1 + n per block
+    assert bench.air_launches(6, tuning(tiles, 3), 3) == 2 * (3 + 1 + 3)
