@@ -729,6 +729,14 @@ int tpt_vox_save_restore_air(const tpt_vox_save *s, float *vx, float *vy, float 
  * resources, so the context stays usable. Synchronises the device.
  */
 int tpt_check_device_errors(void);
+/*
+ * Exercises that failure path without a fault: launches one device wait on
+ * a barrier that nothing completes, bounded by `limit_clocks` SM clocks, in
+ * the same bounded-wait code the batched kernels use. After it, the next
+ * tpt_check_device_errors returns TPT_ERR_DEVICE_TIMEOUT (and clears it);
+ * the context stays usable.
+ */
+int tpt_selftest_wait_timeout(uint32_t limit_clocks, tpt_stream_t stream);
 
 /* Message of the last failure on the calling thread ("" if none). */
 const char *tpt_last_error_string(void);

@@ -12,6 +12,7 @@
 #include "grav_dft.hpp"
 #include "grav_particles.hpp"
 #include "grav_plan.hpp"
+#include "tc.cuh"
 #include "tmap.hpp"
 
 namespace tpt {
@@ -114,19 +115,42 @@ struct tpt_grav_plan {
     dft::DftSet *dft = nullptr;
 };
 
+// The failure path of the bounded device waits, run without a fault: one
+// thread waits on an mbarrier that nothing arrives at, through the same
+// bounded wait the tensor-core and TMA pipelines use, and gives up after
+// `limit` SM clocks, recording ERR_WAIT_TIMEOUT in its own error word.
+static __device__ uint32_t g_selftest_err;
+
+__global__ void k_selftest_wait(long long limit) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x != 0) return;
+    tc::mbar_init(&bar, 1);
+    tc::fence_mbar_init();
+    tc::mbar_wait_limit(&bar, 0u, &g_selftest_err, limit);
+}
+
 extern "C" {
 
 const char *tpt_last_error_string(void) { return g_err; }
 
 int tpt_check_device_errors(void) {
     TPT_CUDA(cudaDeviceSynchronize());
-    uint32_t bits = 0, abits = 0;
+    uint32_t bits = 0, abits = 0, sbits = 0, z = 0;
     int rc = dft::read_errors(&bits);
     if (rc) return rc;
     rc = air::read_errors(&abits);
     if (rc) return rc;
-    bits |= abits;
+    TPT_CUDA(cudaMemcpyFromSymbol(&sbits, g_selftest_err, sizeof(sbits)));
+    TPT_CUDA(cudaMemcpyToSymbol(g_selftest_err, &z, sizeof(z)));
+    bits |= abits | sbits;
     if (bits) TPT_FAIL(TPT_ERR_DEVICE_TIMEOUT, "a device-side wait timed out (error bits 0x%x)", bits);
+    return TPT_OK;
+}
+int tpt_selftest_wait_timeout(uint32_t limit_clocks, tpt_stream_t stream) {
+    int rc = require_sm100();
+    if (rc) return rc;
+    k_selftest_wait<<<1, 32, 0, (cudaStream_t)stream>>>((long long)limit_clocks);
+    TPT_LAUNCHED();
     return TPT_OK;
 }
 uint64_t tpt_kernel_launch_count(void) { return g_launches.load(); }

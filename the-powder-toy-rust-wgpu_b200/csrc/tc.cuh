@@ -50,17 +50,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 }
 
 // Waits for the phase of `parity` to complete. Returns false (and records
-// ERR_WAIT_TIMEOUT in *err) if it does not complete within the limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *err) {
+// ERR_WAIT_TIMEOUT in *err) if it does not complete within `limit` SM clocks.
+__device__ __forceinline__ bool mbar_wait_limit(uint64_t *bar, uint32_t parity, uint32_t *err, long long limit) {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > WAIT_LIMIT_CLOCKS) {
+        if (clock64() - t0 > limit) {
             atomicOr(err, ERR_WAIT_TIMEOUT);
             return false;
         }
     }
     return true;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t *err) {
+    return mbar_wait_limit(bar, parity, err, WAIT_LIMIT_CLOCKS);
 }
 
 // 2-D TMA tile load global -> shared, completion counted on `bar`.

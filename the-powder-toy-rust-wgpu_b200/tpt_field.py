@@ -56,7 +56,7 @@ EXPORTS = [
     "tpt_save_retain_air_pressure", "tpt_save_instance_desc", "tpt_vox_save_config_default", "tpt_vox_save_create",
     "tpt_vox_save_decode", "tpt_vox_save_encode", "tpt_vox_save_destroy", "tpt_vox_save_get_info",
     "tpt_vox_save_get_config", "tpt_vox_save_set_config", "tpt_vox_save_array_read", "tpt_vox_save_array_write",
-    "tpt_vox_save_restore_air", "tpt_check_device_errors",
+    "tpt_vox_save_restore_air", "tpt_check_device_errors", "tpt_selftest_wait_timeout",
     "tpt_last_error_string", "tpt_kernel_launch_count", "tpt_version",
 ]
 SAVE_GRIDS = ("air_vx", "air_vy", "air_pv", "air_hv", "fan_vx", "fan_vy", "wall_bmap", "wall_emap")
@@ -267,6 +267,7 @@ def lib() -> ctypes.CDLL:
         L.tpt_vox_save_array_read.argtypes = [P, i32, P, ctypes.c_size_t]
         L.tpt_vox_save_array_write.argtypes = [P, i32, P, ctypes.c_size_t]
         L.tpt_vox_save_restore_air.argtypes = [P] * 7
+        L.tpt_selftest_wait_timeout.argtypes = [u32, P]
         L.tpt_last_error_string.restype = ctypes.c_char_p
         L.tpt_kernel_launch_count.restype = ctypes.c_uint64
         L.tpt_version.restype = ctypes.c_char_p
