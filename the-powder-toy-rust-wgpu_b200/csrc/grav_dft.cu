@@ -242,18 +242,18 @@ __global__ void __launch_bounds__(THREADS, 1)
                         // K' tile kt: real parts (planes 0, 1), then imaginary parts (2, 3)
                         const uint32_t kh = P.ktiles / 2, part = kt >= kh ? 1u : 0u;
                         const int32_t k0 = (int32_t)((kt - part * kh) * KT);
+                        if (P.a_mn) {
+                            // MN-major A: planes 2 part (hi) and 2 part + 1 (lo), each four
+                            // 32(m) x 32(k) blocks 2 KB apart, as one 4-D box
+                            const uint32_t f = P.a_mn - 1;
+                            tc::tma_load_4d(st, P.ta, 0, (int32_t)((4 * part + f) * P.a_rows) + k0, m0 / 32, 0,
+                                            &full_bar[s]);
+                        }
                         for (uint32_t p = 0; p < 2; ++p) {
                             const uint32_t pl = 2 * part + p;
-                            if (P.a_mn) {
-                                // MN-major A: four 32(m) x 32(k) boxes, 2 KB apart
-                                const uint32_t f = P.a_mn - 1;
-                                for (uint32_t j = 0; j < 4; ++j)
-                                    tc::tma_load_2d(st + p * TILE_BYTES + j * 2048, P.ta, m0 + (int32_t)(32 * j),
-                                                    (int32_t)((pl * 2 + f) * P.a_rows) + k0, &full_bar[s]);
-                            } else {
+                            if (!P.a_mn)
                                 tc::tma_load_2d(st + p * TILE_BYTES, P.ta, k0, (int32_t)(pl * P.a_rows) + m0,
                                                 &full_bar[s]);
-                            }
                             tc::tma_load_2d(st + B_OFF + p * BPB, P.tb, k0, (int32_t)(pl * P.b_rows) + n0,
                                             &full_bar[s]);
                         }
@@ -828,6 +828,27 @@ struct DftImpl {
 
 // Row-major bf16 matrix of `rows_total` rows of `kpitch` elements; boxes of
 // 32 elements (64 bytes) x box_rows rows.
+// R^-1's MN-major A operand of a Toeplitz group (aRiT: rows (plane, f, kx)
+// of MpT m' each) as one box per K tile: both planes of one part (hi, lo:
+// 2 * kpRi rows apart), four blocks of 32 m' (64 bytes apart in memory),
+// 32 kx rows -- in shared memory [plane][m block][kx][32 m'], i.e. the four
+// 32 x 32 boxes per plane 2 KB apart that the MN-major descriptor reads.
+// Dims (m' in block, row, m block, plane); rows cover the bases (4 part + f)
+// kpRi + k0 the loads use.
+static int make_tmap_mn4(CUtensorMap *out, const bf16 *base, uint32_t MpT, uint32_t kpRi) {
+    auto fn = encode_fn();
+    if (!fn) TPT_FAIL(TPT_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled is not available from the driver");
+    cuuint64_t dims[4] = {32, (cuuint64_t)6 * kpRi, MpT / 32, 2};
+    cuuint64_t strides[3] = {(cuuint64_t)MpT * 2, 64, (cuuint64_t)2 * kpRi * MpT * 2};
+    cuuint32_t box[4] = {32, KT, 4, 2};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = fn(out, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16 *>(base), dims, strides, box, estr,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) TPT_FAIL(TPT_ERR_CUDA, "cuTensorMapEncodeTiled (4-D MN-major operand) failed (%d)", (int)r);
+    return TPT_OK;
+}
+
 static int make_tmap(CUtensorMap *out, const bf16 *base, uint32_t kpitch, uint32_t rows_total,
                      uint32_t box_rows = MT) {
     auto fn = encode_fn();
@@ -1068,8 +1089,8 @@ int DftSet::create(const std::vector<JobShape> &shapes) {
             // T: A = bT (rows (kx, inst, re/im)), B = the (f, kx) strips (sbox-row boxes)
             if ((rc = make_tmap(&tmh[2], H.ts, KT, 2 * 2 * g.N1h * g.SR, g.sbox))) return rc;
             if ((rc = make_tmap(&tmh[3], g.bT, g.kpC, 2 * g.rowsT))) return rc;
-            // R^-1: A = aRiT read M-major, 32 x 32 boxes (rows (plane, f, kx))
-            if ((rc = make_tmap(&tmh[6], g.aRiT, g.MpT, 8 * g.kpRi, 32))) return rc;
+            // R^-1: A = aRiT read M-major, both planes of a K tile in one 4-D box
+            if ((rc = make_tmap_mn4(&tmh[6], g.aRiT, g.MpT, g.kpRi))) return rc;
             const uint32_t pt = (uint32_t)pr.size();
             pr.push_back({tmd + 3, tmd + 2, gi32, 2 * g.G, g.Y, g.kpC / KT, g.rowsT, 0, 0});
             // kx slowest, so the tiles of one kx (both fields, all M tiles)
