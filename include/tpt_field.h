@@ -357,7 +357,9 @@ enum {
 
 /* Tuning knobs the autotuner picks (and a caller may pin). Results are the
  * same for every value: they change how the work is laid out, not what is
- * computed. */
+ * computed. A new batch starts at {32, 8, 1, 0, 0, TPT_AIR_FORM_TILES, 1}:
+ * 32x8 tiles, no temporal blocking, each pass at its own residency, one
+ * gravity stream, the tile form with the work queue. */
 typedef struct tpt_batch_tuning {
     /* The air form's work unit. Tile form: the tile, tile_x x tile_y cells,
      * one of 32x8 (the default), 64x8, 32x16 and 64x16, one thread per cell.
@@ -386,10 +388,10 @@ typedef struct tpt_batch_tuning {
      * for every value. */
     uint32_t grav_side_ctas;
     uint32_t air_form;  /* TPT_AIR_FORM_TILES or TPT_AIR_FORM_SWEEP */
-    /* Tile form: 1 = the persistent CTAs take tiles from an atomic work
-     * queue (a counter per pass, cleared by the other pass's launch), 0 =
-     * they stride the tile list statically. The sweep form always takes its
-     * work items from a queue; 0 or 1. */
+    /* Tile form: 1 (the default) = the persistent CTAs take tiles from an
+     * atomic work queue (a counter per pass, cleared by the other pass's
+     * launch), 0 = they stride the tile list statically. The sweep form
+     * always takes its work items from a queue; 0 or 1. */
     uint32_t work_queue;
 } tpt_batch_tuning;
 
