@@ -87,9 +87,12 @@ __global__ void __launch_bounds__(NT) rows_inverse(const Job *__restrict__ jobs,
 }
 
 // ---- the warp form: one warp per 1-D transform ---------------------------------
-// 128-thread CTAs: the kernels hold a whole transform per warp in registers
-// (91 to 168 per thread), so CTAs of four warps let three or more share an SM
-// where CTAs of eight warps left registers unused (C4 solve 1.36 -> 1.06 ms).
+// 128-thread CTAs: the kernels hold a whole transform per warp in registers,
+// so CTAs of four warps let several share an SM where CTAs of eight warps left
+// registers unused (C4 solve 1.36 -> 1.06 ms). The register caps trade a few
+// spills for more resident warps: forward rows 6 CTAs per SM (80 registers),
+// columns 4 (128), inverse rows 5 (96); uncapped (91, 168, 158 registers: 5,
+// 3, 3 CTAs) the C4 solve took 1.074 ms per tick, capped 0.988 ms.
 constexpr int NTW = 128;
 constexpr int WARPS = NTW / 32;
 
@@ -113,7 +116,7 @@ template <int M> __device__ __forceinline__ void row_fwd_warp(const Job &J, uint
     for (int k = 0; k < M; ++k) dst[32 * k + lane] = v[k];
 }
 
-__global__ void __launch_bounds__(NTW) rows_forward_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
+__global__ void __launch_bounds__(NTW, 6) rows_forward_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
                                                      uint32_t nrefs, const JobIO io) {
     const uint32_t w = blockIdx.x * WARPS + threadIdx.x / 32;
     if (w >= nrefs) return;
@@ -180,7 +183,7 @@ __device__ __forceinline__ void col_warp(const Job &J, uint32_t c, float2 *tx, f
 // 2 * WARPS consecutive positions), each warp transforms one column, and both
 // fields' Y x WARPS tiles go back the same way. Per warp: `ystride` entries of
 // the x field tile, `fstride` (>= n2) of the spectrum stash / y field tile.
-__global__ void __launch_bounds__(NTW) cols_convolve_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
+__global__ void __launch_bounds__(NTW, 4) cols_convolve_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
                                                       uint32_t ystride, uint32_t fstride) {
     extern __shared__ float2 sm2[];
     const BlockRef r = refs[blockIdx.x];
@@ -255,7 +258,7 @@ template <int M> __device__ __forceinline__ void row_inv_warp(const Job &J, uint
     }
 }
 
-__global__ void __launch_bounds__(NTW) rows_inverse_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
+__global__ void __launch_bounds__(NTW, 5) rows_inverse_w(const Job *__restrict__ jobs, const BlockRef *__restrict__ refs,
                                                      uint32_t nrefs, const JobIO io) {
     const uint32_t w = blockIdx.x * WARPS + threadIdx.x / 32;
     if (w >= nrefs) return;
