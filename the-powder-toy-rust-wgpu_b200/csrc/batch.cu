@@ -7,10 +7,13 @@
 // The air state (pv, vx, vy, hv and the two wall masks) has a second copy
 // (ping-pong) for the air tick's two forms, chosen by the tuning: the tile
 // form (air_tiles.cu; two TMA-staged tile passes per tick, heat and masks in
-// the ping-pong halves, pv/vx/vy in place) or the row sweep (air_sweep.cu;
-// one launch per tick plus a velocity pre-pass that only works for instances
-// flagged by the previous tick, every state grid in ping-pong halves). After
-// an odd tick count one copy-back restores the canonical buffers. Gravity (instances with
+// the ping-pong halves, pv/vx/vy in place; with temporal blocking, blocks of
+// k ticks whose middle launches fuse one tick's second pass with the next
+// tick's first, air_fused.cu) or the row sweep (air_sweep.cu; one launch per
+// tick plus a velocity pre-pass that only works for instances flagged by the
+// previous tick, every state grid in ping-pong halves). The sweep's halves
+// serve the tile form as the second set of velocity-pass outputs. After an
+// odd tick count one copy-back restores the canonical buffers. Gravity (instances with
 // newton_grav) is independent of air in the field step
 // (crates/tpt-sim/src/air_kernel/heat.rs:182-203 uses the configured
 // direction, not the Newtonian field), so it runs on a second stream branch
