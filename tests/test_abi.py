@@ -111,3 +111,29 @@ def test_python_mirror_fails_loudly_without_a_gpu(tf):
         setattr(b, name, 16)  # never dereferenced: the device check comes first
     rc = tf.lib().tpt_air_step(ctypes.byref(p), ctypes.byref(b), None)
     assert rc in (-3, -7)
+
+
+def test_python_struct_mirrors_match_the_header(tf):
+    """The ctypes mirrors of the C structs the batch API passes by pointer
+    (tpt_batch_tuning, tpt_batch_profile) list the header's fields in the
+    header's order, so a field appended to one side only fails here on CPU."""
+    import os
+    import re
+
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include",
+                            "tpt_field.h")).read()
+
+    def fields(struct):
+        body = re.search(r"typedef struct %s \{(.*?)\} %s;" % (struct, struct), hdr, re.S).group(1)
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        names = []
+        for decl in body.split(";"):
+            decl = decl.strip()
+            if not decl:
+                continue
+            decl = re.sub(r"^\w+\s+", "", decl)  # the type
+            names += [n.strip() for n in decl.split(",")]
+        return names
+
+    assert fields("tpt_batch_tuning") == [n for n, _ in tf.BatchTuning._fields_]
+    assert fields("tpt_batch_profile") == [n for n, _ in tf.BatchProfile._fields_]
