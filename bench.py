@@ -823,8 +823,8 @@ def main():
                     help="with --air-form: tile (tiles) or lanes x rows (sweep), e.g. 64x16")
     ap.add_argument("--temporal-depth", type=int, default=1,
                     help="with --air-form tiles: ticks per temporally blocked run (1 = none)")
-    ap.add_argument("--work-queue", type=int, choices=(0, 1), default=0,
-                    help="with --air-form tiles: 1 = atomic tile queue, 0 = static striding")
+    ap.add_argument("--work-queue", type=int, choices=(0, 1), default=1,
+                    help="with --air-form tiles: 1 = atomic tile queue (the library's default), 0 = static striding")
     ap.add_argument("--skip-tune", action="store_true", help="keep the batch's default tuning (profiling captures)")
     ap.add_argument("--instances", type=int, default=0,
                     help="only the first N instances of the workload (profiling captures on a smaller case)")
